@@ -1,0 +1,326 @@
+"""Benchmark of the l2 LD-score hot path: r^2-pairs/sec on one B200.
+
+Workload (N = 1): the exact biobank-scale configuration -- synthetic panel
+N = 50,000 individuals x M = 100,000 SNPs (200 founders, 1% missing, 100 cM),
+--ld-wind-cm 1 --snp-level-masking.  One step = one full l2 pass over the
+panel (decode + band Gram + r^2 epilogue + l2 back to the host) in the
+INT8-exact form.  The plain FP64 form is timed on the same panel for the
+INT8-vs-FP64 ratio.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With --gpus N (launched by torchrun) each rank computes its own chromosome
+(an independent 100,000-SNP panel, seed + rank): weak scaling, no collective
+on the data path; the time is the max over ranks.  The reference arm
+(--impl reference) times the C restatement of the reference's CPU l2 path
+(the reference is Rust and cannot be compiled in this image) on all host
+cores, on a bounded SNP sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "r2 pairs/sec (INT8 exact vs FP64 plain, same GPU); p50/p99 request latency"
+CPU_SAMPLE_SNPS = 3000
+
+
+def workload_spec(seed_offset=0):
+    from ldsc_b200 import synth
+    s = synth.spec_biobank()
+    s.seed += seed_offset
+    return s
+
+
+def config_dict(spec, workload="biobank exact l2, 1 cM, per-SNP masking"):
+    return {"workload": workload, "n_indiv": spec.n_indiv, "n_snp": spec.m, "founders": spec.founders,
+            "missing": spec.miss, "window": "1 cM", "snp_level_masking": True, "chunk_size": 200,
+            "l2_flush": "inputs larger than L2 (1.25 GB packed panel, 10 GB INT8 operands)"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+def committed_traffic(kernel: str):
+    """DRAM bytes per launch of the kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get(kernel)
+    return None
+
+
+def cpu_baseline(body_rows, spec, chr_, cm, bp, n_threads=0):
+    """The C restatement of the reference's l2 (OpenMP, all host threads) on
+    the first CPU_SAMPLE_SNPS SNPs of the panel, same flags."""
+    sys.path.insert(0, ROOT)
+    from oracle import OracleL2Args, max_threads, oracle_l2
+    m = body_rows.shape[0]
+    a = OracleL2Args(bed_body=body_rows, n_file_indiv=spec.n_indiv, chr=chr_[:m], cm=cm[:m], bp=bp[:m],
+                     mode="cm", wind=1.0, chunk_c=200, masking=True, per_chr=True, n_threads=n_threads)
+    t0 = time.perf_counter()
+    _, _, pairs, _ = oracle_l2(a)
+    dt = time.perf_counter() - t0
+    return pairs / dt, pairs, dt, (n_threads or max_threads())
+
+
+def run_reference(args):
+    """--impl reference: the reference's CPU path (C restatement) on host cores."""
+    from ldsc_b200 import synth
+    spec = workload_spec()
+    chr_, cm, bp = synth.positions(spec)
+    rows = synth.bed_body(spec, 0, CPU_SAMPLE_SNPS)
+    for _ in range(args.warmup):
+        cpu_baseline(rows[:200], spec, chr_, cm, bp)
+    vals, tot_pairs, tot_t = [], 0, 0.0
+    cores = None
+    for _ in range(args.steps):
+        v, pairs, dt, cores = cpu_baseline(rows, spec, chr_, cm, bp)
+        vals.append(v)
+        tot_pairs += pairs
+        tot_t += dt
+    value = tot_pairs / tot_t
+    sample = (f"first {CPU_SAMPLE_SNPS} SNPs of the N=50,000 x M=100,000 panel per step "
+              "(1 cM, per-SNP masking, chunk 200, f64)")
+    out = {"metric": METRIC, "impl": "reference", "value": value, "unit": "r2 pairs/s", "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_t / args.steps,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic (seeded founder-mosaic panel)", "config": config_dict(spec),
+           "cpu_baseline": {"value": value, "unit": "r2 pairs/s", "cores": cores, "kind": "port",
+                            "sample": sample},
+           "e2e": {"value": value, "unit": "r2 pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+           "note": "reference is Rust (no cargo/rustc in this image); timed arm is the C restatement "
+                   "oracle/ldsc_oracle.c of its CPU l2 path"}
+    print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--fp64-steps", type=int, default=2)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        run_reference(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from ldsc_b200.build import build
+    build()
+    from ldsc_b200 import synth
+    from ldsc_b200.api import Context, WindowMode, l2_from_bed_bytes, pair_count, run_l2
+    from ldsc_b200.plink import BimTable
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    ctx = Context(local)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+
+    spec = workload_spec(seed_offset=rank)
+    chr_, cm, bp = synth.positions(spec)
+    m = spec.m
+    snps = BimTable(chr_, [f"rs{i}" for i in range(m)], cm, bp, np.arange(m, dtype=np.int64))
+    panel = ctx.synth(spec.n_indiv, m, spec.founders, spec.switch_p, spec.miss, spec.seed)
+    wm = WindowMode.Cm(1.0)
+    npairs = pair_count(snps, wm, 200, snp_level_masking=True)
+
+    def step(precision):
+        return run_l2(ctx, snps, panel, wm, 200, snp_level_masking=True, precision=precision, yes_really=True)
+
+    # ---- INT8 form, inputs resident in HBM ----
+    for _ in range(args.warmup):
+        step("int8")
+    sampler = ClockSampler(local)
+    sampler.start()
+    barrier()
+    torch.cuda.synchronize()
+    k0 = ctx.kernel_count
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    gram_s = []
+    for _ in range(args.steps):
+        _, _, perf = step("int8")
+        gram_s.append(perf.ab_dot_secs)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.stop()
+    launches = ctx.kernel_count - k0
+    t_local = ev0.elapsed_time(ev1) / 1e3
+    t_max, pairs_all = t_local, npairs
+    if world > 1:
+        tt = torch.tensor([t_local], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        pp = torch.tensor([npairs], device="cuda", dtype=torch.float64)
+        dist.all_reduce(pp, op=dist.ReduceOp.SUM)
+        t_max, pairs_all = float(tt.item()), float(pp.item())
+    value = pairs_all * args.steps / t_max
+    gram_avg = float(np.mean(gram_s))
+
+    # ---- FP64 plain form, same panel ----
+    step("fp64")
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    fp64_gram = []
+    for _ in range(args.fp64_steps):
+        _, _, p64 = step("fp64")
+        fp64_gram.append(p64.ab_dot_secs)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t64 = e0.elapsed_time(e1) / 1e3
+    fp64_value = npairs * args.fp64_steps / t64
+
+    # ---- end to end through the whole-file C ABI entry point, host buffers ----
+    e2e = None
+    if not args.no_e2e:
+        rows = panel.download()
+        bed = torch.empty(3 + rows.size, dtype=torch.uint8, pin_memory=True)
+        bnp = bed.numpy()
+        bnp[:3] = [0x6C, 0x1B, 0x01]
+        bnp[3:] = rows.reshape(-1)
+        del rows
+        for _ in range(1):
+            l2_from_bed_bytes(ctx, bnp, spec.n_indiv, snps, wm, 200, precision="int8", snp_level_masking=True)
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            l2_from_bed_bytes(ctx, bnp, spec.n_indiv, snps, wm, 200, precision="int8", snp_level_masking=True)
+        torch.cuda.synchronize()
+        te = time.perf_counter() - t0
+        if world > 1:
+            tt = torch.tensor([te], device="cuda", dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            te = float(tt.item())
+        e2e = {"value": pairs_all * args.steps / te, "unit": "r2 pairs/s", "h2d_bytes_per_step": int(bnp.size),
+               "d2h_bytes_per_step": int(16 * m), "ms_per_step": 1e3 * te / args.steps,
+               "api": "ldsc_l2_from_bed (validate + upload + compute + download)"}
+
+    # ---- roofline of the dominant kernel (INT8 band Gram) ----
+    hbm, bf16, src = measured_peaks()
+    int8_peak = 2.0 * bf16   # dense int8 tensor rate is 2x bf16 on sm_100
+    ops = 8.0 * spec.n_indiv * npairs   # 4 integer products x 2 ops x N per in-band pair
+    achieved = ops / gram_avg / 1e12
+    roofline = {"bound": "tensor", "achieved": achieved, "peak": int8_peak, "unit": "TFLOP/s",
+                "frac": achieved / int8_peak, "traffic": committed_traffic("k_gram_i8"),
+                "kernel": "k_gram_i8 (tcgen05.mma kind::i8)",
+                "note": f"int8 ops counted like flops (2 per MAC, 4 products per pair); peak = 2 x {src} "
+                        "bf16 dense burst (MEASURED_PEAKS.json), nominal int8 dense 4500"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        rows = panel.download(0, CPU_SAMPLE_SNPS)
+        v, pairs_s, dt, cores = cpu_baseline(rows, spec, chr_, cm, bp)
+        cpu = {"value": v, "unit": "r2 pairs/s", "cores": cores, "kind": "port",
+               "sample": f"first {CPU_SAMPLE_SNPS} SNPs of the panel ({pairs_s} pairs, {dt:.1f} s), same flags, f64"}
+
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": "r2 pairs/s", "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "int8 (int32 accumulate, f64 epilogue)",
+               "data": "synthetic (seeded founder-mosaic panel generated on the device)",
+               "config": config_dict(spec), "e2e": e2e, "gpu_launches": int(launches),
+               "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
+               "forms": {"int8_pairs_per_s": value / world, "fp64_pairs_per_s": fp64_value,
+                         "int8_over_fp64": (value / world) / fp64_value,
+                         "int8_gram_ms": 1e3 * gram_avg, "fp64_gram_ms": 1e3 * float(np.mean(fp64_gram)),
+                         "n_pairs_per_rank": npairs}}
+        print(json.dumps(out))
+    panel.close()
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

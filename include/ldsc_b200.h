@@ -1,0 +1,224 @@
+/*
+ * ldsc_b200.h -- C ABI of the B200 LD-score engine (libldsc_b200.so).
+ *
+ * Plain C types only: pointers, sizes, status codes.  Every entry point
+ * returns an `int` status (LDSC_OK = 0, negative on error); the message of the
+ * last failure on a context is available from ldsc_last_error().
+ *
+ * The engine replaces the compute core of ldsc-rs's `l2` subcommand:
+ *
+ *   compute_ldscore_global(all_snps, bed, mmap_bed, n_indiv, mode, chunk_c,
+ *       annot, iid_indices, pq_exp, yes_really, [gpu_ctx, gpu_config],
+ *       use_f32, verbose_timing, sketch, sketch_maf_aware,
+ *       snp_level_masking, on_progress) -> (l2 M x K, maf, L2Perf)
+ *   (reference: src/l2/compute.rs:1009-1028)
+ *
+ * and the per-chromosome / --global-pass fan-out around it in `l2::run`
+ * (src/l2/mod.rs:439-575).  One call of ldsc_l2_run() computes every
+ * chromosome of the record list; in the default per-chromosome mode each
+ * chromosome is chunked from its own first SNP exactly as the reference's
+ * per-chromosome rayon tasks do.
+ *
+ * Thread safety: a context serialises its calls with an internal mutex, so
+ * the reference's concurrent per-chromosome callers (src/l2/mod.rs:502-553)
+ * may share one context.  There is no CPU fallback: every compute entry point
+ * fails with LDSC_E_CUDA when no usable GPU is present.
+ */
+#ifndef LDSC_B200_H
+#define LDSC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LDSC_B200_ABI_VERSION 1
+
+typedef struct ldsc_ctx ldsc_ctx;
+typedef struct ldsc_panel ldsc_panel;
+
+/* Status codes. */
+enum {
+    LDSC_OK = 0,
+    LDSC_E_INVALID = -1,      /* malformed arguments (anyhow::ensure! failures in the reference) */
+    LDSC_E_NOMEM = -2,        /* device allocation failed */
+    LDSC_E_CUDA = -3,         /* CUDA runtime / driver error, or no GPU */
+    LDSC_E_TIMEOUT = -4,      /* a device wait exceeded its bound and the kernel gave up */
+    LDSC_E_UNSUPPORTED = -5,  /* valid request outside what this build implements */
+    LDSC_E_BED = -6           /* BED header / length validation failed (src/bed.rs:73-110) */
+};
+
+/* Window definition, WindowMode (src/l2/window.rs:5-12). */
+enum { LDSC_WINDOW_CM = 0, LDSC_WINDOW_KB = 1, LDSC_WINDOW_SNP = 2 };
+
+/* Arithmetic form of the exact window Gram. */
+enum {
+    LDSC_PRECISION_FP64 = 0,  /* plain form: standardised f64 columns, f64 Gram (the reference method) */
+    LDSC_PRECISION_INT8 = 1   /* genotype/mask INT8 tcgen05 Gram, INT32 accumulation, exact epilogue */
+};
+
+/* Per-chunk progress, L2Progress (src/l2/mod.rs:22-39).  The engine reports
+ * progress per Gram launch rather than per 200-SNP chunk. */
+typedef struct {
+    uint64_t chunks_done;
+    uint64_t chunks_total;
+    uint64_t snps_done;
+    uint64_t snps_total;
+    double chunk_wall_ms;
+} ldsc_progress;
+
+typedef void (*ldsc_progress_fn)(const ldsc_progress *progress, void *user);
+
+/* Per-phase timing, L2Perf (src/l2/mod.rs:1016-1034), plus device detail.
+ * Phase times are device (CUDA event) times of this call's kernels. */
+typedef struct {
+    uint64_t m;                 /* SNP records of the call */
+    uint64_t n_indiv;           /* individuals used (after --keep) */
+    double bed_read_secs;       /* host->device upload of BED bytes done by this call */
+    double norm_secs;           /* decode + per-SNP stats + standardisation */
+    double sketch_secs;         /* CountSketch projection; negative when not sketching */
+    double bb_dot_secs;         /* 0: the within-chunk block is part of the band Gram */
+    double ab_dot_secs;         /* band Gram + r^2 epilogue + l2 accumulation */
+    double ring_store_secs;     /* 0: the panel is resident, there is no ring buffer */
+    uint64_t n_pairs;           /* off-diagonal (j,k) pairs contributing to l2 in this mode */
+    uint64_t n_tiles;           /* Gram tiles launched */
+    uint32_t kernel_launches;   /* kernels launched by this call */
+    uint32_t gram_kind;         /* 0 fp64, 1 int8 tcgen05, 2 fp32 sketch */
+    double device_ms;           /* whole call, device time */
+} ldsc_perf;
+
+/* Arguments of one l2 computation.  Record i of the call is BED row
+ * bed_idx[i] of the panel (the reference's BimRecord.bed_idx). */
+typedef struct {
+    uint64_t n_snp;               /* number of SNP records */
+    const uint64_t *bed_idx;      /* BED row per record; NULL = records are rows 0..n_snp-1 */
+    const uint8_t *chr;           /* chromosome code per record (BimRecord.chr) */
+    const double *cm;             /* genetic position (cM) per record */
+    const uint32_t *bp;           /* physical position per record */
+    int32_t window_mode;          /* LDSC_WINDOW_* */
+    double window_size;           /* cM or kb */
+    uint64_t window_snps;         /* half-window in SNPs for LDSC_WINDOW_SNP */
+    uint32_t chunk_size;          /* --chunk-size (default 200) */
+    int32_t global_pass;          /* 1 = --global-pass; 0 = per-chromosome (default) */
+    int32_t snp_level_masking;    /* --snp-level-masking */
+    int32_t precision;            /* LDSC_PRECISION_* for exact mode */
+    int32_t use_f32;              /* --fast-f32: accepted; exact modes keep their own arithmetic */
+    uint32_t sketch_d;            /* --sketch d; 0 = exact */
+    int32_t sketch_maf_aware;     /* --sketch-maf-aware */
+    const int64_t *keep_iids;     /* --keep: FAM indices of kept individuals; NULL = all */
+    uint64_t n_keep;
+    const double *annot;          /* M x K column-major annotation; NULL = single all-ones column */
+    uint32_t n_annot;             /* K */
+    int32_t has_pq_exp;           /* --pq-exp / --per-allele applied inside the compute */
+    double pq_exp;
+    int32_t yes_really;           /* --yes-really: silence the whole-chromosome window warning */
+    ldsc_progress_fn on_progress; /* optional */
+    void *progress_user;
+} ldsc_l2_args;
+
+/* Synthetic panel description (seeded founder mosaic; see ldsc_b200/synth.py). */
+typedef struct {
+    uint64_t n_indiv;
+    uint64_t n_snp;
+    uint32_t founders;
+    double switch_p;
+    double miss;
+    uint64_t seed;
+} ldsc_synth_spec;
+
+/* ---- library / context ------------------------------------------------ */
+
+int ldsc_abi_version(void);
+
+/* Create a context on CUDA device `device` (the reference creates one
+ * GpuContext per run and shares it across chromosomes: src/l2/mod.rs:410-436).
+ * flags: reserved, pass 0. */
+int ldsc_ctx_create(int device, uint32_t flags, ldsc_ctx **out);
+int ldsc_ctx_destroy(ldsc_ctx *ctx);
+
+/* Launch this context's work on an existing cudaStream_t (NULL = the
+ * context's own stream). */
+int ldsc_ctx_set_stream(ldsc_ctx *ctx, void *cuda_stream);
+
+/* Copy the last error message of the context into buf (always terminated). */
+int ldsc_last_error(const ldsc_ctx *ctx, char *buf, size_t len);
+
+/* Number of kernels this context has launched since creation. */
+uint64_t ldsc_ctx_kernel_count(const ldsc_ctx *ctx);
+
+/* ---- BED validation and resident panels -------------------------------- */
+
+/* Bed::from_bytes header/length validation (src/bed.rs:53-128) on a whole
+ * .bed image (magic + body).  Host only; no GPU needed.  Returns LDSC_E_BED
+ * with the reference's message ("invalid magic bytes", "not SNP-major",
+ * "invalid length") in err. */
+int ldsc_bed_validate(const uint8_t *bed_file, uint64_t len, uint64_t n_indiv, uint64_t n_snp,
+                      char *err, size_t errlen);
+
+/* Upload a BED body (SNP-major, ceil(n_indiv/4) bytes per SNP, no magic)
+ * into device memory, where it stays resident until ldsc_panel_destroy. */
+int ldsc_panel_upload(ldsc_ctx *ctx, const uint8_t *bed_body, uint64_t body_bytes,
+                      uint64_t n_indiv, uint64_t n_snp, ldsc_panel **out);
+
+/* Generate a synthetic panel directly in device memory. */
+int ldsc_panel_synth(ldsc_ctx *ctx, const ldsc_synth_spec *spec, ldsc_panel **out);
+
+/* Copy BED rows [snp_begin, snp_end) of a panel to host (ceil(n_indiv/4)
+ * bytes per row, no magic). */
+int ldsc_panel_download(ldsc_ctx *ctx, const ldsc_panel *panel, uint64_t snp_begin,
+                        uint64_t snp_end, uint8_t *out);
+
+int ldsc_panel_destroy(ldsc_panel *panel);
+
+/* ---- the l2 computation ------------------------------------------------ */
+
+/* compute_ldscore_global on a resident panel.  l2_out: n_snp x K column-major
+ * (K = n_annot, or 1 without annotation); maf_out: n_snp.  Host pointers. */
+int ldsc_l2_run(ldsc_ctx *ctx, const ldsc_panel *panel, const ldsc_l2_args *args, double *l2_out,
+                double *maf_out, ldsc_perf *perf);
+
+/* compute_l2_from_bytes / compute_l2_from_bed (src/l2/mod.rs:1049-1169) on a
+ * whole .bed image in host memory: validate, upload, compute, return. */
+int ldsc_l2_from_bed(ldsc_ctx *ctx, const uint8_t *bed_file, uint64_t len, uint64_t n_indiv,
+                     const ldsc_l2_args *args, double *l2_out, double *maf_out, ldsc_perf *perf);
+
+/* Number of off-diagonal pairs the call would accumulate (host only). */
+int ldsc_l2_pair_count(const ldsc_l2_args *args, uint64_t *n_pairs);
+
+/* Per-record left window limit L[i] (host only): record i pairs with every
+ * record k, L[i] <= k < i.  Masked mode: the per-SNP block_left
+ * (src/l2/window.rs:32-90); chunked mode: the chunk's ring-window start
+ * (src/l2/compute.rs:1164-1184,1288-1299). */
+int ldsc_l2_left_limits(const ldsc_l2_args *args, int64_t *left_out);
+
+/* ---- CountSketch ------------------------------------------------------- */
+
+/* CountSketchProj::new(n_indiv, d, seed) bucket/sign stream
+ * (src/l2/compute.rs:178-192; fastrand 2.3.0 WyRand).  Host only. */
+int ldsc_countsketch_hash(uint64_t n_indiv, uint32_t d, uint64_t seed, uint32_t *bucket,
+                          float *sign);
+
+/* Fused decode -> standardise -> CountSketch scatter -> ratio renorm of BED
+ * rows [snp_begin, snp_end) with explicit bucket/sign arrays
+ * (scatter_one_column_f32, src/wasm_simd.rs:1617-1784).  out: rows x d f32,
+ * row-major (one sketched SNP per row).  keep_iids may be NULL. */
+int ldsc_sketch_project(ldsc_ctx *ctx, const ldsc_panel *panel, uint64_t snp_begin,
+                        uint64_t snp_end, const int64_t *keep_iids, uint64_t n_keep,
+                        const uint32_t *bucket, const float *sign, uint32_t d, float *out);
+
+/* ---- diagnostics ------------------------------------------------------- */
+
+/* Raw INT32 accumulators of the INT8 tcgen05 Gram for one tile: A side =
+ * records [k0, k0+64) (genotype row, mask row interleaved: 128 rows), B side =
+ * records [j0, j0+128) (256 rows).  out: 128 x 256 int32 row-major.  Used to
+ * check the tensor-core Gram bit-exactly against an integer recompute. */
+int ldsc_debug_gram_i8_tile(ldsc_ctx *ctx, const ldsc_panel *panel, uint64_t k0, uint64_t j0,
+                            int32_t *out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LDSC_B200_H */

@@ -1,0 +1,119 @@
+"""ctypes declarations of the C ABI in include/ldsc_b200.h.
+
+The shared library is built in-tree (``python -m ldsc_b200.build``).  There is
+no fallback: if ``libldsc_b200.so`` is missing, importing the compute API
+raises, and every compute call fails on a machine without a B200.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libldsc_b200.so")
+
+LDSC_OK = 0
+LDSC_E_INVALID = -1
+LDSC_E_NOMEM = -2
+LDSC_E_CUDA = -3
+LDSC_E_TIMEOUT = -4
+LDSC_E_UNSUPPORTED = -5
+LDSC_E_BED = -6
+
+STATUS_NAMES = {
+    LDSC_E_INVALID: "invalid argument",
+    LDSC_E_NOMEM: "out of device memory",
+    LDSC_E_CUDA: "CUDA error",
+    LDSC_E_TIMEOUT: "device wait timed out",
+    LDSC_E_UNSUPPORTED: "unsupported",
+    LDSC_E_BED: "invalid BED",
+}
+
+WINDOW_CM, WINDOW_KB, WINDOW_SNP = 0, 1, 2
+PRECISION_FP64, PRECISION_INT8 = 0, 1
+
+
+class Progress(C.Structure):
+    _fields_ = [("chunks_done", C.c_uint64), ("chunks_total", C.c_uint64),
+                ("snps_done", C.c_uint64), ("snps_total", C.c_uint64),
+                ("chunk_wall_ms", C.c_double)]
+
+
+PROGRESS_FN = C.CFUNCTYPE(None, C.POINTER(Progress), C.c_void_p)
+
+
+class Perf(C.Structure):
+    _fields_ = [("m", C.c_uint64), ("n_indiv", C.c_uint64), ("bed_read_secs", C.c_double),
+                ("norm_secs", C.c_double), ("sketch_secs", C.c_double),
+                ("bb_dot_secs", C.c_double), ("ab_dot_secs", C.c_double),
+                ("ring_store_secs", C.c_double), ("n_pairs", C.c_uint64),
+                ("n_tiles", C.c_uint64), ("kernel_launches", C.c_uint32),
+                ("gram_kind", C.c_uint32), ("device_ms", C.c_double)]
+
+
+class L2Args(C.Structure):
+    _fields_ = [
+        ("n_snp", C.c_uint64), ("bed_idx", C.c_void_p), ("chr", C.c_void_p), ("cm", C.c_void_p),
+        ("bp", C.c_void_p), ("window_mode", C.c_int32), ("window_size", C.c_double),
+        ("window_snps", C.c_uint64), ("chunk_size", C.c_uint32), ("global_pass", C.c_int32),
+        ("snp_level_masking", C.c_int32), ("precision", C.c_int32), ("use_f32", C.c_int32),
+        ("sketch_d", C.c_uint32), ("sketch_maf_aware", C.c_int32), ("keep_iids", C.c_void_p),
+        ("n_keep", C.c_uint64), ("annot", C.c_void_p), ("n_annot", C.c_uint32),
+        ("has_pq_exp", C.c_int32), ("pq_exp", C.c_double), ("yes_really", C.c_int32),
+        ("on_progress", PROGRESS_FN), ("progress_user", C.c_void_p),
+    ]
+
+
+class SynthSpec(C.Structure):
+    _fields_ = [("n_indiv", C.c_uint64), ("n_snp", C.c_uint64), ("founders", C.c_uint32),
+                ("switch_p", C.c_double), ("miss", C.c_double), ("seed", C.c_uint64)]
+
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "ldsc_abi_version": (C.c_int, []),
+    "ldsc_ctx_create": (C.c_int, [C.c_int, C.c_uint32, C.POINTER(C.c_void_p)]),
+    "ldsc_ctx_destroy": (C.c_int, [C.c_void_p]),
+    "ldsc_ctx_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "ldsc_last_error": (C.c_int, [C.c_void_p, C.c_char_p, C.c_size_t]),
+    "ldsc_ctx_kernel_count": (C.c_uint64, [C.c_void_p]),
+    "ldsc_bed_validate": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint64, C.c_char_p,
+                                    C.c_size_t]),
+    "ldsc_panel_upload": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint64,
+                                    C.POINTER(C.c_void_p)]),
+    "ldsc_panel_synth": (C.c_int, [C.c_void_p, C.POINTER(SynthSpec), C.POINTER(C.c_void_p)]),
+    "ldsc_panel_download": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64, C.c_void_p]),
+    "ldsc_panel_destroy": (C.c_int, [C.c_void_p]),
+    "ldsc_l2_run": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(L2Args), C.c_void_p, C.c_void_p,
+                              C.POINTER(Perf)]),
+    "ldsc_l2_from_bed": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64,
+                                   C.POINTER(L2Args), C.c_void_p, C.c_void_p, C.POINTER(Perf)]),
+    "ldsc_l2_pair_count": (C.c_int, [C.POINTER(L2Args), C.POINTER(C.c_uint64)]),
+    "ldsc_l2_left_limits": (C.c_int, [C.POINTER(L2Args), C.c_void_p]),
+    "ldsc_countsketch_hash": (C.c_int, [C.c_uint64, C.c_uint32, C.c_uint64, C.c_void_p,
+                                        C.c_void_p]),
+    "ldsc_sketch_project": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64, C.c_void_p,
+                                      C.c_uint64, C.c_void_p, C.c_void_p, C.c_uint32,
+                                      C.c_void_p]),
+    "ldsc_debug_gram_i8_tile": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64,
+                                          C.c_void_p]),
+}
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Load libldsc_b200.so; raise if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python -m ldsc_b200.build` "
+                "(there is no CPU fallback)")
+        lib = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib

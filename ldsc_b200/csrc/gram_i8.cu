@@ -1,0 +1,362 @@
+// gram_i8.cu -- INT8-exact band Gram on the 5th-generation tensor cores.
+//
+// Operands: for record r, row 2r holds its genotypes G (0/1/2, 0 at missing)
+// and row 2r+1 its non-missing mask M (0/1), one byte per individual, rows of
+// `ld` bytes (a multiple of 128).  One UMMA tile multiplies 128 A rows
+// (64 left records k) by 256 B rows (128 right records j) over K = individuals
+// with INT32 accumulation in TMEM, which yields for every record pair the
+// four integer products
+//     GG = sum G_k G_j,  GM = sum G_k M_j,  MG = sum M_k G_j,  MM = sum M_k M_j.
+// With n, s, q the per-record non-missing count, genotype sum and sum of
+// squares, the reference's standardised dot product (normalize.rs:71-110
+// followed by the A^T B GEMM, compute.rs:1897-2236) is recovered exactly:
+//     X   = n_k n_j GG - n_k s_j GM - s_k n_j MG + s_k s_j MM   (int64, exact)
+//     r   = X / sqrt(n_k V_k n_j V_j),  V = n q - s^2            (f64)
+//     r2u = r^2 (1 + 1/(N-2)) - 1/(N-2)                           (f64)
+// N cancels from r; a monomorphic record (V = 0) gives r = 0 and
+// r2u = -1/(N-2), as the reference's zero inv_std does.
+//
+// Kernel structure (persistent, one CTA per SM, 6 warps):
+//   warp 0     TMA producer: A 128x128 B + B 256x128 B per stage, 128-byte swizzle
+//   warp 1     TMEM allocator (512 columns = two 256-column accumulators) and
+//              UMMA issuer (tcgen05.mma kind::i8, M=128 N=256 K=32, four per stage)
+//   warps 2-5  epilogue: tcgen05.ld of the accumulator, exact r^2, band mask,
+//              l2 accumulation; accumulator double-buffering overlaps the
+//              epilogue of tile t with the MMAs of tile t+1.
+// Every mbarrier wait is bounded; on timeout the kernel records an error word,
+// drains its own in-flight copies / MMAs (bounded), frees TMEM and returns.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include "engine.h"
+#include "epilogue.cuh"
+#include "sm100.cuh"
+
+namespace ldsc {
+
+namespace {
+
+constexpr int TA = 64;             // left records per tile (A rows = 128)
+constexpr int TB = 128;            // right records per tile (B rows = 256)
+constexpr int A_BYTES = 128 * 128; // one stage of A
+constexpr int B_BYTES = 256 * 128; // one stage of B
+constexpr int NTHREADS = 192;
+constexpr int RLD = TB + 1;
+constexpr uint64_t WAIT_LIMIT_NS = 2000000000ull;  // 2 s per wait
+
+__device__ __forceinline__ int64_t shfl_xor_i64(int64_t v, int mask) {
+    int lo = (int)(v & 0xFFFFFFFF), hi = (int)(v >> 32);
+    lo = __shfl_xor_sync(0xFFFFFFFFu, lo, mask);
+    hi = __shfl_xor_sync(0xFFFFFFFFu, hi, mask);
+    return ((int64_t)hi << 32) | (uint32_t)lo;
+}
+
+template <int STAGES>
+__global__ void __launch_bounds__(NTHREADS, 1)
+    k_gram_i8(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+              int num_kb, const Tile* __restrict__ tiles, int64_t n_tiles, EpilogueArgs ep,
+              int32_t* __restrict__ dbg) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    const uint32_t pad = (1024u - (smem_u32(smem_raw) & 1023u)) & 1023u;
+    uint8_t* smem = smem_raw + pad;
+    uint8_t* sA = smem;
+    uint8_t* sB = sA + STAGES * A_BYTES;
+    uint64_t* full = reinterpret_cast<uint64_t*>(sB + STAGES * B_BYTES);
+    uint64_t* empty = full + STAGES;
+    uint64_t* tfull = empty + STAGES;   // [2]
+    uint64_t* tempty = tfull + 2;       // [2]
+    uint64_t* drain = tempty + 2;       // [1]
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+    double* cpart = reinterpret_cast<double*>(drain + 2);  // [4][TB]
+    float* Rs = reinterpret_cast<float*>(cpart + 4 * TB);  // [TA][RLD], K > 1 only
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; b++) {
+            mbar_init(&tfull[b], 1);
+            mbar_init(&tempty[b], 128);
+        }
+        mbar_init(drain, 1);
+        fence_mbar_init();
+    }
+    if (warp == 1) {
+        tmem_alloc(tmem_slot, 512);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+
+    if (warp == 0) {
+        // ------------------------------------------------ TMA producer
+        if (elect_one_sync()) {
+            tma_prefetch_desc(&tmA);
+            tma_prefetch_desc(&tmB);
+            int stage = 0;
+            uint32_t phase = 0;
+            bool ok = true;
+            uint32_t armed = 0;        // bit s: stage s has a load in flight we may need to drain
+            uint32_t armed_par = 0;    // bit s: parity of that load's phase
+            for (int64_t t = blockIdx.x; t < n_tiles && ok; t += gridDim.x) {
+                const Tile tl = tiles[t];
+                const int32_t ya = (int32_t)tl.a_blk * (2 * TA);
+                const int32_t yb = (int32_t)tl.b_blk * (2 * TB);
+                for (int kb = 0; kb < num_kb; kb++) {
+                    if (!mbar_wait(&empty[stage], phase ^ 1, WAIT_LIMIT_NS)) {
+                        ok = false;
+                        break;
+                    }
+                    mbar_arrive_expect_tx(&full[stage], A_BYTES + B_BYTES);
+                    tma_load_2d(sA + stage * A_BYTES, &tmA, &full[stage], kb * 128, ya);
+                    tma_load_2d(sB + stage * B_BYTES, &tmB, &full[stage], kb * 128, yb);
+                    armed |= 1u << stage;
+                    armed_par = (armed_par & ~(1u << stage)) | (phase << stage);
+                    if (++stage == STAGES) {
+                        stage = 0;
+                        phase ^= 1;
+                    }
+                }
+            }
+            if (!ok) {
+                atomicOr(ep.err, 1u);
+                // our copies in flight must land before the CTA's smem is released
+                for (int s = 0; s < STAGES; s++)
+                    if (armed & (1u << s)) mbar_wait(&full[s], (armed_par >> s) & 1u, WAIT_LIMIT_NS);
+            }
+        }
+    } else if (warp == 1) {
+        // ------------------------------------------------ UMMA issuer
+        if (elect_one_sync()) {
+            const uint32_t idesc = idesc_i8(128, 256);
+            int stage = 0;
+            uint32_t phase = 0;
+            int acc = 0;
+            uint32_t aphase = 0;
+            bool ok = true;
+            bool issued = false;
+            for (int64_t t = blockIdx.x; t < n_tiles && ok; t += gridDim.x) {
+                if (!mbar_wait(&tempty[acc], aphase ^ 1, WAIT_LIMIT_NS)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t d_tmem = tmem_base + (uint32_t)acc * 256u;
+                for (int kb = 0; kb < num_kb; kb++) {
+                    if (!mbar_wait(&full[stage], phase, WAIT_LIMIT_NS)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t a_addr = smem_u32(sA + stage * A_BYTES);
+                    const uint32_t b_addr = smem_u32(sB + stage * B_BYTES);
+#pragma unroll
+                    for (int kk = 0; kk < 4; kk++) {
+                        umma_i8(d_tmem, sdesc_k_sw128(a_addr + kk * 32), sdesc_k_sw128(b_addr + kk * 32),
+                                idesc, (kb | kk) != 0 ? 1u : 0u);
+                    }
+                    issued = true;
+                    umma_commit(&empty[stage]);
+                    if (++stage == STAGES) {
+                        stage = 0;
+                        phase ^= 1;
+                    }
+                }
+                if (!ok) break;
+                umma_commit(&tfull[acc]);
+                if (++acc == 2) {
+                    acc = 0;
+                    aphase ^= 1;
+                }
+            }
+            if (!ok) atomicOr(ep.err, 2u);
+            if (issued) {
+                // all of this thread's MMAs complete before TMEM is freed
+                umma_commit(drain);
+                mbar_wait(drain, 0, WAIT_LIMIT_NS);
+            }
+        }
+    } else {
+        // ------------------------------------------------ epilogue (128 threads)
+        const int et = threadIdx.x - 64;         // 0..127
+        const int ew = et >> 5;                  // epilogue warp 0..3
+        const int quarter = warp & 3;            // TMEM lanes this warp may access
+        const int row = quarter * 32 + lane;     // accumulator row = A row
+        const bool grow = (row & 1) == 0;        // genotype row (else mask row)
+        const int64_t m = ep.m;
+        int acc = 0;
+        uint32_t aphase = 0;
+        for (int64_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+            const Tile tl = tiles[t];
+            const int64_t k0 = (int64_t)tl.a_blk * TA, j0 = (int64_t)tl.b_blk * TB;
+            const int64_t k = k0 + (row >> 1);
+            const bool kval = k < m;
+            const int64_t nk = kval ? __ldg(ep.n + k) : 0;
+            const int64_t sk = kval ? __ldg(ep.s + k) : 0;
+            const double qk = kval ? __ldg(ep.qinv + k) : 0.0;
+            const double ak = (kval && ep.K == 1) ? __ldg(ep.aeff + k) : 0.0;
+
+            // One thread does the bounded wait; the decision is made uniform for
+            // all 128 epilogue threads through shared memory before anyone
+            // continues, so no thread can be left waiting at a named barrier.
+            volatile uint32_t* go = tmem_slot + 1;
+            if (et == 0) *go = mbar_wait(&tfull[acc], aphase, WAIT_LIMIT_NS) ? 1u : 0u;
+            named_bar_sync(2, 128);
+            if (*go == 0u) {
+                if (et == 0) atomicOr(ep.err, 4u);
+                break;
+            }
+            tc_fence_after();
+            double rsum = 0.0;
+            for (int c = 0; c < 4; c++) {
+                uint32_t v[64];
+                tmem_ld_32x32b_x64(tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)acc * 256u +
+                                       (uint32_t)c * 64u,
+                                   v);
+                tmem_ld_wait();
+                if (c == 3) {
+                    // accumulator fully read: hand it back to the MMA warp
+                    tc_fence_before();
+                    mbar_arrive(&tempty[acc]);
+                }
+                if (dbg != nullptr && t == 0) {
+#pragma unroll
+                    for (int q = 0; q < 64; q++) dbg[row * 256 + c * 64 + q] = (int32_t)v[q];
+                }
+#pragma unroll
+                for (int p = 0; p < 32; p += 2) {
+                    const int64_t ja = j0 + c * 32 + p, jb = ja + 1;
+                    const int64_t nja = ja < m ? __ldg(ep.n + ja) : 0, sja = ja < m ? __ldg(ep.s + ja) : 0;
+                    const int64_t njb = jb < m ? __ldg(ep.n + jb) : 0, sjb = jb < m ? __ldg(ep.s + jb) : 0;
+                    const int64_t ga = (int32_t)v[2 * p], ma = (int32_t)v[2 * p + 1];
+                    const int64_t gb = (int32_t)v[2 * p + 2], mb = (int32_t)v[2 * p + 3];
+                    int64_t Pa, Pb;
+                    if (grow) {
+                        Pa = nk * (nja * ga - sja * ma);   // n_k n_j GG - n_k s_j GM
+                        Pb = nk * (njb * gb - sjb * mb);
+                    } else {
+                        Pa = sk * (sja * ma - nja * ga);   // s_k s_j MM - s_k n_j MG
+                        Pb = sk * (sjb * mb - njb * gb);
+                    }
+                    const int64_t send = grow ? Pb : Pa;
+                    const int64_t recv = shfl_xor_i64(send, 1);
+                    const int64_t X = (grow ? Pa : Pb) + recv;
+                    const int64_t j = grow ? ja : jb;
+                    double r2u = 0.0;
+                    const bool valid = kval && pair_in_band(k, j, m, ep.left);
+                    if (valid) {
+                        const double r = (double)X * qk * __ldg(ep.qinv + j);
+                        r2u = r * r * ep.r2u_a + ep.r2u_b;
+                    }
+                    if (ep.K == 1) {
+                        if (valid) rsum += r2u * __ldg(ep.aeff + j);
+                        // column j: sum over the 16 same-parity lanes of this warp
+                        double cv = r2u * ak;
+                        cv += __shfl_xor_sync(0xFFFFFFFFu, cv, 2);
+                        cv += __shfl_xor_sync(0xFFFFFFFFu, cv, 4);
+                        cv += __shfl_xor_sync(0xFFFFFFFFu, cv, 8);
+                        cv += __shfl_xor_sync(0xFFFFFFFFu, cv, 16);
+                        if (lane < 2) cpart[ew * TB + c * 32 + p + lane] = cv;
+                    } else {
+                        Rs[(row >> 1) * RLD + c * 32 + p + (grow ? 0 : 1)] = (float)r2u;
+                    }
+                }
+            }
+            if (ep.K == 1) {
+                rsum += __shfl_xor_sync(0xFFFFFFFFu, rsum, 1);
+                if (grow && kval && rsum != 0.0) atomicAdd(ep.l2 + k, rsum);
+                named_bar_sync(1, 128);
+                const int64_t j = j0 + et;
+                const double cs = cpart[et] + cpart[TB + et] + cpart[2 * TB + et] + cpart[3 * TB + et];
+                if (j < m && cs != 0.0) atomicAdd(ep.l2 + j, cs);
+                named_bar_sync(1, 128);
+            } else {
+                named_bar_sync(1, 128);
+                contract_tile_smem(Rs, RLD, TA, TB, k0, j0, ep, et, 128);
+                named_bar_sync(1, 128);
+            }
+            if (++acc == 2) {
+                acc = 0;
+                aphase ^= 1;
+            }
+        }
+    }
+
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 1) tmem_dealloc(tmem_base, 512);
+}
+
+}  // namespace
+
+using PFN_encodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                     const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                     const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                     CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static PFN_encodeTiled get_encode() {
+    static PFN_encodeTiled fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_encodeTiled>(p);
+    }
+    return fn;
+}
+
+static bool make_map(CUtensorMap* map, const uint8_t* base, uint64_t ld, uint64_t rows,
+                     uint32_t box_rows) {
+    PFN_encodeTiled enc = get_encode();
+    if (!enc) return false;
+    cuuint64_t dims[2] = {ld, rows};
+    cuuint64_t strides[1] = {ld};
+    cuuint32_t box[2] = {128, box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<uint8_t*>(base), dims, strides,
+                     box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+cudaError_t launch_gram_i8(const uint8_t* ops, uint64_t ld, int64_t m, const Tile* tiles,
+                           int64_t n_tiles, const EpilogueArgs& ep, int32_t* dbg, int sms,
+                           cudaStream_t stream) {
+    if (n_tiles <= 0) return cudaSuccess;
+    if (ld % 128 != 0 || (reinterpret_cast<uintptr_t>(ops) & 15) != 0) return cudaErrorInvalidValue;
+    CUtensorMap tmA, tmB;
+    const uint64_t rows = (uint64_t)(2 * m);
+    if (!make_map(&tmA, ops, ld, rows, 2 * TA) || !make_map(&tmB, ops, ld, rows, 2 * TB))
+        return cudaErrorInvalidValue;
+    const int num_kb = (int)(ld / 128);
+    const size_t ctrl = 8 * (2 * 4 + 2 + 2 + 1 + 1);  // barriers + tmem slot (upper bound)
+    const size_t cbytes = sizeof(double) * 4 * TB;
+    int64_t grid = n_tiles < sms ? n_tiles : sms;
+    if (dbg) grid = 1;
+    if (ep.K == 1) {
+        const size_t smem = 1024 + 4 * (size_t)(A_BYTES + B_BYTES) + ctrl + cbytes;
+        cudaError_t e = cudaFuncSetAttribute(k_gram_i8<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+        k_gram_i8<4><<<(unsigned)grid, NTHREADS, smem, stream>>>(tmA, tmB, num_kb, tiles,
+                                                                 dbg ? 1 : n_tiles, ep, dbg);
+    } else {
+        const size_t smem = 1024 + 3 * (size_t)(A_BYTES + B_BYTES) + ctrl + cbytes +
+                            sizeof(float) * TA * RLD;
+        cudaError_t e = cudaFuncSetAttribute(k_gram_i8<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+        k_gram_i8<3><<<(unsigned)grid, NTHREADS, smem, stream>>>(tmA, tmB, num_kb, tiles,
+                                                                 dbg ? 1 : n_tiles, ep, dbg);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace ldsc

@@ -1,0 +1,232 @@
+"""GPU parity of the l2 engine against the CPU oracle (through the C ABI)."""
+import os
+
+import numpy as np
+import pytest
+
+from ldsc_b200 import synth
+from ldsc_b200.plink import BimTable
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+# exact modes: max |l2 - oracle| / max(|oracle|, 1) (FP64 reorders sums; INT8 is exact up to rounding)
+EXACT_TOL = 1e-9
+# K > 1 contracts r2u tiles in f32: relative to the column's scale
+ANNOT_TOL = 2e-6
+
+
+def table(chr_, cm, bp):
+    m = len(chr_)
+    return BimTable(np.asarray(chr_, np.uint8), [f"rs{i}" for i in range(m)], np.asarray(cm, float),
+                    np.asarray(bp, np.uint32), np.arange(m, dtype=np.int64))
+
+
+def relerr(a, b):
+    return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1.0)))
+
+
+@pytest.fixture(scope="module")
+def small():
+    z = np.load(os.path.join(GOLDEN, "small_panel.npz"))
+    return z
+
+
+@pytest.fixture(scope="module")
+def small_panel(ctx, small):
+    return ctx.upload(small["body"], int(small["n_indiv"]))
+
+
+def run_mode(ctx, small, panel, name, precision):
+    from golden.make_golden import MODES, annot3
+    from ldsc_b200.api import WindowMode, run_l2
+    mode, wind, chunk, masking, per_chr, f32, sk, has_annot, pq = MODES[name]
+    wm = {"cm": WindowMode.Cm, "kb": WindowMode.Kb, "snp": WindowMode.Snp}[mode](wind)
+    snps = table(small["chr"], small["cm"], small["bp"])
+    A = annot3(len(snps)) if has_annot else None
+    return run_l2(ctx, snps, panel, wm, chunk, annot=A, pq_exp=pq, use_f32=f32, sketch=sk or None,
+                  snp_level_masking=masking, global_pass=not per_chr, precision=precision,
+                  yes_really=True)
+
+
+def test_micro_known_answer_from_bytes(ctx):
+    """src/l2/mod.rs:1191-1225 through the whole-file entry point."""
+    from ldsc_b200.api import L2Config, WindowMode, compute_l2_from_bytes
+    bim = "1\trs1\t0\t100\tA\tG\n1\trs2\t0\t200\tA\tG\n"
+    fam = "".join(f"F{i}\tI{i}\t0\t0\t1\t-9\n" for i in range(1, 5))
+    bed = bytes([0x6C, 0x1B, 0x01, 0xF0, 0xF0])
+    for prec in ("fp64", "int8"):
+        out = compute_l2_from_bytes(bed, bim, fam, L2Config(mode=WindowMode.Kb(100.0), chunk_size=2,
+                                                            precision=prec), ctx=ctx)
+        np.testing.assert_allclose(out.l2, [2.0, 2.0], atol=1e-9)
+        np.testing.assert_allclose(out.maf, [0.5, 0.5], atol=1e-9)
+
+
+def test_truncated_bed_is_rejected(ctx):
+    from ldsc_b200.api import L2Config, LdscError, compute_l2_from_bytes
+    bim = "1\trs1\t0\t100\tA\tG\n1\trs2\t0\t200\tA\tG\n"
+    fam = "".join(f"F{i}\tI{i}\t0\t0\t1\t-9\n" for i in range(1, 5))
+    with pytest.raises(LdscError, match="invalid length"):
+        compute_l2_from_bytes(bytes([0x6C, 0x1B, 0x01, 0xF0]), bim, fam, L2Config(), ctx=ctx)
+
+
+EXACT_MODES = ["cm1_chunk50", "cm1_masked", "cm1_global", "kb500_chunk40", "snp25_masked",
+               "cm1_perallele"]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "int8"])
+@pytest.mark.parametrize("name", EXACT_MODES)
+def test_exact_modes_match_oracle(ctx, small, small_panel, name, precision):
+    l2, maf, perf = run_mode(ctx, small, small_panel, name, precision)
+    assert relerr(l2, small[f"l2_{name}"]) < EXACT_TOL
+    np.testing.assert_allclose(maf, small[f"maf_{name}"], atol=1e-15)
+    assert perf.n_pairs == int(small[f"pairs_{name}"])
+
+
+@pytest.mark.parametrize("precision", ["fp64", "int8"])
+def test_annotations_match_oracle(ctx, small, small_panel, precision):
+    l2, _, _ = run_mode(ctx, small, small_panel, "cm1_annot3", precision)
+    ref = small["l2_cm1_annot3"]
+    scale = np.maximum(np.abs(ref).max(axis=0, keepdims=True), 1.0)
+    assert np.max(np.abs(l2 - ref) / scale) < ANNOT_TOL
+
+
+def test_fast_f32_flag_within_reference_tolerance(ctx, small, small_panel):
+    """--fast-f32 is accepted; the GPU keeps exact arithmetic, which agrees
+    with the reference's f32 output within its 2e-2 parity tolerance."""
+    l2, _, _ = run_mode(ctx, small, small_panel, "cm1_f32", "int8")
+    assert np.max(np.abs(l2 - small["l2_cm1_f32"])) < 2e-2
+    assert relerr(l2, small["l2_cm1_chunk50"]) < EXACT_TOL
+
+
+def test_sketch_matches_oracle(ctx, small, small_panel):
+    """CountSketch d = 50, seed-42 stream.  The sketched columns differ from
+    the reference's f32 scatter only by its accumulation rounding."""
+    l2, maf, _ = run_mode(ctx, small, small_panel, "cm1_sketch50", "fp64")
+    ref = small["l2_cm1_sketch50"]
+    assert np.max(np.abs(l2 - ref)) < 1e-3 * max(1.0, np.abs(ref).max())
+    np.testing.assert_allclose(maf, small["maf_cm1_sketch50"], atol=1e-15)
+
+
+def test_keep_subset_matches_oracle(ctx, small, small_panel):
+    from ldsc_b200.api import WindowMode, run_l2
+    from oracle import OracleL2Args, oracle_l2
+    n = int(small["n_indiv"])
+    keep = np.arange(3, n, 2, dtype=np.int64)
+    snps = table(small["chr"], small["cm"], small["bp"])
+    ref, ref_maf, _, _ = oracle_l2(OracleL2Args(bed_body=small["body"], n_file_indiv=n, chr=small["chr"],
+                                                cm=small["cm"], bp=small["bp"], chunk_c=50, iid_idx=keep))
+    for prec in ("fp64", "int8"):
+        l2, maf, _ = run_l2(ctx, snps, small_panel, WindowMode.Cm(1.0), 50, iid_indices=keep,
+                            precision=prec, yes_really=True)
+        assert relerr(l2, ref) < EXACT_TOL
+        np.testing.assert_allclose(maf, ref_maf, atol=1e-15)
+
+
+def test_extract_subset_matches_oracle(ctx, small, small_panel):
+    """Non-contiguous SNP records (--extract with gaps)."""
+    from ldsc_b200.api import WindowMode, run_l2
+    from oracle import OracleL2Args, oracle_l2
+    n = int(small["n_indiv"])
+    rows = np.sort(np.random.default_rng(3).choice(len(small["chr"]), 900, replace=False))
+    snps = table(small["chr"][rows], small["cm"][rows], small["bp"][rows])
+    snps.bed_idx = rows.astype(np.int64)
+    ref, _, _, _ = oracle_l2(OracleL2Args(bed_body=small["body"], n_file_indiv=n, chr=small["chr"][rows],
+                                          cm=small["cm"][rows], bp=small["bp"][rows], bed_idx=rows,
+                                          chunk_c=50, masking=True))
+    for prec in ("fp64", "int8"):
+        l2, _, _ = run_l2(ctx, snps, small_panel, WindowMode.Cm(1.0), 50, snp_level_masking=True,
+                          precision=prec, yes_really=True)
+        assert relerr(l2, ref) < EXACT_TOL
+
+
+def test_int8_gram_tile_is_bit_exact(ctx):
+    """Raw INT32 accumulators of one tcgen05 tile vs an integer recompute."""
+    from ldsc_b200.api import debug_gram_i8_tile
+    from ldsc_b200.plink import decode_genotypes
+    spec = synth.PanelSpec(n_indiv=777, chrom_sizes=[300], chrom_cm=[3.0], founders=9, miss=0.05, seed=5)
+    body = synth.bed_body(spec)
+    panel = ctx.upload(body, spec.n_indiv)
+    G = decode_genotypes(body, spec.n_indiv)
+    Gi = np.where(np.isnan(G), 0, G).astype(np.int64)
+    Mi = (~np.isnan(G)).astype(np.int64)
+    for k0, j0 in [(0, 0), (64, 128), (192, 128), (256, 256)]:
+        D = debug_gram_i8_tile(ctx, panel, k0, j0).astype(np.int64)
+        A = np.zeros((128, spec.n_indiv), np.int64)
+        B = np.zeros((256, spec.n_indiv), np.int64)
+        for r in range(64):
+            if k0 + r < spec.m:
+                A[2 * r], A[2 * r + 1] = Gi[k0 + r], Mi[k0 + r]
+        for r in range(128):
+            if j0 + r < spec.m:
+                B[2 * r], B[2 * r + 1] = Gi[j0 + r], Mi[j0 + r]
+        assert np.array_equal(D, A @ B.T), (k0, j0)
+
+
+def test_device_synth_matches_numpy(ctx):
+    spec = synth.PanelSpec(n_indiv=1001, chrom_sizes=[2500], chrom_cm=[10.0], founders=40, miss=0.01, seed=9)
+    panel = ctx.synth(spec.n_indiv, spec.m, spec.founders, spec.switch_p, spec.miss, spec.seed)
+    assert np.array_equal(panel.download(), synth.bed_body(spec))
+
+
+def test_sketch_project_matches_reference_scatter(ctx):
+    """Port of scatter_one_column_f32_matches_ref_all_iids (src/wasm_simd.rs:2918-2998)."""
+    from ldsc_b200.api import sketch_project
+    from test_oracle import direct_scatter_f32, lcg_bed_fixture, lcg_bucket_sign, snp_mean_inv
+    c, n, d = 8, 503, 50
+    raw = lcg_bed_fixture(42, c, n)
+    bpr = (n + 3) // 4
+    bucket, sign = lcg_bucket_sign(n, d, 7)
+    panel = ctx.upload(raw, n)
+    got = sketch_project(ctx, panel, 0, c, bucket, sign, d)
+    for j in range(c):
+        g, mean, inv = snp_mean_inv(raw, bpr, j, n)
+        exp = direct_scatter_f32(g, bucket, sign, mean, inv, float(n), d)
+        diff = np.abs(got[j] - exp)
+        assert np.all((diff < 1e-4) | (diff / np.maximum(np.abs(exp), 1e-6) < 1e-4))
+    # full keep list == all individuals, bit for bit
+    sub = sketch_project(ctx, panel, 0, c, bucket, sign, d, keep=np.arange(n))
+    assert np.array_equal(sub, got)
+
+
+def test_argument_errors(ctx, small, small_panel):
+    from ldsc_b200.api import LdscError, WindowMode, run_l2
+    snps = table(small["chr"], small["cm"], small["bp"])
+    with pytest.raises(LdscError, match="chunk_size must be >= 1"):
+        run_l2(ctx, snps, small_panel, WindowMode.Cm(1.0), 0)
+    with pytest.raises(LdscError, match="out of bounds"):
+        run_l2(ctx, snps, small_panel, WindowMode.Cm(1.0), 50, sketch=2)
+    with pytest.raises(LdscError, match="Annotation matrix has"):
+        run_l2(ctx, snps, small_panel, WindowMode.Cm(1.0), 50, annot=np.ones((5, 2)))
+    # the context stays usable after errors
+    l2, _, _ = run_mode(ctx, small, small_panel, "cm1_masked", "int8")
+    assert relerr(l2, small["l2_cm1_masked"]) < EXACT_TOL
+
+
+@pytest.fixture(scope="module")
+def cfg_small():
+    spec = synth.spec_small()
+    body = synth.bed_body(spec)
+    chr_, cm, bp = synth.positions(spec)
+    return spec, body, chr_, cm, bp
+
+
+@pytest.mark.parametrize("masking", [False, True])
+def test_small_config_parity(ctx, cfg_small, masking):
+    """N = 2,490 x M = 18,627, 1 cM, chunk 200: both exact forms within
+    1e-6 relative of the f64 oracle (the bar), in practice ~1e-12."""
+    from ldsc_b200.api import WindowMode, run_l2
+    from oracle import OracleL2Args, oracle_l2
+    spec, body, chr_, cm, bp = cfg_small
+    ref, ref_maf, npairs, _ = oracle_l2(OracleL2Args(bed_body=body, n_file_indiv=spec.n_indiv, chr=chr_,
+                                                     cm=cm, bp=bp, chunk_c=200, masking=masking))
+    panel = ctx.upload(body, spec.n_indiv)
+    snps = table(chr_, cm, bp)
+    for prec in ("fp64", "int8"):
+        l2, maf, perf = run_l2(ctx, snps, panel, WindowMode.Cm(1.0), 200, snp_level_masking=masking,
+                               precision=prec, yes_really=True)
+        err = float(np.max(np.abs(l2 - ref) / np.abs(ref)))
+        assert err < 1e-6, (prec, err)
+        assert relerr(l2, ref) < EXACT_TOL
+        assert perf.n_pairs == npairs
+        np.testing.assert_allclose(maf, ref_maf, atol=1e-15)
