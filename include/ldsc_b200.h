@@ -208,6 +208,37 @@ int ldsc_sketch_project(ldsc_ctx *ctx, const ldsc_panel *panel, uint64_t snp_beg
                         uint64_t snp_end, const int64_t *keep_iids, uint64_t n_keep,
                         const uint32_t *bucket, const float *sign, uint32_t d, float *out);
 
+/* ---- allocation-free entry point ---------------------------------------- */
+
+/* No counterpart in the reference: this entry point exists for callers that
+ * cannot allocate device memory -- a host that owns all device memory through
+ * its own arena, code that runs while a stream is being captured into a CUDA
+ * graph (cudaMalloc cannot be captured), or a latency-critical request loop in
+ * which an allocation would synchronise the device.
+ *
+ * It runs the INT8-exact l2 pass (all-ones annotation, K = 1) on device
+ * buffers the caller owns and allocates nothing: all scratch lives in one
+ * static device array of LDSC_NOALLOC_SCRATCH_BYTES bytes inside the library,
+ * which every GPU that loads the library holds until the process exits.
+ *   d_rows   device BED rows, n_snp rows of `pitch` bytes (pitch a multiple of
+ *            16, >= ceil(n_indiv/4); 16-byte aligned)
+ *   left     HOST array of n_snp window limits (ldsc_l2_left_limits)
+ *   d_l2     device output, n_snp doubles;  d_maf  device output, n_snp doubles
+ *   stream   cudaStream_t to run on (NULL = the legacy default stream)
+ * Requests whose scratch (about 2 * n_snp * round_up(n_indiv, 128) bytes plus
+ * 48 bytes per SNP) exceeds the array are rejected with LDSC_E_INVALID.  All
+ * calls share the array, which keeps the last call's contents; calls that
+ * overlap on the GPU race.  The first call on a device looks up the array's
+ * address and should come before any stream capture.  The call waits for its
+ * own work before returning.  Messages: ldsc_noalloc_last_error(). */
+#define LDSC_NOALLOC_SCRATCH_BYTES (64u * 1024u * 1024u)
+
+int ldsc_l2_int8_noalloc(const uint8_t *d_rows, uint64_t pitch, uint64_t n_indiv, uint64_t n_snp,
+                         const int64_t *left, double *d_l2, double *d_maf, void *stream);
+
+/* Last error message of ldsc_l2_int8_noalloc (process-wide). */
+int ldsc_noalloc_last_error(char *buf, size_t len);
+
 /* ---- diagnostics ------------------------------------------------------- */
 
 /* Raw INT32 accumulators of the INT8 tcgen05 Gram for one tile: A side =

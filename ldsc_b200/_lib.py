@@ -97,7 +97,12 @@ SIGNATURES = {
                                       C.c_void_p]),
     "ldsc_debug_gram_i8_tile": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64,
                                           C.c_void_p]),
+    "ldsc_l2_int8_noalloc": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p,
+                                       C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ldsc_noalloc_last_error": (C.c_int, [C.c_char_p, C.c_size_t]),
 }
+
+NOALLOC_SCRATCH_BYTES = 64 * 1024 * 1024
 
 _lib = None
 
