@@ -168,6 +168,116 @@ def run_reference(args):
     print(json.dumps(out))
 
 
+def _timed_passes(ctx, stream, fn, warmup, steps):
+    """Run fn() warmup times, then time `steps` calls on the stream (CUDA events)."""
+    import torch
+    outs = []
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        outs.append(fn())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / 1e3, outs
+
+
+def run_sketch_workload(args, ctx, stream):
+    """Fused CountSketch l2: N=100,000 x M=200,000 (1% missing, 150 cM),
+    --sketch d --snp-level-masking, 1 cM.  Prints one JSON line per d with
+    the sketch pass rate, the scatter kernel's HBM roofline, and the error of
+    the sketched l2 against exact l2 (INT8 form) on the same panel."""
+    from ldsc_b200 import synth
+    from ldsc_b200.api import WindowMode, pair_count, run_l2
+    from ldsc_b200.plink import BimTable
+    spec = synth.spec_sketch()
+    if args.sketch_snps:
+        spec.chrom_sizes = [args.sketch_snps]
+        spec.chrom_cm = [150.0 * args.sketch_snps / 200000]
+    chr_, cm, bp = synth.positions(spec)
+    m = spec.m
+    snps = BimTable(chr_, [f"rs{i}" for i in range(m)], cm, bp, np.arange(m, dtype=np.int64))
+    panel = ctx.synth(spec.n_indiv, m, spec.founders, spec.switch_p, spec.miss, spec.seed)
+    wm = WindowMode.Cm(1.0)
+    npairs = pair_count(snps, wm, 200, snp_level_masking=True)
+    t_ex, outs = _timed_passes(ctx, stream, lambda: run_l2(ctx, snps, panel, wm, 200, snp_level_masking=True,
+                                                           precision="int8", yes_really=True), 1, 1)
+    exact = outs[0][0][:, 0]
+    hbm, _, src = measured_peaks()
+    for d in [int(x) for x in args.sketch_d.split(",")]:
+        t, outs = _timed_passes(ctx, stream, lambda: run_l2(ctx, snps, panel, wm, 200, snp_level_masking=True,
+                                                            sketch=d, yes_really=True), args.warmup, args.steps)
+        sk = outs[-1][0][:, 0]
+        perf = outs[-1][2]
+        sk_s = float(np.mean([o[2].sketch_secs for o in outs]))
+        gram_s = float(np.mean([o[2].ab_dot_secs for o in outs]))
+        bpr = (spec.n_indiv + 3) // 4
+        alg_bytes = m * bpr + m * d * 4 + spec.n_indiv * 4
+        achieved = alg_bytes / sk_s / 1e9
+        out = {"workload": "sketch", "config": {"n_indiv": spec.n_indiv, "n_snp": m, "sketch_d": d,
+                                                "window": "1 cM", "snp_level_masking": True},
+               "metric": "r2 pairs/sec (sketch form)", "value": npairs * args.steps / t, "unit": "r2 pairs/s",
+               "ms_per_step": 1e3 * t / args.steps, "n_pairs": npairs,
+               "exact_int8_pairs_per_s": npairs / t_ex,
+               "sketch_kernel_ms": 1e3 * sk_s, "sketch_gram_ms": 1e3 * gram_s, "decode_ms": 1e3 * perf.norm_secs,
+               "sketch_roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                                   "frac": achieved / hbm, "algorithmic_bytes": alg_bytes, "peak_source": src},
+               "vs_exact": {"pearson_r": float(np.corrcoef(sk, exact)[0, 1]),
+                            "max_abs_err": float(np.max(np.abs(sk - exact))),
+                            "mean_abs_err": float(np.mean(np.abs(sk - exact))),
+                            "mean_exact_l2": float(np.mean(exact))}}
+        print(json.dumps(out), flush=True)
+    panel.close()
+
+
+def run_partitioned_workload(args, ctx, stream):
+    """Partitioned LD scores: N=10,000, M=500,000 over 22 chromosomes, 97
+    annotations, 1 cM windows, chunk 200 (default mode), all chromosomes in
+    one call.  INT8 and FP64 forms; the last three chromosomes are checked
+    against the C oracle."""
+    from ldsc_b200 import synth
+    from ldsc_b200.api import WindowMode, pair_count, run_l2
+    from ldsc_b200.plink import BimTable
+    from oracle import OracleL2Args, oracle_l2
+    spec = synth.spec_partitioned()
+    chr_, cm, bp = synth.positions(spec)
+    m = spec.m
+    snps = BimTable(chr_, [f"rs{i}" for i in range(m)], cm, bp, np.arange(m, dtype=np.int64))
+    annot = synth.partitioned_annot(m)
+    panel = ctx.synth(spec.n_indiv, m, spec.founders, spec.switch_p, spec.miss, spec.seed)
+    wm = WindowMode.Cm(1.0)
+    npairs = pair_count(snps, wm, 200)
+    res = {}
+    for prec in ("int8", "fp64"):
+        t, outs = _timed_passes(ctx, stream, lambda: run_l2(ctx, snps, panel, wm, 200, annot=annot,
+                                                            precision=prec, yes_really=True),
+                                args.warmup if prec == "int8" else 1, args.steps if prec == "int8" else 2)
+        res[prec] = (t / (args.steps if prec == "int8" else 2), outs[-1])
+    l2i = res["int8"][1][0]
+    l2f = res["fp64"][1][0]
+    # oracle on the three smallest chromosomes (independent in per-chromosome mode)
+    start = int(np.searchsorted(chr_, 20))
+    rows = panel.download(start, m)
+    ref, _, _, _ = oracle_l2(OracleL2Args(bed_body=rows, n_file_indiv=spec.n_indiv, chr=chr_[start:], cm=cm[start:],
+                                          bp=bp[start:], chunk_c=200, annot=annot[start:]))
+    scale = np.maximum(np.abs(ref).max(axis=0, keepdims=True), 1.0)
+    out = {"workload": "partitioned", "config": {"n_indiv": spec.n_indiv, "n_snp": m, "chromosomes": 22,
+                                                 "annotations": annot.shape[1], "window": "1 cM", "chunk_size": 200},
+           "metric": "r2 pairs/sec", "n_pairs": npairs,
+           "int8": {"pairs_per_s": npairs / res["int8"][0], "ms_per_step": 1e3 * res["int8"][0],
+                    "gram_ms": 1e3 * res["int8"][1][2].ab_dot_secs},
+           "fp64": {"pairs_per_s": npairs / res["fp64"][0], "ms_per_step": 1e3 * res["fp64"][0],
+                    "gram_ms": 1e3 * res["fp64"][1][2].ab_dot_secs},
+           "int8_vs_oracle_chr20_22": float(np.max(np.abs(l2i[start:] - ref) / scale)),
+           "fp64_vs_oracle_chr20_22": float(np.max(np.abs(l2f[start:] - ref) / scale)),
+           "int8_vs_fp64_all": float(np.max(np.abs(l2i - l2f) / np.maximum(np.abs(l2f).max(axis=0, keepdims=True), 1.0))),
+           "error_metric": "max |l2_jC - ref_jC| / max(max_j |ref_jC|, 1) per annotation column"}
+    print(json.dumps(out), flush=True)
+    panel.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -177,7 +287,9 @@ def main():
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="biobank", choices=["biobank", "profile"])
+    ap.add_argument("--workload", default="biobank", choices=["biobank", "profile", "sketch", "partitioned"])
+    ap.add_argument("--sketch-d", default="200,1000,5000")
+    ap.add_argument("--sketch-snps", type=int, default=0, help="truncate the sketch panel (profiling)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -212,6 +324,13 @@ def main():
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
 
+    if args.workload == "sketch":
+        run_sketch_workload(args, ctx, stream)
+        return
+    if args.workload == "partitioned":
+        run_partitioned_workload(args, ctx, stream)
+        return
+
     spec = workload_spec(seed_offset=rank, workload=args.workload)
     chr_, cm, bp = synth.positions(spec)
     m = spec.m
@@ -233,10 +352,12 @@ def main():
     k0 = ctx.kernel_count
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
-    gram_s = []
+    gram_s, dec_s, dev_ms = [], [], []
     for _ in range(args.steps):
         _, _, perf = step("int8")
         gram_s.append(perf.ab_dot_secs)
+        dec_s.append(perf.norm_secs)
+        dev_ms.append(perf.device_ms)
     ev1.record(stream)
     torch.cuda.synchronize()
     barrier()
@@ -323,6 +444,8 @@ def main():
                "forms": {"int8_pairs_per_s": value / world, "fp64_pairs_per_s": fp64_value,
                          "int8_over_fp64": (value / world) / fp64_value if fp64_value else None,
                          "int8_gram_ms": 1e3 * gram_avg, "fp64_gram_ms": 1e3 * float(np.mean(fp64_gram)),
+                         "int8_decode_ms": 1e3 * float(np.mean(dec_s)),
+                         "int8_device_ms_per_pass": float(np.mean(dev_ms)),
                          "n_pairs_per_rank": npairs}}
         print(json.dumps(out))
     panel.close()

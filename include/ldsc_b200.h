@@ -208,6 +208,68 @@ int ldsc_sketch_project(ldsc_ctx *ctx, const ldsc_panel *panel, uint64_t snp_beg
                         uint64_t snp_end, const int64_t *keep_iids, uint64_t n_keep,
                         const uint32_t *bucket, const float *sign, uint32_t d, float *out);
 
+/* ---- LD-score regressions (h2 / rg) ------------------------------------ */
+
+/* Batched h2 regressions against one LD-score column (K = 1): weights
+ * (ldsc_weights, src/h2.rs:185-206), two IRWLS re-weightings (irwls_ldsc,
+ * src/h2.rs:435-458) and the block jackknife (jackknife_fast,
+ * src/h2.rs:100-183; jackknife_se_cov, src/jackknife.rs:10-59), as in
+ * run_h2_ldsc / run_hsq_ldsc (src/h2.rs:258-433, src/regressions.rs:1648-1825)
+ * without --two-step.  One regression per trait; all traits share the SNPs,
+ * ref_l2 and w_l2. */
+typedef struct {
+    uint64_t n_snp;
+    uint32_t n_traits;
+    uint32_t n_blocks;            /* --n-blocks (200); must be <= n_snp */
+    const double *chi2;           /* n_traits x n_snp, row-major */
+    const double *n_per_snp;      /* n_traits x n_snp sample sizes, or NULL */
+    const double *n_scalar;       /* n_traits sample sizes (when n_per_snp is NULL) */
+    const double *ref_l2;         /* n_snp LD scores */
+    const double *w_l2;           /* n_snp regression-weight LD scores */
+    double m_snps;                /* M */
+    int32_t fixed_intercept;      /* --intercept-h2 */
+    double intercept;
+    int32_t want_lambda_gc;       /* median(chi2) / 0.4549 (exact order statistics) */
+    int32_t device_pointers;      /* 1: the arrays above are device pointers */
+} ldsc_h2_args;
+
+typedef struct {
+    double h2, h2_se, intercept, intercept_se;
+    double mean_chi2, lambda_gc, ratio, ratio_se;  /* ratio: NaN when mean_chi2 <= 1 or fixed */
+    double coef, coef_se;                          /* slope per unit of N * l2 */
+} ldsc_h2_result;
+
+int ldsc_h2_batch(ldsc_ctx *ctx, const ldsc_h2_args *args, ldsc_h2_result *results);
+
+/* Batched genetic correlations (run_rg, src/regressions.rs:2113-2460): per
+ * pair, two h2 fits on z^2, the genetic-covariance fit on z1 * z2
+ * (gencov_weights, run_gencov_ldsc, src/regressions.rs:1612-1645,1828-2052),
+ * rg = gencov / sqrt(h2_1 h2_2) and its ratio-jackknife SE
+ * (ratio_jackknife, src/regressions.rs:1067-1120).  Free intercepts, no
+ * --two-step. */
+typedef struct {
+    uint64_t n_snp;
+    uint32_t n_pairs;
+    uint32_t n_blocks;
+    const double *z1;             /* n_pairs x n_snp signed z-scores of trait 1 */
+    const double *z2;             /* n_pairs x n_snp of trait 2 */
+    const double *n1;             /* n_pairs scalar sample sizes */
+    const double *n2;
+    const double *ref_l2;
+    const double *w_l2;
+    double m_snps;
+    int32_t device_pointers;
+} ldsc_rg_args;
+
+typedef struct {
+    double rg, rg_se, z, p;
+    double gencov, gencov_se, gencov_intercept, gencov_intercept_se;
+    double h2_1, h2_1_se, h2_2, h2_2_se;
+    double mean_z1z2;
+} ldsc_rg_result;
+
+int ldsc_rg_batch(ldsc_ctx *ctx, const ldsc_rg_args *args, ldsc_rg_result *results);
+
 /* ---- allocation-free entry point ---------------------------------------- */
 
 /* No counterpart in the reference: this entry point exists for callers that

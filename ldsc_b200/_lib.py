@@ -69,6 +69,32 @@ class SynthSpec(C.Structure):
                 ("switch_p", C.c_double), ("miss", C.c_double), ("seed", C.c_uint64)]
 
 
+class H2Args(C.Structure):
+    _fields_ = [("n_snp", C.c_uint64), ("n_traits", C.c_uint32), ("n_blocks", C.c_uint32),
+                ("chi2", C.c_void_p), ("n_per_snp", C.c_void_p), ("n_scalar", C.c_void_p),
+                ("ref_l2", C.c_void_p), ("w_l2", C.c_void_p), ("m_snps", C.c_double),
+                ("fixed_intercept", C.c_int32), ("intercept", C.c_double),
+                ("want_lambda_gc", C.c_int32), ("device_pointers", C.c_int32)]
+
+
+class H2Result(C.Structure):
+    _fields_ = [(f, C.c_double) for f in ("h2", "h2_se", "intercept", "intercept_se", "mean_chi2",
+                                          "lambda_gc", "ratio", "ratio_se", "coef", "coef_se")]
+
+
+class RgArgs(C.Structure):
+    _fields_ = [("n_snp", C.c_uint64), ("n_pairs", C.c_uint32), ("n_blocks", C.c_uint32),
+                ("z1", C.c_void_p), ("z2", C.c_void_p), ("n1", C.c_void_p), ("n2", C.c_void_p),
+                ("ref_l2", C.c_void_p), ("w_l2", C.c_void_p), ("m_snps", C.c_double),
+                ("device_pointers", C.c_int32)]
+
+
+class RgResult(C.Structure):
+    _fields_ = [(f, C.c_double) for f in ("rg", "rg_se", "z", "p", "gencov", "gencov_se",
+                                          "gencov_intercept", "gencov_intercept_se", "h2_1",
+                                          "h2_1_se", "h2_2", "h2_2_se", "mean_z1z2")]
+
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     "ldsc_abi_version": (C.c_int, []),
@@ -100,6 +126,8 @@ SIGNATURES = {
     "ldsc_l2_int8_noalloc": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p,
                                        C.c_void_p, C.c_void_p, C.c_void_p]),
     "ldsc_noalloc_last_error": (C.c_int, [C.c_char_p, C.c_size_t]),
+    "ldsc_h2_batch": (C.c_int, [C.c_void_p, C.POINTER(H2Args), C.c_void_p]),
+    "ldsc_rg_batch": (C.c_int, [C.c_void_p, C.POINTER(RgArgs), C.c_void_p]),
 }
 
 NOALLOC_SCRATCH_BYTES = 64 * 1024 * 1024

@@ -421,3 +421,49 @@ def compute_l2_from_bytes(bed_bytes: bytes, bim_text: str, fam_text: str, config
     finally:
         if own:
             ctx.close()
+
+
+# ---- regressions (src/h2.rs, src/regressions.rs) ----
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def h2_batch(ctx: Context, chi2, n, ref_l2, w_l2, m_snps: float, n_blocks: int = 200,
+             intercept: Optional[float] = None, lambda_gc: bool = True) -> np.ndarray:
+    """run_h2_ldsc for many traits (K = 1, no --two-step).  chi2: T x n_snp;
+    n: T scalars or T x n_snp.  Returns a structured array with the fields of
+    ldsc_h2_result."""
+    chi2 = _f64(np.atleast_2d(chi2))
+    T, m = chi2.shape
+    n = _f64(n)
+    per_snp = n.ndim == 2
+    ref_l2, w_l2 = _f64(ref_l2), _f64(w_l2)
+    args = L.H2Args(n_snp=m, n_traits=T, n_blocks=n_blocks, chi2=chi2.ctypes.data,
+                    n_per_snp=n.ctypes.data if per_snp else None,
+                    n_scalar=None if per_snp else n.ctypes.data,
+                    ref_l2=ref_l2.ctypes.data, w_l2=w_l2.ctypes.data, m_snps=float(m_snps),
+                    fixed_intercept=int(intercept is not None), intercept=float(intercept or 0.0),
+                    want_lambda_gc=int(lambda_gc), device_pointers=0)
+    out = (L.H2Result * T)()
+    ctx.check(ctx.lib.ldsc_h2_batch(ctx.h, C.byref(args), C.cast(out, C.c_void_p)))
+    names = [f for f, _ in L.H2Result._fields_]
+    return np.array([tuple(getattr(r, f) for f in names) for r in out],
+                    dtype=[(f, np.float64) for f in names])
+
+
+def rg_batch(ctx: Context, z1, z2, n1, n2, ref_l2, w_l2, m_snps: float,
+             n_blocks: int = 200) -> np.ndarray:
+    """run_rg for many trait pairs (free intercepts, no --two-step)."""
+    z1, z2 = _f64(np.atleast_2d(z1)), _f64(np.atleast_2d(z2))
+    P, m = z1.shape
+    n1, n2 = _f64(np.broadcast_to(n1, (P,))), _f64(np.broadcast_to(n2, (P,)))
+    ref_l2, w_l2 = _f64(ref_l2), _f64(w_l2)
+    args = L.RgArgs(n_snp=m, n_pairs=P, n_blocks=n_blocks, z1=z1.ctypes.data, z2=z2.ctypes.data,
+                    n1=n1.ctypes.data, n2=n2.ctypes.data, ref_l2=ref_l2.ctypes.data,
+                    w_l2=w_l2.ctypes.data, m_snps=float(m_snps), device_pointers=0)
+    out = (L.RgResult * P)()
+    ctx.check(ctx.lib.ldsc_rg_batch(ctx.h, C.byref(args), C.cast(out, C.c_void_p)))
+    names = [f for f, _ in L.RgResult._fields_]
+    return np.array([tuple(getattr(r, f) for f in names) for r in out],
+                    dtype=[(f, np.float64) for f in names])

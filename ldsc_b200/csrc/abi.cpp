@@ -18,6 +18,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <atomic>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -25,6 +26,7 @@
 #include "../../include/ldsc_b200.h"
 #include "engine.h"
 #include "plan.h"
+#include "regress.h"
 
 using namespace ldsc;
 
@@ -69,13 +71,23 @@ struct ldsc_ctx {
     // workspace (grow-only)
     DevBuf ops, xf64, xsk, recrows, keep, left, tiles, annot, aeff, aeff32, l2, maf, pq, err;
     DevBuf st_n, st_s, st_q, st_q3, st_q4, st_mean, st_inv, st_qinv, st_kappa, packed, tsum, dbg;
+    // CountSketch cache: bucket-major order and the permuted panel, keyed by
+    // (panel id, individuals used, d, keep-list hash)
+    DevBuf sk_perm, sk_seg, sk_wseg, sk_pp;
+    DevBuf rtiles, cptr_r, cidx_r, cptr_l, cidx_l;  // K > 1 contraction: r2u tiles and CSR tile lists
+    DevBuf rg_jobs, rg_states, rg_outs, rg_part, rg_tdel, rg_y, rg_y2, rg_n, rg_ld, rg_wld, rg_sel, rg_pairs, rg_res;
+    uint64_t sk_panel = 0, sk_n = 0, sk_key = 0, sk_pitch_words = 0;
+    uint32_t sk_d = 0;
 };
 
 struct ldsc_panel {
     ldsc_ctx* ctx = nullptr;
     uint8_t* rows = nullptr;
     uint64_t n_snp = 0, n_indiv = 0, bpr = 0, pitch = 0;
+    uint64_t id = 0;  // unique per panel, keys the CountSketch permuted-panel cache
 };
+
+static std::atomic<uint64_t> g_panel_ids{1};
 
 static int fail(ldsc_ctx* ctx, int code, const std::string& msg) {
     if (ctx) ctx->last_error = msg;
@@ -132,7 +144,12 @@ int ldsc_ctx_destroy(ldsc_ctx* ctx) {
                       &ctx->tiles, &ctx->annot, &ctx->aeff, &ctx->aeff32, &ctx->l2, &ctx->maf,
                       &ctx->pq, &ctx->err, &ctx->st_n, &ctx->st_s, &ctx->st_q, &ctx->st_q3,
                       &ctx->st_q4, &ctx->st_mean, &ctx->st_inv, &ctx->st_qinv, &ctx->st_kappa,
-                      &ctx->packed, &ctx->tsum, &ctx->dbg};
+                      &ctx->packed, &ctx->tsum, &ctx->dbg,
+                      &ctx->sk_perm, &ctx->sk_seg, &ctx->sk_wseg, &ctx->sk_pp,
+                      &ctx->rtiles, &ctx->cptr_r, &ctx->cidx_r, &ctx->cptr_l, &ctx->cidx_l,
+                      &ctx->rg_jobs, &ctx->rg_states, &ctx->rg_outs, &ctx->rg_part, &ctx->rg_tdel,
+                      &ctx->rg_y, &ctx->rg_y2, &ctx->rg_n, &ctx->rg_ld, &ctx->rg_wld, &ctx->rg_sel,
+                      &ctx->rg_pairs, &ctx->rg_res};
     for (DevBuf* b : bufs) b->release();
     if (ctx->own) cudaStreamDestroy(ctx->own);
     delete ctx;
@@ -190,6 +207,7 @@ int ldsc_panel_upload(ldsc_ctx* ctx, const uint8_t* body, uint64_t body_bytes, u
     p->n_indiv = n_indiv;
     p->bpr = bpr;
     p->pitch = round_up(bpr, 16);
+    p->id = g_panel_ids.fetch_add(1);
     const size_t bytes = (size_t)p->pitch * (n_snp ? n_snp : 1);
     cudaError_t e = cudaMalloc(&p->rows, bytes);
     if (e != cudaSuccess) {
@@ -222,6 +240,7 @@ int ldsc_panel_synth(ldsc_ctx* ctx, const ldsc_synth_spec* spec, ldsc_panel** ou
     p->n_indiv = spec->n_indiv;
     p->bpr = (spec->n_indiv + 3) / 4;
     p->pitch = round_up(p->bpr, 16);
+    p->id = g_panel_ids.fetch_add(1);
     const size_t bytes = (size_t)p->pitch * (spec->n_snp ? spec->n_snp : 1);
     uint8_t* table = nullptr;
     cudaError_t e = cudaMalloc(&p->rows, bytes);
@@ -317,6 +336,33 @@ struct Events {
     }
 };
 
+// Bucket-major order for a sketch, uploaded, and the panel rewritten in that
+// order (cached in the context until the panel / individuals / d change).
+int sketch_prepare(ldsc_ctx* ctx, const ldsc_panel* panel, uint64_t n_used, uint32_t d, const uint32_t* bucket,
+                   const float* sign, const int64_t* keep) {
+    cudaStream_t s = ctx->stream;
+    SketchOrder o = sketch_order(n_used, d, bucket, sign, keep);
+    const uint64_t words = (n_used + 15) / 16;
+    const uint64_t pitch_words = round_up(words, 4);
+    CK(ctx->sk_perm.ensure(4 * (size_t)n_used));
+    CK(ctx->sk_seg.ensure(4 * o.seg_off.size()));
+    CK(ctx->sk_wseg.ensure(4 * o.word_seg.size()));
+    CK(ctx->sk_pp.ensure((size_t)4 * pitch_words * (panel->n_snp ? panel->n_snp : 1)));
+    CK(cudaMemcpyAsync(ctx->sk_perm.p, o.perm.data(), 4 * (size_t)n_used, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(ctx->sk_seg.p, o.seg_off.data(), 4 * o.seg_off.size(), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(ctx->sk_wseg.p, o.word_seg.data(), 4 * o.word_seg.size(), cudaMemcpyHostToDevice, s));
+    PanelView pv{panel->rows, panel->n_snp, panel->n_indiv, panel->bpr, panel->pitch};
+    CK(launch_sketch_permute(pv, ctx->sk_perm.as<int32_t>(), n_used, ctx->sk_pp.as<uint32_t>(), pitch_words, s));
+    ctx->kernels++;
+    CK(cudaStreamSynchronize(s));  // host vectors go out of scope
+    ctx->sk_panel = panel->id;
+    ctx->sk_n = n_used;
+    ctx->sk_d = d;
+    ctx->sk_key = 0;
+    ctx->sk_pitch_words = pitch_words;
+    return LDSC_OK;
+}
+
 int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double* l2_out, double* maf_out,
            ldsc_perf* perf, double upload_secs) {
     const auto t_wall0 = std::chrono::steady_clock::now();
@@ -350,6 +396,9 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
     if (d > 12288) return fail(ctx, LDSC_E_UNSUPPORTED, "--sketch d > 12288 is not supported on the GPU");
     if (a->precision != LDSC_PRECISION_FP64 && a->precision != LDSC_PRECISION_INT8)
         return fail(ctx, LDSC_E_INVALID, "unknown precision");
+    if (a->window_mode < 0 || a->window_mode > 2) return fail(ctx, LDSC_E_INVALID, "invalid window mode");
+    if (m > 0 && (!a->chr || (a->window_mode == 0 && !a->cm) || (a->window_mode == 1 && !a->bp)))
+        return fail(ctx, LDSC_E_INVALID, "missing chr / cm / bp arrays for the window mode");
     if (!d && a->precision == LDSC_PRECISION_INT8 && n_used > 1000000)
         return fail(ctx, LDSC_E_UNSUPPORTED, "INT8 form supports up to 1,000,000 individuals");
     if (m > 0 && a->bed_idx) {
@@ -365,19 +414,8 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
         return LDSC_OK;
     }
 
-    // ---- host plan ----
-    LeftLimits L;
-    std::string perr;
-    if (!left_limits(m, a->chr, a->cm, a->bp, a->window_mode, a->window_size, a->window_snps, a->chunk_size,
-                     a->snp_level_masking != 0, a->global_pass != 0, &L, &perr))
-        return fail(ctx, LDSC_E_INVALID, perr);
-    if (L.any_full && !a->yes_really)
-        std::printf("WARNING: LD window spans the entire chromosome. Use --yes-really to silence this warning.\n");
-    pf.n_pairs = L.n_pairs;
     const bool exact_i8 = !d && a->precision == LDSC_PRECISION_INT8;
-    const int ta = exact_i8 ? 64 : 128, tb = 128;
-    std::vector<Tile> tiles = band_tiles(L.left, ta, tb);
-    pf.n_tiles = tiles.size();
+    const int ta = (exact_i8 || d) ? 64 : 128, tb = 128;  // tcgen05 tiles: 64 x 128 records
     pf.gram_kind = d ? 2u : (exact_i8 ? 1u : 0u);
 
     cudaStream_t s = ctx->stream;
@@ -386,8 +424,6 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
 
     // ---- device buffers ----
     const uint64_t nmom = (uint64_t)m;
-    CK(ctx->left.ensure(sizeof(int64_t) * nmom));
-    CK(ctx->tiles.ensure(sizeof(Tile) * (tiles.size() + 1)));
     CK(ctx->st_n.ensure(4 * nmom));
     CK(ctx->st_s.ensure(4 * nmom));
     CK(ctx->st_q.ensure(4 * nmom));
@@ -409,9 +445,6 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
     if (a->bed_idx) CK(ctx->recrows.ensure(8 * nmom));
     if (a->keep_iids) CK(ctx->keep.ensure(8 * a->n_keep));
 
-    CK(cudaMemcpyAsync(ctx->left.p, L.left.data(), 8 * nmom, cudaMemcpyHostToDevice, s));
-    if (!tiles.empty())
-        CK(cudaMemcpyAsync(ctx->tiles.p, tiles.data(), sizeof(Tile) * tiles.size(), cudaMemcpyHostToDevice, s));
     if (a->annot) CK(cudaMemcpyAsync(ctx->annot.p, a->annot, 8 * nmom * K, cudaMemcpyHostToDevice, s));
     if (a->bed_idx) CK(cudaMemcpyAsync(ctx->recrows.p, a->bed_idx, 8 * nmom, cudaMemcpyHostToDevice, s));
     if (a->keep_iids) CK(cudaMemcpyAsync(ctx->keep.p, a->keep_iids, 8 * a->n_keep, cudaMemcpyHostToDevice, s));
@@ -433,16 +466,39 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
     st.kappa = maf_aware ? ctx->st_kappa.as<double>() : nullptr;
     st.pq = nullptr;
 
+    if (d) {
+        uint64_t key = 1469598103934665603ull;
+        if (a->keep_iids)
+            for (uint64_t i = 0; i < a->n_keep; i++) key = (key ^ (uint64_t)a->keep_iids[i]) * 1099511628211ull;
+        if (!(ctx->sk_panel == panel->id && ctx->sk_n == n_used && ctx->sk_d == d && ctx->sk_key == key)) {
+            std::vector<uint32_t> bucket(n_used);
+            std::vector<float> sign(n_used);
+            countsketch_hash(n_used, d, 42, bucket.data(), sign.data());  // the reference's seed-42 stream
+            int rc = sketch_prepare(ctx, panel, n_used, d, bucket.data(), sign.data(), a->keep_iids);
+            if (rc != LDSC_OK) return rc;
+            ctx->sk_key = key;
+        }
+        CK(ctx->xsk.ensure((size_t)4 * 2 * nmom * round_up(d, 32)));
+    }
+
     Events ev(s);
     const int e0 = ev.mark();
 
     // ---- decode ----
     const uint64_t ld_i8 = round_up(n_used, 128);
+    const uint64_t ld_sk = round_up(d ? d : 1, 32);  // 128-byte operand rows for TMA
+    int e_sk = -1;
     if (exact_i8) {
         CK(ctx->ops.ensure((size_t)2 * nmom * ld_i8));
         CK(launch_decode_i8(pv, rr, m, sel, ctx->ops.as<uint8_t>(), ld_i8, st, 0, s));
+    } else if (d) {
+        // fused: moments + CountSketch rows in one pass over the permuted panel
+        CK(launch_sketch_seg(ctx->sk_pp.as<uint32_t>(), ctx->sk_pitch_words, rr, m, n_used,
+                             ctx->sk_seg.as<int32_t>(), ctx->sk_wseg.as<int32_t>(), d, st, maf_aware ? 1 : 0, 1,
+                             ctx->xsk.as<float>(), ld_sk, s));
+        e_sk = ev.mark();
     } else {
-        CK(launch_decode_i8(pv, rr, m, sel, nullptr, 0, st, maf_aware ? 1 : 0, s));
+        CK(launch_decode_i8(pv, rr, m, sel, nullptr, 0, st, 0, s));
     }
     ctx->kernels++;
     CK(launch_finalize_stats(m, n_used, st, a->annot ? ctx->annot.as<double>() : nullptr, K, a->has_pq_exp,
@@ -456,33 +512,53 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
         ctx->kernels++;
     }
     const int e1 = ev.mark();
-    int e_sk = -1;
-    const uint64_t ld_sk = round_up(d ? d : 1, 8);
-    if (d) {
-        // CountSketch hash on the host, exactly the reference's stream (seed 42)
-        std::vector<uint32_t> bucket(n_used);
-        std::vector<float> sign(n_used);
-        countsketch_hash(n_used, d, 42, bucket.data(), sign.data());
-        const uint64_t npad = round_up(n_used, 16);
-        std::vector<uint32_t> packed(npad, 0);
-        std::vector<int32_t> tsum(d, 0);
-        for (uint64_t i = 0; i < n_used; i++) {
-            packed[i] = bucket[i] | (sign[i] < 0 ? 0x80000000u : 0u);
-            tsum[bucket[i]] += sign[i] < 0 ? -1 : 1;
-        }
-        CK(ctx->packed.ensure(4 * npad));
-        CK(ctx->tsum.ensure(4 * (size_t)d));
-        CK(ctx->xsk.ensure((size_t)4 * nmom * ld_sk));
-        CK(cudaMemcpyAsync(ctx->packed.p, packed.data(), 4 * npad, cudaMemcpyHostToDevice, s));
-        CK(cudaMemcpyAsync(ctx->tsum.p, tsum.data(), 4 * (size_t)d, cudaMemcpyHostToDevice, s));
-        CK(cudaMemsetAsync(ctx->xsk.p, 0, (size_t)4 * nmom * ld_sk, s));
-        CK(launch_sketch_scatter(pv, rr, m, sel, ctx->packed.as<uint32_t>(), ctx->tsum.as<int32_t>(), d, st,
-                                 ctx->xsk.as<float>(), ld_sk, s));
-        ctx->kernels++;
-        CK(cudaStreamSynchronize(s));  // host vectors go out of scope
-        e_sk = ev.mark();
-    }
 
+    // ---- host plan (runs while the decode kernels execute) ----
+    LeftLimits L;
+    std::string perr;
+    if (!left_limits(m, a->chr, a->cm, a->bp, a->window_mode, a->window_size, a->window_snps, a->chunk_size,
+                     a->snp_level_masking != 0, a->global_pass != 0, &L, &perr))
+        return fail(ctx, LDSC_E_INVALID, perr);
+    if (L.any_full && !a->yes_really)
+        std::printf("WARNING: LD window spans the entire chromosome. Use --yes-really to silence this warning.\n");
+    pf.n_pairs = L.n_pairs;
+    std::vector<Tile> tiles = band_tiles(L.left, ta, tb);
+    pf.n_tiles = tiles.size();
+
+    CK(ctx->left.ensure(sizeof(int64_t) * nmom));
+    CK(ctx->tiles.ensure(sizeof(Tile) * (tiles.size() + 1)));
+    CK(cudaMemcpyAsync(ctx->left.p, L.left.data(), 8 * nmom, cudaMemcpyHostToDevice, s));
+    if (!tiles.empty())
+        CK(cudaMemcpyAsync(ctx->tiles.p, tiles.data(), sizeof(Tile) * tiles.size(), cudaMemcpyHostToDevice, s));
+    // K > 1: CSR lists of tiles per right block and per left block for the contraction
+    const int32_t n_right = (int32_t)((m + tb - 1) / tb), n_left = (int32_t)((m + ta - 1) / ta);
+    std::vector<int32_t> ptr_r, idx_r, ptr_l, idx_l;
+    if (K > 1 && !tiles.empty()) {
+        ptr_r.assign(n_right + 1, 0);
+        ptr_l.assign(n_left + 1, 0);
+        for (const Tile& t : tiles) {
+            ptr_r[t.b_blk + 1]++;
+            ptr_l[t.a_blk + 1]++;
+        }
+        for (int32_t i = 0; i < n_right; i++) ptr_r[i + 1] += ptr_r[i];
+        for (int32_t i = 0; i < n_left; i++) ptr_l[i + 1] += ptr_l[i];
+        idx_r.resize(tiles.size());
+        idx_l.resize(tiles.size());
+        std::vector<int32_t> fr(ptr_r.begin(), ptr_r.end() - 1), fl(ptr_l.begin(), ptr_l.end() - 1);
+        for (int32_t t = 0; t < (int32_t)tiles.size(); t++) {
+            idx_r[fr[tiles[t].b_blk]++] = t;
+            idx_l[fl[tiles[t].a_blk]++] = t;
+        }
+        CK(ctx->rtiles.ensure(sizeof(float) * (size_t)ta * tb * tiles.size()));
+        CK(ctx->cptr_r.ensure(4 * ptr_r.size()));
+        CK(ctx->cidx_r.ensure(4 * idx_r.size()));
+        CK(ctx->cptr_l.ensure(4 * ptr_l.size()));
+        CK(ctx->cidx_l.ensure(4 * idx_l.size()));
+        CK(cudaMemcpyAsync(ctx->cptr_r.p, ptr_r.data(), 4 * ptr_r.size(), cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(ctx->cidx_r.p, idx_r.data(), 4 * idx_r.size(), cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(ctx->cptr_l.p, ptr_l.data(), 4 * ptr_l.size(), cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(ctx->cidx_l.p, idx_l.data(), 4 * idx_l.size(), cudaMemcpyHostToDevice, s));
+    }
     // ---- band Gram + epilogue ----
     EpilogueArgs ep{};
     ep.left = ctx->left.as<int64_t>();
@@ -503,11 +579,12 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
     ep.n_inv_sq = (1.0 / N) * (1.0 / N);
     ep.sketch_d = (double)d;
     ep.err = ctx->err.as<unsigned int>();
-    const int e2 = d ? e_sk : e1;
+    ep.rtiles = (K > 1 && !tiles.empty()) ? ctx->rtiles.as<float>() : nullptr;
+    const int e2 = ev.mark();
     if (!tiles.empty()) {
         if (d) {
-            CK(launch_gram_f32(ctx->xsk.as<float>(), ld_sk, ld_sk, ctx->tiles.as<Tile>(), (int64_t)tiles.size(), ep,
-                               maf_aware ? 1 : 0, ctx->sms, s));
+            CK(launch_gram_tf32(ctx->xsk.as<float>(), ld_sk, m, ctx->tiles.as<Tile>(), (int64_t)tiles.size(), ep,
+                                maf_aware ? 1 : 0, nullptr, ctx->sms, s));
         } else if (exact_i8) {
             CK(launch_gram_i8(ctx->ops.as<uint8_t>(), ld_i8, m, ctx->tiles.as<Tile>(), (int64_t)tiles.size(), ep,
                               nullptr, ctx->sms, s));
@@ -516,6 +593,13 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
                                ep, ctx->sms, s));
         }
         ctx->kernels++;
+        if (K > 1) {
+            CK(launch_contract(ctx->rtiles.as<float>(), ta, tb, ctx->tiles.as<Tile>(), ctx->cptr_r.as<int32_t>(),
+                               ctx->cidx_r.as<int32_t>(), n_right, true, ep, s));
+            CK(launch_contract(ctx->rtiles.as<float>(), ta, tb, ctx->tiles.as<Tile>(), ctx->cptr_l.as<int32_t>(),
+                               ctx->cidx_l.as<int32_t>(), n_left, false, ep, s));
+            ctx->kernels += 2;
+        }
     }
     const int e3 = ev.mark();
     CK(cudaMemcpyAsync(l2_out, ctx->l2.p, 8 * nmom * K, cudaMemcpyDeviceToHost, s));
@@ -527,8 +611,8 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
     if (herr[0] != 0)
         return fail(ctx, LDSC_E_TIMEOUT, "a device wait in the Gram kernel exceeded its bound (error word " +
                                              std::to_string(herr[0]) + ")");
-    pf.norm_secs = ev.ms(e0, e1) / 1e3;
-    if (d) pf.sketch_secs = ev.ms(e1, e_sk) / 1e3;
+    pf.norm_secs = ev.ms(d ? e_sk : e0, e1) / 1e3;
+    if (d) pf.sketch_secs = ev.ms(e0, e_sk) / 1e3;
     pf.ab_dot_secs = ev.ms(e2, e3) / 1e3;
     pf.device_ms = ev.ms(e0, e4);
     pf.kernel_launches = (uint32_t)(ctx->kernels - kernels0);
@@ -594,52 +678,33 @@ int ldsc_sketch_project(ldsc_ctx* ctx, const ldsc_panel* panel, uint64_t b, uint
     const int64_t m = (int64_t)(e - b);
     if (m == 0) return LDSC_OK;
     const uint64_t n_used = keep ? n_keep : panel->n_indiv;
-    cudaStream_t s = ctx->stream;
-    CK(cudaSetDevice(ctx->device));
-    std::vector<uint64_t> rows((size_t)m);
-    for (int64_t i = 0; i < m; i++) rows[i] = b + (uint64_t)i;
-    const uint64_t npad = round_up(n_used, 16);
-    std::vector<uint32_t> packed(npad, 0);
-    std::vector<int32_t> tsum(d, 0);
+    if (n_used == 0) return fail(ctx, LDSC_E_INVALID, "no individuals");
     for (uint64_t i = 0; i < n_used; i++) {
         if (bucket[i] >= d) return fail(ctx, LDSC_E_INVALID, "bucket index >= d");
-        packed[i] = bucket[i] | (sign[i] < 0 ? 0x80000000u : 0u);
-        tsum[bucket[i]] += sign[i] < 0 ? -1 : 1;
+        if (keep && (keep[i] < 0 || (uint64_t)keep[i] >= panel->n_indiv))
+            return fail(ctx, LDSC_E_INVALID, "keep index out of range");
     }
+    cudaStream_t s = ctx->stream;
+    CK(cudaSetDevice(ctx->device));
+    int rc = sketch_prepare(ctx, panel, n_used, d, bucket, sign, keep);
+    ctx->sk_panel = 0;  // explicit bucket/sign arrays: do not reuse for l2 runs
+    if (rc != LDSC_OK) return rc;
+    std::vector<uint64_t> rows((size_t)m);
+    for (int64_t i = 0; i < m; i++) rows[i] = b + (uint64_t)i;
     CK(ctx->recrows.ensure(8 * (size_t)m));
     CK(ctx->st_n.ensure(4 * (size_t)m));
     CK(ctx->st_s.ensure(4 * (size_t)m));
     CK(ctx->st_q.ensure(4 * (size_t)m));
-    CK(ctx->maf.ensure(8 * (size_t)m));
-    CK(ctx->st_mean.ensure(8 * (size_t)m));
-    CK(ctx->st_inv.ensure(8 * (size_t)m));
-    CK(ctx->st_qinv.ensure(8 * (size_t)m));
-    CK(ctx->packed.ensure(4 * npad));
-    CK(ctx->tsum.ensure(4 * (size_t)d));
     CK(ctx->xsk.ensure(4 * (size_t)m * d));
-    if (keep) {
-        CK(ctx->keep.ensure(8 * n_keep));
-        CK(cudaMemcpyAsync(ctx->keep.p, keep, 8 * n_keep, cudaMemcpyHostToDevice, s));
-    }
     CK(cudaMemcpyAsync(ctx->recrows.p, rows.data(), 8 * (size_t)m, cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(ctx->packed.p, packed.data(), 4 * npad, cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(ctx->tsum.p, tsum.data(), 4 * (size_t)d, cudaMemcpyHostToDevice, s));
-    PanelView pv{panel->rows, panel->n_snp, panel->n_indiv, panel->bpr, panel->pitch};
-    IndivSel sel{keep ? ctx->keep.as<int64_t>() : nullptr, n_used};
     RecStats st{};
     st.n = ctx->st_n.as<int32_t>();
     st.s = ctx->st_s.as<int32_t>();
     st.q = ctx->st_q.as<int32_t>();
-    st.maf = ctx->maf.as<double>();
-    st.mean = ctx->st_mean.as<double>();
-    st.inv_std = ctx->st_inv.as<double>();
-    st.qinv = ctx->st_qinv.as<double>();
-    const uint64_t* rr = ctx->recrows.as<uint64_t>();
-    CK(launch_decode_i8(pv, rr, m, sel, nullptr, 0, st, 0, s));
-    CK(launch_finalize_stats(m, n_used, st, nullptr, 0, 0, 0.0, nullptr, nullptr, nullptr, s));
-    CK(launch_sketch_scatter(pv, rr, m, sel, ctx->packed.as<uint32_t>(), ctx->tsum.as<int32_t>(), d, st,
-                             ctx->xsk.as<float>(), d, s));
-    ctx->kernels += 3;
+    CK(launch_sketch_seg(ctx->sk_pp.as<uint32_t>(), ctx->sk_pitch_words, ctx->recrows.as<uint64_t>(), m, n_used,
+                         ctx->sk_seg.as<int32_t>(), ctx->sk_wseg.as<int32_t>(), d, st, 0, 0, ctx->xsk.as<float>(), d,
+                         s));
+    ctx->kernels += 1;
     CK(cudaMemcpyAsync(out, ctx->xsk.p, 4 * (size_t)m * d, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     return LDSC_OK;
@@ -709,3 +774,241 @@ int ldsc_debug_gram_i8_tile(ldsc_ctx* ctx, const ldsc_panel* panel, uint64_t k0,
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// regressions
+// ---------------------------------------------------------------------------
+
+namespace {
+
+// Device copies (or views) of the inputs shared by every job of a batch.
+int reg_inputs(ldsc_ctx* ctx, int device_pointers, uint64_t n, const double* ld, const double* wld,
+               const double** d_ld, const double** d_wld) {
+    if (device_pointers) {
+        *d_ld = ld;
+        *d_wld = wld;
+        return LDSC_OK;
+    }
+    cudaStream_t s = ctx->stream;
+    CK(ctx->rg_ld.ensure(8 * n));
+    CK(ctx->rg_wld.ensure(8 * n));
+    CK(cudaMemcpyAsync(ctx->rg_ld.p, ld, 8 * n, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(ctx->rg_wld.p, wld, 8 * n, cudaMemcpyHostToDevice, s));
+    *d_ld = ctx->rg_ld.as<double>();
+    *d_wld = ctx->rg_wld.as<double>();
+    return LDSC_OK;
+}
+
+const double* dev_array(ldsc_ctx* ctx, DevBuf& buf, const double* src, size_t count, int device_pointers,
+                        cudaError_t* err) {
+    *err = cudaSuccess;
+    if (!src) return nullptr;
+    if (device_pointers) return src;
+    *err = buf.ensure(8 * count);
+    if (*err != cudaSuccess) return nullptr;
+    *err = cudaMemcpyAsync(buf.p, src, 8 * count, cudaMemcpyHostToDevice, ctx->stream);
+    return buf.as<double>();
+}
+
+}  // namespace
+
+extern "C" int ldsc_h2_batch(ldsc_ctx* ctx, const ldsc_h2_args* a, ldsc_h2_result* res) {
+    if (!ctx || !a || !res) return LDSC_E_INVALID;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    const uint64_t n = a->n_snp;
+    const int T = (int)a->n_traits;
+    if (T == 0) return LDSC_OK;
+    if (n == 0 || !a->chi2 || !a->ref_l2 || !a->w_l2 || (!a->n_per_snp && !a->n_scalar))
+        return fail(ctx, LDSC_E_INVALID, "ldsc_h2_batch: missing inputs");
+    // n_blocks = min(n_obs, --n-blocks) as the callers do (src/regressions.rs:697, 2389)
+    const int nb = (int)std::min<uint64_t>(a->n_blocks, n);
+    if (nb < 2) return fail(ctx, LDSC_E_INVALID, "n_blocks must be >= 2");
+    if (!(a->m_snps > 0)) return fail(ctx, LDSC_E_INVALID, "M must be > 0");
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->stream;
+    const double *d_ld, *d_wld;
+    int rc = reg_inputs(ctx, a->device_pointers, n, a->ref_l2, a->w_l2, &d_ld, &d_wld);
+    if (rc != LDSC_OK) return rc;
+    cudaError_t e;
+    const double* d_y = dev_array(ctx, ctx->rg_y, a->chi2, (size_t)T * n, a->device_pointers, &e);
+    CK(e);
+    const double* d_n = dev_array(ctx, ctx->rg_n, a->n_per_snp, (size_t)T * n, a->device_pointers, &e);
+    CK(e);
+    std::vector<RegJob> jobs(T);
+    for (int t = 0; t < T; t++) {
+        RegJob& jb = jobs[t];
+        std::memset(&jb, 0, sizeof(jb));
+        jb.ya = d_y + (size_t)t * n;
+        jb.ymode = REG_Y_DIRECT;
+        jb.kind = REG_HSQ;
+        jb.n1 = d_n ? d_n + (size_t)t * n : nullptr;
+        jb.n1s = a->n_scalar && !d_n ? (a->device_pointers ? 0.0 : a->n_scalar[t]) : 0.0;
+        jb.fixed = a->fixed_intercept;
+        jb.fixed_int = a->intercept;
+        jb.hsq1 = jb.hsq2 = -1;
+    }
+    if (a->device_pointers && !d_n) {
+        // scalar sample sizes live on the device: fetch them (T doubles)
+        std::vector<double> ns(T);
+        CK(cudaMemcpyAsync(ns.data(), a->n_scalar, 8 * (size_t)T, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        for (int t = 0; t < T; t++) jobs[t].n1s = ns[t];
+    }
+    CK(ctx->rg_jobs.ensure(sizeof(RegJob) * T));
+    CK(ctx->rg_states.ensure(sizeof(RegState) * T));
+    CK(ctx->rg_outs.ensure(sizeof(RegOut) * T));
+    CK(ctx->rg_part.ensure(sizeof(double) * 5 * (size_t)T * nb));
+    CK(ctx->rg_sel.ensure(sizeof(double) * 2 * T));
+    CK(cudaMemcpyAsync(ctx->rg_jobs.p, jobs.data(), sizeof(RegJob) * T, cudaMemcpyHostToDevice, s));
+    CK(launch_regressions(ctx->rg_jobs.as<RegJob>(), ctx->rg_states.as<RegState>(), ctx->rg_outs.as<RegOut>(),
+                          nullptr, ctx->rg_part.as<double>(), nullptr, d_ld, d_wld, n, nb, a->m_snps, T, s));
+    ctx->kernels += 8;
+    if (a->want_lambda_gc) {
+        // median (src/h2.rs:394-414): middle order statistic, mean of the two for even n
+        CK(launch_select(ctx->rg_jobs.as<RegJob>(), n, n / 2, ctx->rg_sel.as<double>(), T, s));
+        if (n % 2 == 0) CK(launch_select(ctx->rg_jobs.as<RegJob>(), n, n / 2 - 1, ctx->rg_sel.as<double>() + T, T, s));
+        ctx->kernels += n % 2 == 0 ? 2 : 1;
+    }
+    std::vector<RegOut> outs(T);
+    std::vector<double> sel(2 * T, NAN);
+    CK(cudaMemcpyAsync(outs.data(), ctx->rg_outs.p, sizeof(RegOut) * T, cudaMemcpyDeviceToHost, s));
+    if (a->want_lambda_gc) CK(cudaMemcpyAsync(sel.data(), ctx->rg_sel.p, 8 * 2 * (size_t)T, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    for (int t = 0; t < T; t++) {
+        const RegOut& o = outs[t];
+        ldsc_h2_result& r = res[t];
+        r.h2 = o.tot;
+        r.h2_se = o.tot_se;
+        r.intercept = o.intercept;
+        r.intercept_se = o.intercept_se;
+        r.mean_chi2 = o.mean_y;
+        r.coef = o.est[0] / o.nbar;
+        r.coef_se = o.se[0] / o.nbar;
+        r.lambda_gc = NAN;
+        if (a->want_lambda_gc) {
+            const double med = n % 2 == 0 ? (sel[t] + sel[T + t]) / 2.0 : sel[t];
+            r.lambda_gc = med / 0.4549;
+        }
+        if (!a->fixed_intercept && r.mean_chi2 > 1.0) {
+            r.ratio = (r.intercept - 1.0) / (r.mean_chi2 - 1.0);
+            r.ratio_se = r.intercept_se / (r.mean_chi2 - 1.0);
+        } else {
+            r.ratio = NAN;
+            r.ratio_se = NAN;
+        }
+    }
+    return LDSC_OK;
+}
+
+extern "C" int ldsc_rg_batch(ldsc_ctx* ctx, const ldsc_rg_args* a, ldsc_rg_result* res) {
+    if (!ctx || !a || !res) return LDSC_E_INVALID;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    const uint64_t n = a->n_snp;
+    const int P = (int)a->n_pairs;
+    if (P == 0) return LDSC_OK;
+    if (n == 0 || !a->z1 || !a->z2 || !a->n1 || !a->n2 || !a->ref_l2 || !a->w_l2)
+        return fail(ctx, LDSC_E_INVALID, "ldsc_rg_batch: missing inputs");
+    // n_blocks = min(n_obs, --n-blocks) as the callers do (src/regressions.rs:697, 2389)
+    const int nb = (int)std::min<uint64_t>(a->n_blocks, n);
+    if (nb < 2) return fail(ctx, LDSC_E_INVALID, "n_blocks must be >= 2");
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->stream;
+    const double *d_ld, *d_wld;
+    int rc = reg_inputs(ctx, a->device_pointers, n, a->ref_l2, a->w_l2, &d_ld, &d_wld);
+    if (rc != LDSC_OK) return rc;
+    cudaError_t e;
+    const double* d_z1 = dev_array(ctx, ctx->rg_y, a->z1, (size_t)P * n, a->device_pointers, &e);
+    CK(e);
+    const double* d_z2 = dev_array(ctx, ctx->rg_y2, a->z2, (size_t)P * n, a->device_pointers, &e);
+    CK(e);
+    std::vector<double> n1(P), n2(P);
+    if (a->device_pointers) {
+        CK(cudaMemcpyAsync(n1.data(), a->n1, 8 * (size_t)P, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(n2.data(), a->n2, 8 * (size_t)P, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+    } else {
+        for (int p = 0; p < P; p++) {
+            n1[p] = a->n1[p];
+            n2[p] = a->n2[p];
+        }
+    }
+    // jobs 0..2P-1: h2 of z1^2 and z2^2; jobs 2P..3P-1: genetic covariance
+    std::vector<RegJob> jobs(3 * P);
+    std::vector<RgPairIdx> idx(P);
+    for (int p = 0; p < P; p++) {
+        for (int q = 0; q < 3; q++) {
+            RegJob& jb = jobs[q == 2 ? 2 * P + p : 2 * p + q];
+            std::memset(&jb, 0, sizeof(jb));
+            jb.hsq1 = jb.hsq2 = -1;
+        }
+        RegJob& h1 = jobs[2 * p];
+        h1.ya = d_z1 + (size_t)p * n;
+        h1.ymode = REG_Y_SQUARE;
+        h1.kind = REG_HSQ;
+        h1.n1s = n1[p];
+        RegJob& h2 = jobs[2 * p + 1];
+        h2.ya = d_z2 + (size_t)p * n;
+        h2.ymode = REG_Y_SQUARE;
+        h2.kind = REG_HSQ;
+        h2.n1s = n2[p];
+        RegJob& gc = jobs[2 * P + p];
+        gc.ya = d_z1 + (size_t)p * n;
+        gc.yb = d_z2 + (size_t)p * n;
+        gc.ymode = REG_Y_PRODUCT;
+        gc.kind = REG_GENCOV;
+        gc.n1s = n1[p];
+        gc.n2s = n2[p];
+        gc.hsq1 = 2 * p;
+        gc.hsq2 = 2 * p + 1;
+        idx[p] = RgPairIdx{2 * p, 2 * p + 1, 2 * P + p};
+    }
+    const int J = 3 * P;
+    CK(ctx->rg_jobs.ensure(sizeof(RegJob) * J));
+    CK(ctx->rg_states.ensure(sizeof(RegState) * J));
+    CK(ctx->rg_outs.ensure(sizeof(RegOut) * J));
+    CK(ctx->rg_part.ensure(sizeof(double) * 5 * (size_t)J * nb));
+    CK(ctx->rg_tdel.ensure(sizeof(double) * (size_t)J * nb));
+    CK(ctx->rg_pairs.ensure(sizeof(RgPairIdx) * P));
+    CK(ctx->rg_res.ensure(sizeof(RgOut) * P));
+    CK(cudaMemcpyAsync(ctx->rg_jobs.p, jobs.data(), sizeof(RegJob) * J, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(ctx->rg_pairs.p, idx.data(), sizeof(RgPairIdx) * P, cudaMemcpyHostToDevice, s));
+    RegJob* dj = ctx->rg_jobs.as<RegJob>();
+    RegState* dst = ctx->rg_states.as<RegState>();
+    RegOut* dout = ctx->rg_outs.as<RegOut>();
+    double* dtd = ctx->rg_tdel.as<double>();
+    // stage 1: the h2 fits; stage 2: the covariance fits, whose weights use them
+    CK(launch_regressions(dj, dst, dout, nullptr, ctx->rg_part.as<double>(), dtd, d_ld, d_wld, n, nb, a->m_snps,
+                          2 * P, s));
+    CK(launch_regressions(dj + 2 * P, dst + 2 * P, dout + 2 * P, dout,
+                          ctx->rg_part.as<double>() + (size_t)2 * P * nb * 5, dtd + (size_t)2 * P * nb, d_ld, d_wld,
+                          n, nb, a->m_snps, P, s));
+    CK(launch_rg_finish(ctx->rg_pairs.as<RgPairIdx>(), dout, dtd, nb, ctx->rg_res.as<RgOut>(), P, s));
+    ctx->kernels += 17;
+    std::vector<RgOut> outs(P);
+    CK(cudaMemcpyAsync(outs.data(), ctx->rg_res.p, sizeof(RgOut) * P, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    for (int p = 0; p < P; p++) {
+        const RgOut& o = outs[p];
+        ldsc_rg_result& r = res[p];
+        r.rg = o.rg;
+        r.rg_se = o.rg_se;
+        r.gencov = o.gencov;
+        r.gencov_se = o.gencov_se;
+        r.gencov_intercept = o.gencov_intercept;
+        r.gencov_intercept_se = o.gencov_intercept_se;
+        r.h2_1 = o.h2_1;
+        r.h2_1_se = o.h2_1_se;
+        r.h2_2 = o.h2_2;
+        r.h2_2_se = o.h2_2_se;
+        r.mean_z1z2 = o.mean_z1z2;
+        // p_z_norm: two-sided normal p-value (1 - chi2_1 cdf of z^2)
+        if (std::isfinite(r.rg_se) && r.rg_se != 0.0) {
+            r.z = r.rg / r.rg_se;
+            r.p = std::isfinite(r.z) ? std::erfc(std::fabs(r.z) / std::sqrt(2.0)) : 0.0;
+        } else {
+            r.z = INFINITY;
+            r.p = 0.0;
+        }
+    }
+    return LDSC_OK;
+}

@@ -1,6 +1,6 @@
 // decode.cu -- PLINK BED decode kernels (HBM-bound).
 //
-// One warp per SNP record.  Each lane takes 16 individuals per step as one
+// One warp per SNP record.  Each lane takes 16 individuals at a time as one
 // 32-bit word of 2-bit codes (count-A1 LUT [2, missing, 1, 0], reference
 // src/bed.rs:470-521) and turns it into per-slot bit masks:
 //     lo = bit 0 of each code, hi = bit 1
@@ -61,6 +61,35 @@ __device__ __forceinline__ T warp_sum(T v) {
     return v;
 }
 
+// Expand one 16-individual code word into genotype and mask bytes and
+// accumulate the moment counts.
+__device__ __forceinline__ void expand16(uint32_t w, uint8_t* grow, uint8_t* mrow, uint64_t i0, uint32_t& cn,
+                                         uint32_t& c1, uint32_t& c2) {
+    const uint32_t lo = w & kEven;
+    const uint32_t hi = (w >> 1) & kEven;
+    const uint32_t pres = (~lo | hi) & kEven;
+    const uint32_t two = ~lo & ~hi & kEven;
+    const uint32_t one = ~lo & hi & kEven;
+    cn += __popc(pres);
+    c1 += __popc(one);
+    c2 += __popc(two);
+    if (grow) {
+        uint4 g, mk;
+        g.x = spread4(one) + 2u * spread4(two);
+        g.y = spread4(one >> 8) + 2u * spread4(two >> 8);
+        g.z = spread4(one >> 16) + 2u * spread4(two >> 16);
+        g.w = spread4(one >> 24) + 2u * spread4(two >> 24);
+        mk.x = spread4(pres);
+        mk.y = spread4(pres >> 8);
+        mk.z = spread4(pres >> 16);
+        mk.w = spread4(pres >> 24);
+        *reinterpret_cast<uint4*>(grow + i0) = g;   // a warp stores 512 contiguous bytes
+        *reinterpret_cast<uint4*>(mrow + i0) = mk;
+    }
+}
+
+// A warp decodes 2,048 individuals per step: lane l takes words l, l+32,
+// l+64, l+96 of the step (loads issued together, stores coalesced).
 __global__ void __launch_bounds__(256) k_decode_i8(PanelView p, const uint64_t* __restrict__ rec_rows,
                                                    int64_t m, IndivSel sel, uint8_t* __restrict__ ops,
                                                    uint64_t ld, RecStats st, int want_moments) {
@@ -70,50 +99,29 @@ __global__ void __launch_bounds__(256) k_decode_i8(PanelView p, const uint64_t* 
     for (int64_t r = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < m; r += warps) {
         const uint64_t brow = rec_rows ? rec_rows[r] : (uint64_t)r;
         const uint8_t* row = p.rows + brow * p.pitch;
-        uint32_t cn = 0, cs = 0, cq = 0, c3 = 0, c4 = 0;
+        uint32_t cn = 0, c1 = 0, c2 = 0;
         uint8_t* grow = ops ? ops + (uint64_t)(2 * r) * ld : nullptr;
         uint8_t* mrow = ops ? grow + ld : nullptr;
-        for (uint64_t i0 = (uint64_t)lane * 16; i0 < span; i0 += 512) {
-            const uint32_t w = codes16(row, sel, i0);
-            const uint32_t lo = w & kEven;
-            const uint32_t hi = (w >> 1) & kEven;
-            const uint32_t pres = (~lo | hi) & kEven;
-            const uint32_t two = ~lo & ~hi & kEven;
-            const uint32_t one = ~lo & hi & kEven;
-            const uint32_t p1 = __popc(one), p2 = __popc(two);
-            cn += __popc(pres);
-            cs += p1 + 2 * p2;
-            cq += p1 + 4 * p2;
-            c3 += p1 + 8 * p2;
-            c4 += p1 + 16 * p2;
-            if (ops) {
-                uint4 g, mk;
-                g.x = spread4(one) + 2u * spread4(two);
-                g.y = spread4(one >> 8) + 2u * spread4(two >> 8);
-                g.z = spread4(one >> 16) + 2u * spread4(two >> 16);
-                g.w = spread4(one >> 24) + 2u * spread4(two >> 24);
-                mk.x = spread4(pres);
-                mk.y = spread4(pres >> 8);
-                mk.z = spread4(pres >> 16);
-                mk.w = spread4(pres >> 24);
-                *reinterpret_cast<uint4*>(grow + i0) = g;
-                *reinterpret_cast<uint4*>(mrow + i0) = mk;
+        for (uint64_t s0 = 0; s0 < span; s0 += 2048) {
+            uint32_t w[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) w[u] = codes16(row, sel, s0 + 512 * u + 16 * lane);
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const uint64_t i0 = s0 + 512 * u + 16 * lane;
+                if (i0 < span) expand16(w[u], grow, mrow, i0, cn, c1, c2);
             }
         }
-        cn = warp_sum(cn);
-        cs = warp_sum(cs);
-        cq = warp_sum(cq);
-        if (want_moments) {
-            c3 = warp_sum(c3);
-            c4 = warp_sum(c4);
-        }
+        const uint32_t cs = c1 + 2 * c2, cq = c1 + 4 * c2, c3 = c1 + 8 * c2, c4 = c1 + 16 * c2;
+        const uint32_t tn = warp_sum(cn), ts = warp_sum(cs), tq = warp_sum(cq);
+        const uint32_t t3 = want_moments ? warp_sum(c3) : 0u, t4 = want_moments ? warp_sum(c4) : 0u;
         if (lane == 0) {
-            st.n[r] = (int32_t)cn;
-            st.s[r] = (int32_t)cs;
-            st.q[r] = (int32_t)cq;
+            st.n[r] = (int32_t)tn;
+            st.s[r] = (int32_t)ts;
+            st.q[r] = (int32_t)tq;
             if (want_moments && st.q3) {
-                st.q3[r] = (int32_t)c3;
-                st.q4[r] = (int32_t)c4;
+                st.q3[r] = (int32_t)t3;
+                st.q4[r] = (int32_t)t4;
             }
         }
     }

@@ -63,6 +63,7 @@ struct EpilogueArgs {
     double n_inv_sq;          // 1 / N^2       (sketch form)
     double sketch_d;          // d as double   (sketch form)
     unsigned int* err;        // device error word (non-zero = a bounded wait gave up)
+    float* rtiles;            // K > 1: tile t's masked r2u values, ta x tb f32 at t * ta * tb
 };
 
 // ---- kernels (launchers return cudaError_t of the launch) ----
@@ -96,17 +97,42 @@ cudaError_t launch_gram_i8(const uint8_t* ops, uint64_t ld, int64_t m, const Til
                            int64_t n_tiles, const EpilogueArgs& ep, int32_t* dbg, int sms,
                            cudaStream_t stream);
 
-// CountSketch: per record, scatter into d buckets and ratio-renormalise.
-// `packed` holds bucket | (sign < 0) << 31 per individual; tsum[b] = sum of
-// signs of bucket b over all used individuals.  out: m rows of `ld` floats.
-cudaError_t launch_sketch_scatter(const PanelView& p, const uint64_t* rec_rows, int64_t m,
-                                  IndivSel sel, const uint32_t* packed, const int32_t* tsum,
-                                  uint32_t d, RecStats st, float* out, uint64_t ld,
-                                  cudaStream_t stream);
+// CountSketch, step 1 (once per panel, sketch dimension and individual set):
+// rewrite every panel row in bucket-major individual order, perm[p] = FAM
+// index of the individual at permuted position p.  out: n_snp rows of
+// out_pitch_words 32-bit words (16 codes each).
+cudaError_t launch_sketch_permute(const PanelView& p, const int32_t* perm, uint64_t n_used, uint32_t* out,
+                                  uint64_t out_pitch_words, cudaStream_t stream);
+
+// CountSketch, step 2 (per call): per record, run sums over the permuted row,
+// per-SNP moments into st.n/s/q (and q3/q4 when want_moments), standardised
+// and renormalised bucket values.  seg_off: 2d+1 run starts (run k = bucket
+// k/2, sign + for even k); word_seg[w]: run containing position 16w.
+// out: m rows of `ld` floats, or with split = 1 the tensor-core operand form:
+// rows 2r = tf32(v) and 2r+1 = tf32(v - tf32(v)), `ld` floats each.
+cudaError_t launch_sketch_seg(const uint32_t* pp, uint64_t pp_pitch_words, const uint64_t* rec_rows, int64_t m,
+                              uint64_t n_used, const int32_t* seg_off, const int32_t* word_seg, uint32_t d,
+                              RecStats st, int want_moments, int split, float* out, uint64_t ld,
+                              cudaStream_t stream);
+
+// CountSketch band Gram on tcgen05 kind::tf32 over split rows (hi/lo
+// interleaved, `ld` floats per row, ld*4 a multiple of 128) + quadratic
+// bias-correction epilogue (TA = 64, TB = 128 records per tile).
+cudaError_t launch_gram_tf32(const float* ops, uint64_t ld, int64_t m, const Tile* tiles, int64_t n_tiles,
+                             const EpilogueArgs& ep, int maf_aware, int32_t* dbg, int sms, cudaStream_t stream);
 
 // FP32 band Gram of sketched rows + quadratic bias correction epilogue.
 cudaError_t launch_gram_f32(const float* x, uint64_t ld, uint64_t kdim, const Tile* tiles,
                             int64_t n_tiles, const EpilogueArgs& ep, int maf_aware, int sms,
+                            cudaStream_t stream);
+
+// K > 1 annotation contraction from the R tiles a Gram wrote (no atomics, each
+// l2 row owned by one CTA per pass):
+//   by right block:  l2[j, C] += sum over tiles of block, sum_k R[k][j] a[k, C]
+//   by left block:   l2[k, C] += sum over tiles of block, sum_j R[k][j] a[j, C]
+// ptr/idx: CSR lists of tile indices per right block (by_right) or per left block.
+cudaError_t launch_contract(const float* rtiles, int ta, int tb, const Tile* tiles, const int32_t* ptr,
+                            const int32_t* idx, int32_t nblocks, bool by_right, const EpilogueArgs& ep,
                             cudaStream_t stream);
 
 // Synthetic panel generator (founder mosaic, counter-based RNG).

@@ -167,7 +167,14 @@ __global__ void __launch_bounds__(NT, 1)
                 }
             }
             __syncthreads();
-            contract_tile_smem(Rs, RLD, TA, TB, k0, j0, ep, tid, NT);
+            // K > 1: the masked r2u tile goes to global memory for the banded
+            // annotation contraction (contract.cu)
+            float4* dst = reinterpret_cast<float4*>(ep.rtiles + (size_t)t * TA * TB);
+            for (int q = tid; q < TA * TB / 4; q += NT) {
+                const int e = q * 4, rr = e / TB, cc = e % TB;
+                dst[q] = make_float4(Rs[rr * RLD + cc], Rs[rr * RLD + cc + 1], Rs[rr * RLD + cc + 2],
+                                     Rs[rr * RLD + cc + 3]);
+            }
             __syncthreads();
         }
     }

@@ -1,5 +1,14 @@
-// gram_i8.cu -- INT8-exact band Gram on the 5th-generation tensor cores.
+// gram_tc.cu -- band Gram on the 5th-generation tensor cores (tcgen05), in
+// two operand kinds that share one tile structure:
+//   * INT8-exact form (kind::i8): genotype / mask rows, exact epilogue;
+//   * CountSketch form (kind::tf32): each sketched f32 value v is split as
+//     v = hi + lo with hi = tf32(v), lo = tf32(v - hi), stored as rows 2r (hi)
+//     and 2r+1 (lo); one UMMA then yields hi.hi, hi.lo, lo.hi, lo.lo for every
+//     pair, whose sum is the f32-accurate dot product (the reference's f32
+//     GEMM, src/l2/compute.rs:1897-2079), followed by the quadratic bias
+//     inversion (src/l2/compute.rs:947-998) in f64.
 //
+// INT8-exact form:
 // Operands: for record r, row 2r holds its genotypes G (0/1/2, 0 at missing)
 // and row 2r+1 its non-missing mask M (0/1), one byte per individual, rows of
 // `ld` bytes (a multiple of 128).  One UMMA tile multiplies 128 A rows
@@ -51,11 +60,25 @@ __device__ __forceinline__ int64_t shfl_xor_i64(int64_t v, int mask) {
     return ((int64_t)hi << 32) | (uint32_t)lo;
 }
 
-template <int STAGES>
+// MODE 0: INT8 exact r^2; 1: TF32 sketch, quadratic correction; 2: same, MAF-aware.
+template <int MODE>
+__device__ __forceinline__ double sketch_r2u(float val, int64_t k, int64_t j, const EpilogueArgs& ep) {
+    const double v = (double)val;
+    const double kap = MODE == 2 ? __ldg(ep.kappa + k) + __ldg(ep.kappa + j) : 0.0;
+    const double tilde = v * v * ep.n_inv_sq;
+    const double dm3 = ep.sketch_d - 3.0 - 2.0 * kap;
+    const double disc = dm3 * dm3 + 8.0 * (ep.sketch_d * tilde - 1.0);
+    const double r2 = disc >= 0.0 ? (-dm3 + sqrt(disc)) * 0.25 : 0.0;
+    return r2 * ep.r2u_a + ep.r2u_b;
+}
+
+template <int STAGES, int MODE>
 __global__ void __launch_bounds__(NTHREADS, 1)
-    k_gram_i8(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+    k_gram_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
               int num_kb, const Tile* __restrict__ tiles, int64_t n_tiles, EpilogueArgs ep,
               int32_t* __restrict__ dbg) {
+    // elements per 128-byte stage row: 128 (INT8) or 32 (TF32); TMA x is in elements
+    constexpr int KSTEP = MODE == 0 ? 128 : 32;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     const uint32_t pad = (1024u - (smem_u32(smem_raw) & 1023u)) & 1023u;
     uint8_t* smem = smem_raw + pad;
@@ -113,8 +136,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                         break;
                     }
                     mbar_arrive_expect_tx(&full[stage], A_BYTES + B_BYTES);
-                    tma_load_2d(sA + stage * A_BYTES, &tmA, &full[stage], kb * 128, ya);
-                    tma_load_2d(sB + stage * B_BYTES, &tmB, &full[stage], kb * 128, yb);
+                    tma_load_2d(sA + stage * A_BYTES, &tmA, &full[stage], kb * KSTEP, ya);
+                    tma_load_2d(sB + stage * B_BYTES, &tmB, &full[stage], kb * KSTEP, yb);
                     armed |= 1u << stage;
                     armed_par = (armed_par & ~(1u << stage)) | (phase << stage);
                     if (++stage == STAGES) {
@@ -133,7 +156,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     } else if (warp == 1) {
         // ------------------------------------------------ UMMA issuer
         if (elect_one_sync()) {
-            const uint32_t idesc = idesc_i8(128, 256);
+            const uint32_t idesc = MODE == 0 ? idesc_i8(128, 256) : idesc_tf32(128, 256);
             int stage = 0;
             uint32_t phase = 0;
             int acc = 0;
@@ -157,8 +180,12 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                     const uint32_t b_addr = smem_u32(sB + stage * B_BYTES);
 #pragma unroll
                     for (int kk = 0; kk < 4; kk++) {
-                        umma_i8(d_tmem, sdesc_k_sw128(a_addr + kk * 32), sdesc_k_sw128(b_addr + kk * 32),
-                                idesc, (kb | kk) != 0 ? 1u : 0u);
+                        if (MODE == 0)
+                            umma_i8(d_tmem, sdesc_k_sw128(a_addr + kk * 32), sdesc_k_sw128(b_addr + kk * 32),
+                                    idesc, (kb | kk) != 0 ? 1u : 0u);
+                        else
+                            umma_tf32(d_tmem, sdesc_k_sw128(a_addr + kk * 32), sdesc_k_sw128(b_addr + kk * 32),
+                                      idesc, (kb | kk) != 0 ? 1u : 0u);
                     }
                     issued = true;
                     umma_commit(&empty[stage]);
@@ -196,9 +223,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             const int64_t k0 = (int64_t)tl.a_blk * TA, j0 = (int64_t)tl.b_blk * TB;
             const int64_t k = k0 + (row >> 1);
             const bool kval = k < m;
-            const int64_t nk = kval ? __ldg(ep.n + k) : 0;
-            const int64_t sk = kval ? __ldg(ep.s + k) : 0;
-            const double qk = kval ? __ldg(ep.qinv + k) : 0.0;
+            const int64_t nk = (MODE == 0 && kval) ? __ldg(ep.n + k) : 0;
+            const int64_t sk = (MODE == 0 && kval) ? __ldg(ep.s + k) : 0;
+            const double qk = (MODE == 0 && kval) ? __ldg(ep.qinv + k) : 0.0;
             const double ak = (kval && ep.K == 1) ? __ldg(ep.aeff + k) : 0.0;
 
             // One thread does the bounded wait; the decision is made uniform for
@@ -231,27 +258,41 @@ __global__ void __launch_bounds__(NTHREADS, 1)
 #pragma unroll
                 for (int p = 0; p < 32; p += 2) {
                     const int64_t ja = j0 + c * 32 + p, jb = ja + 1;
-                    const int64_t nja = ja < m ? __ldg(ep.n + ja) : 0, sja = ja < m ? __ldg(ep.s + ja) : 0;
-                    const int64_t njb = jb < m ? __ldg(ep.n + jb) : 0, sjb = jb < m ? __ldg(ep.s + jb) : 0;
-                    const int64_t ga = (int32_t)v[2 * p], ma = (int32_t)v[2 * p + 1];
-                    const int64_t gb = (int32_t)v[2 * p + 2], mb = (int32_t)v[2 * p + 3];
-                    int64_t Pa, Pb;
-                    if (grow) {
-                        Pa = nk * (nja * ga - sja * ma);   // n_k n_j GG - n_k s_j GM
-                        Pb = nk * (njb * gb - sjb * mb);
-                    } else {
-                        Pa = sk * (sja * ma - nja * ga);   // s_k s_j MM - s_k n_j MG
-                        Pb = sk * (sjb * mb - njb * gb);
-                    }
-                    const int64_t send = grow ? Pb : Pa;
-                    const int64_t recv = shfl_xor_i64(send, 1);
-                    const int64_t X = (grow ? Pa : Pb) + recv;
-                    const int64_t j = grow ? ja : jb;
+                    int64_t j;
+                    bool valid;
                     double r2u = 0.0;
-                    const bool valid = kval && pair_in_band(k, j, m, ep.left);
-                    if (valid) {
-                        const double r = (double)X * qk * __ldg(ep.qinv + j);
-                        r2u = r * r * ep.r2u_a + ep.r2u_b;
+                    if (MODE == 0) {
+                        const int64_t nja = ja < m ? __ldg(ep.n + ja) : 0, sja = ja < m ? __ldg(ep.s + ja) : 0;
+                        const int64_t njb = jb < m ? __ldg(ep.n + jb) : 0, sjb = jb < m ? __ldg(ep.s + jb) : 0;
+                        const int64_t ga = (int32_t)v[2 * p], ma = (int32_t)v[2 * p + 1];
+                        const int64_t gb = (int32_t)v[2 * p + 2], mb = (int32_t)v[2 * p + 3];
+                        int64_t Pa, Pb;
+                        if (grow) {
+                            Pa = nk * (nja * ga - sja * ma);   // n_k n_j GG - n_k s_j GM
+                            Pb = nk * (njb * gb - sjb * mb);
+                        } else {
+                            Pa = sk * (sja * ma - nja * ga);   // s_k s_j MM - s_k n_j MG
+                            Pb = sk * (sjb * mb - njb * gb);
+                        }
+                        const int64_t send = grow ? Pb : Pa;
+                        const int64_t recv = shfl_xor_i64(send, 1);
+                        const int64_t X = (grow ? Pa : Pb) + recv;
+                        j = grow ? ja : jb;
+                        valid = kval && pair_in_band(k, j, m, ep.left);
+                        if (valid) {
+                            const double r = (double)X * qk * __ldg(ep.qinv + j);
+                            r2u = r * r * ep.r2u_a + ep.r2u_b;
+                        }
+                    } else {
+                        // this row's (hi or lo)_k times (hi_j + lo_j); the partner lane holds the other half
+                        const float pa = __uint_as_float(v[2 * p]) + __uint_as_float(v[2 * p + 1]);
+                        const float pb = __uint_as_float(v[2 * p + 2]) + __uint_as_float(v[2 * p + 3]);
+                        const float send = grow ? pb : pa;
+                        const float recv = __shfl_xor_sync(0xFFFFFFFFu, send, 1);
+                        const float val = (grow ? pa : pb) + recv;
+                        j = grow ? ja : jb;
+                        valid = kval && pair_in_band(k, j, m, ep.left);
+                        if (valid) r2u = sketch_r2u<MODE>(val, k, j, ep);
                     }
                     if (ep.K == 1) {
                         if (valid) rsum += r2u * __ldg(ep.aeff + j);
@@ -276,8 +317,15 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                 if (j < m && cs != 0.0) atomicAdd(ep.l2 + j, cs);
                 named_bar_sync(1, 128);
             } else {
+                // K > 1: the masked r2u tile goes to global memory for the
+                // banded annotation contraction (contract.cu)
                 named_bar_sync(1, 128);
-                contract_tile_smem(Rs, RLD, TA, TB, k0, j0, ep, et, 128);
+                float4* dst = reinterpret_cast<float4*>(ep.rtiles + (size_t)t * TA * TB);
+                for (int q = et; q < TA * TB / 4; q += 128) {
+                    const int e = q * 4, rr = e / TB, cc = e % TB;
+                    dst[q] = make_float4(Rs[rr * RLD + cc], Rs[rr * RLD + cc + 1], Rs[rr * RLD + cc + 2],
+                                         Rs[rr * RLD + cc + 3]);
+                }
                 named_bar_sync(1, 128);
             }
             if (++acc == 2) {
@@ -312,51 +360,65 @@ static PFN_encodeTiled get_encode() {
     return fn;
 }
 
-static bool make_map(CUtensorMap* map, const uint8_t* base, uint64_t ld, uint64_t rows,
-                     uint32_t box_rows) {
+static bool make_map(CUtensorMap* map, const void* base, CUtensorMapDataType dt, uint64_t ld_elems,
+                     uint64_t elem_bytes, uint64_t rows, uint32_t box_rows) {
     PFN_encodeTiled enc = get_encode();
     if (!enc) return false;
-    cuuint64_t dims[2] = {ld, rows};
-    cuuint64_t strides[1] = {ld};
-    cuuint32_t box[2] = {128, box_rows};
+    cuuint64_t dims[2] = {ld_elems, rows};
+    cuuint64_t strides[1] = {ld_elems * elem_bytes};
+    cuuint32_t box[2] = {(cuuint32_t)(128 / elem_bytes), box_rows};  // 128-byte rows
     cuuint32_t estr[2] = {1, 1};
-    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<uint8_t*>(base), dims, strides,
-                     box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    CUresult r = enc(map, dt, 2, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS;
 }
 
-cudaError_t launch_gram_i8(const uint8_t* ops, uint64_t ld, int64_t m, const Tile* tiles,
-                           int64_t n_tiles, const EpilogueArgs& ep, int32_t* dbg, int sms,
-                           cudaStream_t stream) {
+template <int MODE>
+static cudaError_t launch_tc(const void* ops, CUtensorMapDataType dt, uint64_t elem_bytes, uint64_t ld_elems,
+                             int64_t m, const Tile* tiles, int64_t n_tiles, const EpilogueArgs& ep, int32_t* dbg,
+                             int sms, cudaStream_t stream) {
     if (n_tiles <= 0) return cudaSuccess;
-    if (ld % 128 != 0 || (reinterpret_cast<uintptr_t>(ops) & 15) != 0) return cudaErrorInvalidValue;
+    if ((ld_elems * elem_bytes) % 128 != 0 || (reinterpret_cast<uintptr_t>(ops) & 15) != 0)
+        return cudaErrorInvalidValue;
     CUtensorMap tmA, tmB;
     const uint64_t rows = (uint64_t)(2 * m);
-    if (!make_map(&tmA, ops, ld, rows, 2 * TA) || !make_map(&tmB, ops, ld, rows, 2 * TB))
+    if (!make_map(&tmA, ops, dt, ld_elems, elem_bytes, rows, 2 * TA) ||
+        !make_map(&tmB, ops, dt, ld_elems, elem_bytes, rows, 2 * TB))
         return cudaErrorInvalidValue;
-    const int num_kb = (int)(ld / 128);
+    const int num_kb = (int)(ld_elems * elem_bytes / 128);
     const size_t ctrl = 8 * (2 * 4 + 2 + 2 + 1 + 1);  // barriers + tmem slot (upper bound)
     const size_t cbytes = sizeof(double) * 4 * TB;
     int64_t grid = n_tiles < sms ? n_tiles : sms;
     if (dbg) grid = 1;
     if (ep.K == 1) {
         const size_t smem = 1024 + 4 * (size_t)(A_BYTES + B_BYTES) + ctrl + cbytes;
-        cudaError_t e = cudaFuncSetAttribute(k_gram_i8<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaError_t e = cudaFuncSetAttribute(k_gram_tc<4, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
         if (e != cudaSuccess) return e;
-        k_gram_i8<4><<<(unsigned)grid, NTHREADS, smem, stream>>>(tmA, tmB, num_kb, tiles,
-                                                                 dbg ? 1 : n_tiles, ep, dbg);
+        k_gram_tc<4, MODE><<<(unsigned)grid, NTHREADS, smem, stream>>>(tmA, tmB, num_kb, tiles,
+                                                                       dbg ? 1 : n_tiles, ep, dbg);
     } else {
-        const size_t smem = 1024 + 3 * (size_t)(A_BYTES + B_BYTES) + ctrl + cbytes +
-                            sizeof(float) * TA * RLD;
-        cudaError_t e = cudaFuncSetAttribute(k_gram_i8<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        const size_t smem = 1024 + 3 * (size_t)(A_BYTES + B_BYTES) + ctrl + cbytes + sizeof(float) * TA * RLD;
+        cudaError_t e = cudaFuncSetAttribute(k_gram_tc<3, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
         if (e != cudaSuccess) return e;
-        k_gram_i8<3><<<(unsigned)grid, NTHREADS, smem, stream>>>(tmA, tmB, num_kb, tiles,
-                                                                 dbg ? 1 : n_tiles, ep, dbg);
+        k_gram_tc<3, MODE><<<(unsigned)grid, NTHREADS, smem, stream>>>(tmA, tmB, num_kb, tiles,
+                                                                       dbg ? 1 : n_tiles, ep, dbg);
     }
     return cudaGetLastError();
+}
+
+cudaError_t launch_gram_i8(const uint8_t* ops, uint64_t ld, int64_t m, const Tile* tiles, int64_t n_tiles,
+                           const EpilogueArgs& ep, int32_t* dbg, int sms, cudaStream_t stream) {
+    return launch_tc<0>(ops, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, ld, m, tiles, n_tiles, ep, dbg, sms, stream);
+}
+
+cudaError_t launch_gram_tf32(const float* ops, uint64_t ld, int64_t m, const Tile* tiles, int64_t n_tiles,
+                             const EpilogueArgs& ep, int maf_aware, int32_t* dbg, int sms, cudaStream_t stream) {
+    if (maf_aware)
+        return launch_tc<2>(ops, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, ld, m, tiles, n_tiles, ep, dbg, sms, stream);
+    return launch_tc<1>(ops, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, ld, m, tiles, n_tiles, ep, dbg, sms, stream);
 }
 
 }  // namespace ldsc

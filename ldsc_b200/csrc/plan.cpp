@@ -142,4 +142,28 @@ void countsketch_hash(uint64_t n, uint32_t d, uint64_t seed, uint32_t* bucket, f
     for (uint64_t i = 0; i < n; i++) sign[i] = r.coin() ? 1.0f : -1.0f;
 }
 
+SketchOrder sketch_order(uint64_t n_used, uint32_t d, const uint32_t* bucket, const float* sign,
+                         const int64_t* keep) {
+    SketchOrder o;
+    const uint32_t nseg = 2 * d;
+    o.seg_off.assign(nseg + 1, 0);
+    for (uint64_t i = 0; i < n_used; i++) o.seg_off[2 * bucket[i] + (sign[i] < 0 ? 1 : 0) + 1]++;
+    for (uint32_t k = 0; k < nseg; k++) o.seg_off[k + 1] += o.seg_off[k];
+    std::vector<int32_t> fill(o.seg_off.begin(), o.seg_off.end() - 1);
+    o.perm.assign(n_used, 0);
+    for (uint64_t i = 0; i < n_used; i++) {
+        const uint32_t k = 2 * bucket[i] + (sign[i] < 0 ? 1 : 0);
+        o.perm[fill[k]++] = (int32_t)(keep ? keep[i] : (int64_t)i);
+    }
+    const uint64_t words = (n_used + 15) / 16;
+    o.word_seg.assign(words + 4, (int32_t)nseg);
+    uint32_t k = 0;
+    for (uint64_t w = 0; w < words; w++) {
+        const int64_t pos = (int64_t)w * 16;
+        while (k + 1 < nseg + 1 && o.seg_off[k + 1] <= pos) k++;
+        o.word_seg[w] = (int32_t)k;
+    }
+    return o;
+}
+
 }  // namespace ldsc

@@ -40,4 +40,14 @@ std::vector<Tile> band_tiles(const std::vector<int64_t>& left, int ta, int tb);
 // (src/l2/compute.rs:179-184): n bucket draws u32(..d), then n bool draws.
 void countsketch_hash(uint64_t n, uint32_t d, uint64_t seed, uint32_t* bucket, float* sign);
 
+// Bucket-major order of the used individuals for the permuted-panel sketch:
+// runs k = 2*bucket + (sign < 0), stable in individual order.
+struct SketchOrder {
+    std::vector<int32_t> perm;      // FAM index at each permuted position
+    std::vector<int32_t> seg_off;   // 2d + 1 run starts
+    std::vector<int32_t> word_seg;  // run containing position 16 w
+};
+SketchOrder sketch_order(uint64_t n_used, uint32_t d, const uint32_t* bucket, const float* sign,
+                         const int64_t* keep);
+
 }  // namespace ldsc

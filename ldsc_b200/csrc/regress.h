@@ -1,0 +1,66 @@
+// regress.h -- device structures of the batched LD-score regressions.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace ldsc {
+
+enum { REG_HSQ = 0, REG_GENCOV = 1 };
+enum { REG_Y_DIRECT = 0, REG_Y_SQUARE = 1, REG_Y_PRODUCT = 2 };
+
+// One regression: y ~ [x0 = Nx * ld / nbar, 1] with weights of its kind.
+struct RegJob {
+    const double* ya;   // y source (device)
+    const double* yb;   // second factor for REG_Y_PRODUCT
+    int32_t ymode;      // y = ya | max(ya^2, 0) | ya * yb
+    int32_t kind;       // REG_HSQ or REG_GENCOV
+    const double* n1;   // per-SNP sample sizes (device) or null
+    const double* n2;
+    double n1s, n2s;    // scalar sample sizes when n1 / n2 are null
+    int32_t fixed;      // intercept constrained
+    double fixed_int;
+    int32_t hsq1, hsq2; // REG_GENCOV: job indices of the two h2 fits
+};
+
+// Running parameters of a job between passes.
+struct RegState {
+    double nbar, mean_y;
+    double slope;       // hsq (REG_HSQ) or rho_g (REG_GENCOV) used by the weights
+    double intercept;
+    double h1, h2, int_h1, int_h2;  // REG_GENCOV weight constants
+};
+
+struct RegOut {
+    double est[2], se[2], cov[3];   // coefficient on x0 and intercept; cov = (00, 01, 11)
+    double tot, tot_se;             // h2 or genetic covariance: M * est0 / nbar
+    double intercept, intercept_se;
+    double nbar, mean_y, median_y;
+};
+
+struct RgPairIdx {
+    int32_t hsq1, hsq2, gencov;
+};
+
+struct RgOut {
+    double rg, rg_se;
+    double gencov, gencov_se, gencov_intercept, gencov_intercept_se;
+    double h2_1, h2_1_se, h2_2, h2_2_se;
+    double mean_z1z2;
+};
+
+// Aggregate pass, two IRWLS updates and the block jackknife for all jobs.
+// outs[j] receives job j's result; ref_outs holds the h2 results that
+// REG_GENCOV jobs refer to by index.  part: njobs * nb * 5 doubles of
+// scratch; tot_delete (optional): njobs * nb.
+cudaError_t launch_regressions(const RegJob* jobs, RegState* states, RegOut* outs, const RegOut* ref_outs,
+                               double* part, double* tot_delete, const double* ld, const double* wld, uint64_t n,
+                               int nb, double m, int njobs, cudaStream_t s);
+
+cudaError_t launch_rg_finish(const RgPairIdx* pairs, const RegOut* outs, const double* tot_delete, int nb,
+                             RgOut* res, int npairs, cudaStream_t s);
+
+// k-th smallest y of each job (exact), out[job].
+cudaError_t launch_select(const RegJob* jobs, uint64_t n, uint64_t rank, double* out, int njobs, cudaStream_t s);
+
+}  // namespace ldsc

@@ -82,8 +82,8 @@ __device__ __forceinline__ void tma_prefetch_desc(const void* tmap) {
 }
 
 // 2D tiled load global -> shared, completion counted on `bar` in bytes.
-// x is the innermost coordinate (bytes for the uint8 maps used here; the
-// callers keep it a multiple of 128).
+// x is the innermost coordinate in elements of the map's type; callers keep
+// x * element size a multiple of 128 bytes.
 __device__ __forceinline__ void tma_load_2d(void* smem_dst, const void* tmap, uint64_t* bar,
                                             int32_t x, int32_t y) {
     asm volatile(
@@ -132,6 +132,19 @@ __device__ __forceinline__ void umma_i8(uint32_t d_tmem, uint64_t a_desc, uint64
         : "memory");
 }
 
+// D[tmem] (+)= A[smem] * B[smem]^T, kind::tf32 (f32 accumulate), one CTA.
+__device__ __forceinline__ void umma_tf32(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc,
+                                          uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t"
+        ".reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t"
+        "}\n" ::"r"(d_tmem),
+        "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
 // Arrive on `bar` once all previously issued tcgen05.mma of this thread complete.
 __device__ __forceinline__ void umma_commit(uint64_t* bar) {
     asm volatile(
@@ -160,6 +173,23 @@ __host__ __device__ constexpr uint32_t idesc_i8(uint32_t M, uint32_t N) {
            | (0u << 10)           // b_format = unsigned 8-bit
            | ((N >> 3) << 17)     // n_dim
            | ((M >> 4) << 24);    // m_dim
+}
+
+// Instruction descriptor, kind::tf32: TF32 A and B, f32 accumulator, both
+// K-major, M x N tile.
+__host__ __device__ constexpr uint32_t idesc_tf32(uint32_t M, uint32_t N) {
+    return (1u << 4)              // c_format = F32
+           | (2u << 7)            // a_format = TF32
+           | (2u << 10)           // b_format = TF32
+           | ((N >> 3) << 17)     // n_dim
+           | ((M >> 4) << 24);    // m_dim
+}
+
+// Round an f32 to TF32 (round to nearest, ties away), low 13 bits cleared.
+__device__ __forceinline__ float to_tf32(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
 }
 
 // 32 lanes x 32 bits, 64 consecutive columns per thread.

@@ -232,3 +232,35 @@ def partitioned_annot(m: int, seed: int = 21, n_binary: int = 80, n_cont: int = 
     for _ in range(n_cont):
         cols.append(np.clip(rng.standard_normal(m), -3.0, 3.0))
     return np.asfortranarray(np.stack(cols, axis=1))
+
+
+def gwas_traits(l2: np.ndarray, m_snps: float, n_traits: int, seed: int = 31):
+    """Synthetic GWAS chi^2 statistics over LD scores l2: per trait
+    h2 ~ U(0.05, 0.5), N log-uniform in [1e4, 5e5], z_j = sqrt(N h2 l2_j / M) b_j
+    + e_j with b_j, e_j ~ N(0, 1), chi2 = z^2 (so E[chi2] = 1 + N h2 l2 / M).
+    Returns (chi2 [T x M], N [T], h2 [T])."""
+    rng = np.random.default_rng(seed)
+    h2 = rng.uniform(0.05, 0.5, n_traits)
+    n = np.exp(rng.uniform(np.log(1e4), np.log(5e5), n_traits))
+    lm = np.maximum(l2, 0.0)[None, :]
+    z = np.sqrt(n[:, None] * h2[:, None] * lm / m_snps) * rng.standard_normal((n_traits, len(l2))) \
+        + rng.standard_normal((n_traits, len(l2)))
+    return z * z, n, h2
+
+
+def gwas_pairs(l2: np.ndarray, m_snps: float, n_pairs: int, seed: int = 32):
+    """Synthetic z-score pairs with genetic correlation rg ~ U(-0.8, 0.8):
+    z_t = sqrt(N_t h_t l2 / M) b_t + e_t with corr(b_1, b_2) = rg.
+    Returns (z1, z2, n1, n2, rg)."""
+    rng = np.random.default_rng(seed)
+    h1, h2 = rng.uniform(0.05, 0.5, n_pairs), rng.uniform(0.05, 0.5, n_pairs)
+    n1 = np.exp(rng.uniform(np.log(1e4), np.log(5e5), n_pairs))
+    n2 = np.exp(rng.uniform(np.log(1e4), np.log(5e5), n_pairs))
+    rg = rng.uniform(-0.8, 0.8, n_pairs)
+    m = len(l2)
+    b1 = rng.standard_normal((n_pairs, m))
+    b2 = rg[:, None] * b1 + np.sqrt(1 - rg[:, None] ** 2) * rng.standard_normal((n_pairs, m))
+    lm = np.maximum(l2, 0.0)[None, :]
+    z1 = np.sqrt(n1[:, None] * h1[:, None] * lm / m_snps) * b1 + rng.standard_normal((n_pairs, m))
+    z2 = np.sqrt(n2[:, None] * h2[:, None] * lm / m_snps) * b2 + rng.standard_normal((n_pairs, m))
+    return z1, z2, n1, n2, rg

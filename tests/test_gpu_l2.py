@@ -230,3 +230,52 @@ def test_small_config_parity(ctx, cfg_small, masking):
         assert relerr(l2, ref) < EXACT_TOL
         assert perf.n_pairs == npairs
         np.testing.assert_allclose(maf, ref_maf, atol=1e-15)
+
+
+@pytest.mark.parametrize("d", [3, 200, 5000])
+def test_sketch_project_large_panel(ctx, d):
+    """Bucket sums over a 20,000-individual panel with the seed-42 stream
+    (runs shorter and longer than a thread's word range) vs a direct f64
+    scatter; the tolerance is the reference scatter test's (1e-4)."""
+    from ldsc_b200.api import countsketch_hash, sketch_project
+    from ldsc_b200.plink import decode_genotypes
+    spec = synth.PanelSpec(n_indiv=20011, chrom_sizes=[6], chrom_cm=[1.0], founders=30, miss=0.03, seed=8)
+    body = synth.bed_body(spec)
+    panel = ctx.upload(body, spec.n_indiv)
+    bucket, sign = countsketch_hash(spec.n_indiv, d, 42)
+    got = sketch_project(ctx, panel, 0, spec.m, bucket, sign, d)
+    G = decode_genotypes(body, spec.n_indiv)
+    for j in range(spec.m):
+        g = G[j]
+        pres = ~np.isnan(g)
+        mean = g[pres].mean()
+        var = (np.sum(g[pres] ** 2) - pres.sum() * mean * mean) / spec.n_indiv
+        inv = np.float32(1.0 / np.sqrt(var)) if var > 0 else np.float32(0.0)
+        mean32 = np.float32(mean)
+        val = np.where(pres, (np.nan_to_num(g) - float(mean32)) * float(inv), 0.0)
+        col = np.zeros(d)
+        np.add.at(col, bucket, sign.astype(np.float64) * val)
+        nrm = np.sum(col ** 2)
+        if nrm > 0:
+            col *= np.sqrt(spec.n_indiv / nrm)
+        diff = np.abs(got[j] - col)
+        assert np.all((diff < 1e-4) | (diff / np.maximum(np.abs(col), 1e-6) < 1e-4)), (j, diff.max())
+
+
+@pytest.mark.parametrize("precision", ["fp64", "int8"])
+def test_many_annotations_match_oracle(ctx, small, small_panel, precision):
+    """K = 33 columns: the contraction splits columns unevenly between threads."""
+    from ldsc_b200.api import WindowMode, run_l2
+    from oracle import OracleL2Args, oracle_l2
+    m = len(small["chr"])
+    rng = np.random.default_rng(33)
+    A = np.asfortranarray(np.concatenate([np.ones((m, 1)), (rng.random((m, 20)) < 0.2).astype(float),
+                                          np.clip(rng.standard_normal((m, 12)), -3, 3)], axis=1))
+    n = int(small["n_indiv"])
+    ref, _, _, _ = oracle_l2(OracleL2Args(bed_body=small["body"], n_file_indiv=n, chr=small["chr"],
+                                          cm=small["cm"], bp=small["bp"], chunk_c=50, annot=A))
+    snps = table(small["chr"], small["cm"], small["bp"])
+    l2, _, _ = run_l2(ctx, snps, small_panel, WindowMode.Cm(1.0), 50, annot=A, precision=precision,
+                      yes_really=True)
+    scale = np.maximum(np.abs(ref).max(axis=0, keepdims=True), 1.0)
+    assert np.max(np.abs(l2 - ref) / scale) < ANNOT_TOL
