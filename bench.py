@@ -404,8 +404,10 @@ def main():
         barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
+        e2e_perf = []
         for _ in range(args.steps):
-            l2_from_bed_bytes(ctx, bnp, spec.n_indiv, snps, wm, 200, precision="int8", snp_level_masking=True)
+            e2e_perf.append(l2_from_bed_bytes(ctx, bnp, spec.n_indiv, snps, wm, 200, precision="int8",
+                                              snp_level_masking=True)[2])
         torch.cuda.synchronize()
         te = time.perf_counter() - t0
         if world > 1:
@@ -414,7 +416,10 @@ def main():
             te = float(tt.item())
         e2e = {"value": pairs_all * args.steps / te, "unit": "r2 pairs/s", "h2d_bytes_per_step": int(bnp.size),
                "d2h_bytes_per_step": int(16 * m), "ms_per_step": 1e3 * te / args.steps,
-               "api": "ldsc_l2_from_bed (validate + upload + compute + download)"}
+               "api": "ldsc_l2_from_bed (validate + upload + compute + download)",
+               "h2d_ms_median": 1e3 * float(np.median([p.bed_read_secs for p in e2e_perf])),
+               "h2d_gbs": bnp.size / 1e9 / float(np.median([p.bed_read_secs for p in e2e_perf])),
+               "device_ms_median": float(np.median([p.device_ms for p in e2e_perf]))}
 
     # ---- roofline of the dominant kernel (INT8 band Gram) ----
     hbm, bf16, src = measured_peaks()

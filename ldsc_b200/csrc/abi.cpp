@@ -18,6 +18,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
 #include <atomic>
 #include <mutex>
 #include <string>
@@ -65,6 +66,7 @@ struct ldsc_ctx {
     int sms = 148;
     cudaStream_t own = nullptr;
     cudaStream_t stream = nullptr;
+    cudaStream_t copy = nullptr;  // host-to-device BED stream of ldsc_l2_from_bed
     std::mutex mu;
     std::string last_error;
     uint64_t kernels = 0;
@@ -78,6 +80,10 @@ struct ldsc_ctx {
     DevBuf rg_jobs, rg_states, rg_outs, rg_part, rg_tdel, rg_y, rg_y2, rg_n, rg_ld, rg_wld, rg_sel, rg_pairs, rg_res;
     uint64_t sk_panel = 0, sk_n = 0, sk_key = 0, sk_pitch_words = 0;
     uint32_t sk_d = 0;
+    // whole-file entry: staged file rows, the pitched panel, per-chunk events
+    DevBuf bed_stage, bed_rows;
+    std::vector<cudaEvent_t> feed_ev;
+    cudaEvent_t feed_t0 = nullptr, feed_t1 = nullptr, feed_go = nullptr, up_ev = nullptr;
 };
 
 struct ldsc_panel {
@@ -127,7 +133,9 @@ int ldsc_ctx_create(int device, uint32_t flags, ldsc_ctx** out) {
     ldsc_ctx* c = new ldsc_ctx();
     c->device = device;
     c->sms = prop.multiProcessorCount;
-    if (cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess) {
+    if (cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking) != cudaSuccess) {
+        if (c->own) cudaStreamDestroy(c->own);
         delete c;
         return LDSC_E_CUDA;
     }
@@ -149,8 +157,13 @@ int ldsc_ctx_destroy(ldsc_ctx* ctx) {
                       &ctx->rtiles, &ctx->cptr_r, &ctx->cidx_r, &ctx->cptr_l, &ctx->cidx_l,
                       &ctx->rg_jobs, &ctx->rg_states, &ctx->rg_outs, &ctx->rg_part, &ctx->rg_tdel,
                       &ctx->rg_y, &ctx->rg_y2, &ctx->rg_n, &ctx->rg_ld, &ctx->rg_wld, &ctx->rg_sel,
-                      &ctx->rg_pairs, &ctx->rg_res};
+                      &ctx->rg_pairs, &ctx->rg_res, &ctx->bed_stage, &ctx->bed_rows};
+    cudaStreamSynchronize(ctx->copy);
     for (DevBuf* b : bufs) b->release();
+    for (cudaEvent_t e : ctx->feed_ev) cudaEventDestroy(e);
+    for (cudaEvent_t e : {ctx->feed_t0, ctx->feed_t1, ctx->feed_go, ctx->up_ev})
+        if (e) cudaEventDestroy(e);
+    if (ctx->copy) cudaStreamDestroy(ctx->copy);
     if (ctx->own) cudaStreamDestroy(ctx->own);
     delete ctx;
     return LDSC_OK;
@@ -363,8 +376,87 @@ int sketch_prepare(ldsc_ctx* ctx, const ldsc_panel* panel, uint64_t n_used, uint
     return LDSC_OK;
 }
 
+// Streams a BED body from host memory into the pitched panel: every chunk's
+// copy is queued at once on the context's copy stream, and issue(c) makes the
+// compute stream wait for chunk c and re-pitch it, so decoding chunk c
+// overlaps the copies of the chunks after it.
+struct RowFeed {
+    ldsc_ctx* ctx = nullptr;
+    const uint8_t* host = nullptr;  // file body (after the 3 magic bytes)
+    uint64_t bpr = 0, pitch = 0, rows = 0, per = 0;
+    int nchunks = 0, issued = 0;
+    uint8_t* dst = nullptr;
+
+    bool started = false;
+
+    uint64_t row_end(int c) const { return std::min<uint64_t>(rows, (uint64_t)(c + 1) * per); }
+    // buffers and events; the panel's rows pointer is valid after this
+    int prepare() {
+        ldsc_ctx* c = ctx;
+        per = std::max<uint64_t>(1, (64ull << 20) / bpr);
+        nchunks = (int)((rows + per - 1) / per);
+        while ((int)c->feed_ev.size() < nchunks) {
+            cudaEvent_t e;
+            CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            c->feed_ev.push_back(e);
+        }
+        if (!c->feed_t0) CK(cudaEventCreate(&c->feed_t0));
+        if (!c->feed_t1) CK(cudaEventCreate(&c->feed_t1));
+        if (!c->feed_go) CK(cudaEventCreateWithFlags(&c->feed_go, cudaEventDisableTiming));
+        if (!c->up_ev) CK(cudaEventCreateWithFlags(&c->up_ev, cudaEventDisableTiming));
+        CK(c->bed_stage.ensure(bpr * rows));
+        CK(c->bed_rows.ensure(pitch * rows));
+        dst = c->bed_rows.as<uint8_t>();
+        return LDSC_OK;
+    }
+    // queue every chunk's copy (after the small uploads already on the compute
+    // stream, so those are not held behind the file)
+    int start(cudaStream_t s) {
+        ldsc_ctx* c = ctx;
+        if (started) return LDSC_OK;
+        started = true;
+        // the staging buffer may still be read by earlier work on the compute stream
+        CK(cudaEventRecord(c->feed_go, s));
+        CK(cudaStreamWaitEvent(c->copy, c->feed_go, 0));
+        CK(cudaEventRecord(c->feed_t0, c->copy));
+        for (int k = 0; k < nchunks; k++) {
+            const uint64_t r0 = (uint64_t)k * per, r1 = row_end(k);
+            CK(cudaMemcpyAsync(c->bed_stage.as<uint8_t>() + r0 * bpr, host + r0 * bpr, (r1 - r0) * bpr,
+                               cudaMemcpyHostToDevice, c->copy));
+            CK(cudaEventRecord(c->feed_ev[k], c->copy));
+        }
+        CK(cudaEventRecord(c->feed_t1, c->copy));
+        return LDSC_OK;
+    }
+    int issue_until(int k_end, cudaStream_t s) {  // chunks [issued, k_end)
+        ldsc_ctx* c = ctx;
+        if (!started) {
+            int rc = start(s);
+            if (rc != LDSC_OK) return rc;
+        }
+        for (; issued < std::min(k_end, nchunks); issued++) {
+            CK(cudaStreamWaitEvent(s, c->feed_ev[issued], 0));
+            CK(launch_repitch(c->bed_stage.as<uint8_t>(), bpr, dst, pitch, (uint64_t)issued * per, row_end(issued),
+                              s));
+            c->kernels++;
+        }
+        return LDSC_OK;
+    }
+    int issue_all(cudaStream_t s) { return issue_until(nchunks, s); }
+    double upload_secs() const {
+        float t = 0.f;
+        if (!started) return 0.0;
+        if (cudaEventSynchronize(ctx->feed_t1) != cudaSuccess ||
+            cudaEventElapsedTime(&t, ctx->feed_t0, ctx->feed_t1) != cudaSuccess) {
+            cudaGetLastError();
+            return 0.0;
+        }
+        return t / 1e3;
+    }
+};
+
 int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double* l2_out, double* maf_out,
-           ldsc_perf* perf, double upload_secs) {
+           ldsc_perf* perf, double upload_secs, RowFeed* feed = nullptr) {
     const auto t_wall0 = std::chrono::steady_clock::now();
     const int64_t m = (int64_t)a->n_snp;
     const uint64_t n_file = panel->n_indiv;
@@ -445,9 +537,24 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
     if (a->bed_idx) CK(ctx->recrows.ensure(8 * nmom));
     if (a->keep_iids) CK(ctx->keep.ensure(8 * a->n_keep));
 
-    if (a->annot) CK(cudaMemcpyAsync(ctx->annot.p, a->annot, 8 * nmom * K, cudaMemcpyHostToDevice, s));
-    if (a->bed_idx) CK(cudaMemcpyAsync(ctx->recrows.p, a->bed_idx, 8 * nmom, cudaMemcpyHostToDevice, s));
-    if (a->keep_iids) CK(cudaMemcpyAsync(ctx->keep.p, a->keep_iids, 8 * a->n_keep, cudaMemcpyHostToDevice, s));
+    // Host-to-device uploads.  With a streamed file they go through the copy
+    // stream, ahead of the file's chunks: a copy issued on the compute stream
+    // leaves that stream's next operations queued on the copy engine, behind
+    // the whole file.  join_up() makes the compute stream wait for them.
+    cudaStream_t up = feed ? ctx->copy : s;
+    auto join_up = [&]() -> int {
+        if (up == s) return LDSC_OK;
+        CK(cudaEventRecord(ctx->up_ev, up));
+        CK(cudaStreamWaitEvent(s, ctx->up_ev, 0));
+        return LDSC_OK;
+    };
+    if (feed) {  // the buffers below may still be read by earlier work on the compute stream
+        CK(cudaEventRecord(ctx->up_ev, s));
+        CK(cudaStreamWaitEvent(up, ctx->up_ev, 0));
+    }
+    if (a->annot) CK(cudaMemcpyAsync(ctx->annot.p, a->annot, 8 * nmom * K, cudaMemcpyHostToDevice, up));
+    if (a->bed_idx) CK(cudaMemcpyAsync(ctx->recrows.p, a->bed_idx, 8 * nmom, cudaMemcpyHostToDevice, up));
+    if (a->keep_iids) CK(cudaMemcpyAsync(ctx->keep.p, a->keep_iids, 8 * a->n_keep, cudaMemcpyHostToDevice, up));
     CK(cudaMemsetAsync(ctx->err.p, 0, 16, s));
 
     PanelView pv{panel->rows, panel->n_snp, panel->n_indiv, panel->bpr, panel->pitch};
@@ -466,6 +573,20 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
     st.kappa = maf_aware ? ctx->st_kappa.as<double>() : nullptr;
     st.pq = nullptr;
 
+    // decode in feed chunks when records map to rows in order; else wait for the whole panel
+    bool rows_in_order = true;
+    if (a->bed_idx)
+        for (int64_t i = 1; i < m && rows_in_order; i++) rows_in_order = a->bed_idx[i] >= a->bed_idx[i - 1];
+    const bool chunked = feed && !d && rows_in_order;
+    {
+        int rc = join_up();
+        if (rc != LDSC_OK) return rc;
+    }
+    if (feed && !chunked) {
+        int rc = feed->issue_all(s);
+        if (rc != LDSC_OK) return rc;
+    }
+
     if (d) {
         uint64_t key = 1469598103934665603ull;
         if (a->keep_iids)
@@ -481,87 +602,56 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
         CK(ctx->xsk.ensure((size_t)4 * 2 * nmom * round_up(d, 32)));
     }
 
-    Events ev(s);
-    const int e0 = ev.mark();
-
-    // ---- decode ----
-    const uint64_t ld_i8 = round_up(n_used, 128);
-    const uint64_t ld_sk = round_up(d ? d : 1, 32);  // 128-byte operand rows for TMA
-    int e_sk = -1;
-    if (exact_i8) {
-        CK(ctx->ops.ensure((size_t)2 * nmom * ld_i8));
-        CK(launch_decode_i8(pv, rr, m, sel, ctx->ops.as<uint8_t>(), ld_i8, st, 0, s));
-    } else if (d) {
-        // fused: moments + CountSketch rows in one pass over the permuted panel
-        CK(launch_sketch_seg(ctx->sk_pp.as<uint32_t>(), ctx->sk_pitch_words, rr, m, n_used,
-                             ctx->sk_seg.as<int32_t>(), ctx->sk_wseg.as<int32_t>(), d, st, maf_aware ? 1 : 0, 1,
-                             ctx->xsk.as<float>(), ld_sk, s));
-        e_sk = ev.mark();
-    } else {
-        CK(launch_decode_i8(pv, rr, m, sel, nullptr, 0, st, 0, s));
-    }
-    ctx->kernels++;
-    CK(launch_finalize_stats(m, n_used, st, a->annot ? ctx->annot.as<double>() : nullptr, K, a->has_pq_exp,
-                             a->pq_exp, ctx->aeff.as<double>(), K > 1 ? ctx->aeff32.as<float>() : nullptr,
-                             ctx->l2.as<double>(), s));
-    ctx->kernels++;
-    const uint64_t ld_f64 = round_up(n_used, 128);
-    if (!d && !exact_i8) {
-        CK(ctx->xf64.ensure((size_t)8 * nmom * ld_f64));
-        CK(launch_decode_f64(pv, rr, m, sel, st, ctx->xf64.as<double>(), ld_f64, s));
-        ctx->kernels++;
-    }
-    const int e1 = ev.mark();
-
-    // ---- host plan (runs while the decode kernels execute) ----
+    // ---- host plan: left limits, band tiles, contraction lists ----
     LeftLimits L;
-    std::string perr;
-    if (!left_limits(m, a->chr, a->cm, a->bp, a->window_mode, a->window_size, a->window_snps, a->chunk_size,
-                     a->snp_level_masking != 0, a->global_pass != 0, &L, &perr))
-        return fail(ctx, LDSC_E_INVALID, perr);
-    if (L.any_full && !a->yes_really)
-        std::printf("WARNING: LD window spans the entire chromosome. Use --yes-really to silence this warning.\n");
-    pf.n_pairs = L.n_pairs;
-    std::vector<Tile> tiles = band_tiles(L.left, ta, tb);
-    pf.n_tiles = tiles.size();
-
-    CK(ctx->left.ensure(sizeof(int64_t) * nmom));
-    CK(ctx->tiles.ensure(sizeof(Tile) * (tiles.size() + 1)));
-    CK(cudaMemcpyAsync(ctx->left.p, L.left.data(), 8 * nmom, cudaMemcpyHostToDevice, s));
-    if (!tiles.empty())
-        CK(cudaMemcpyAsync(ctx->tiles.p, tiles.data(), sizeof(Tile) * tiles.size(), cudaMemcpyHostToDevice, s));
-    // K > 1: CSR lists of tiles per right block and per left block for the contraction
+    std::vector<Tile> tiles;
     const int32_t n_right = (int32_t)((m + tb - 1) / tb), n_left = (int32_t)((m + ta - 1) / ta);
-    std::vector<int32_t> ptr_r, idx_r, ptr_l, idx_l;
-    if (K > 1 && !tiles.empty()) {
-        ptr_r.assign(n_right + 1, 0);
-        ptr_l.assign(n_left + 1, 0);
-        for (const Tile& t : tiles) {
-            ptr_r[t.b_blk + 1]++;
-            ptr_l[t.a_blk + 1]++;
+    auto plan = [&]() -> int {
+        std::string perr;
+        if (!left_limits(m, a->chr, a->cm, a->bp, a->window_mode, a->window_size, a->window_snps, a->chunk_size,
+                         a->snp_level_masking != 0, a->global_pass != 0, &L, &perr))
+            return fail(ctx, LDSC_E_INVALID, perr);
+        if (L.any_full && !a->yes_really)
+            std::printf("WARNING: LD window spans the entire chromosome. Use --yes-really to silence this warning.\n");
+        pf.n_pairs = L.n_pairs;
+        tiles = band_tiles(L.left, ta, tb);
+        pf.n_tiles = tiles.size();
+        CK(ctx->left.ensure(sizeof(int64_t) * nmom));
+        CK(ctx->tiles.ensure(sizeof(Tile) * (tiles.size() + 1)));
+        CK(cudaMemcpyAsync(ctx->left.p, L.left.data(), 8 * nmom, cudaMemcpyHostToDevice, up));
+        if (!tiles.empty())
+            CK(cudaMemcpyAsync(ctx->tiles.p, tiles.data(), sizeof(Tile) * tiles.size(), cudaMemcpyHostToDevice, up));
+        // K > 1: CSR lists of tiles per right block and per left block for the contraction
+        if (K > 1 && !tiles.empty()) {
+            std::vector<int32_t> ptr_r(n_right + 1, 0), ptr_l(n_left + 1, 0), idx_r(tiles.size()), idx_l(tiles.size());
+            for (const Tile& t : tiles) {
+                ptr_r[t.b_blk + 1]++;
+                ptr_l[t.a_blk + 1]++;
+            }
+            for (int32_t i = 0; i < n_right; i++) ptr_r[i + 1] += ptr_r[i];
+            for (int32_t i = 0; i < n_left; i++) ptr_l[i + 1] += ptr_l[i];
+            std::vector<int32_t> fr(ptr_r.begin(), ptr_r.end() - 1), fl(ptr_l.begin(), ptr_l.end() - 1);
+            for (int32_t t = 0; t < (int32_t)tiles.size(); t++) {
+                idx_r[fr[tiles[t].b_blk]++] = t;
+                idx_l[fl[tiles[t].a_blk]++] = t;
+            }
+            CK(ctx->rtiles.ensure(sizeof(float) * (size_t)ta * tb * tiles.size()));
+            CK(ctx->cptr_r.ensure(4 * ptr_r.size()));
+            CK(ctx->cidx_r.ensure(4 * idx_r.size()));
+            CK(ctx->cptr_l.ensure(4 * ptr_l.size()));
+            CK(ctx->cidx_l.ensure(4 * idx_l.size()));
+            CK(cudaMemcpyAsync(ctx->cptr_r.p, ptr_r.data(), 4 * ptr_r.size(), cudaMemcpyHostToDevice, up));
+            CK(cudaMemcpyAsync(ctx->cidx_r.p, idx_r.data(), 4 * idx_r.size(), cudaMemcpyHostToDevice, up));
+            CK(cudaMemcpyAsync(ctx->cptr_l.p, ptr_l.data(), 4 * ptr_l.size(), cudaMemcpyHostToDevice, up));
+            CK(cudaMemcpyAsync(ctx->cidx_l.p, idx_l.data(), 4 * idx_l.size(), cudaMemcpyHostToDevice, up));
+            // the host vectors are read by the copies above before they go out of scope
+            CK(cudaStreamSynchronize(up));
         }
-        for (int32_t i = 0; i < n_right; i++) ptr_r[i + 1] += ptr_r[i];
-        for (int32_t i = 0; i < n_left; i++) ptr_l[i + 1] += ptr_l[i];
-        idx_r.resize(tiles.size());
-        idx_l.resize(tiles.size());
-        std::vector<int32_t> fr(ptr_r.begin(), ptr_r.end() - 1), fl(ptr_l.begin(), ptr_l.end() - 1);
-        for (int32_t t = 0; t < (int32_t)tiles.size(); t++) {
-            idx_r[fr[tiles[t].b_blk]++] = t;
-            idx_l[fl[tiles[t].a_blk]++] = t;
-        }
-        CK(ctx->rtiles.ensure(sizeof(float) * (size_t)ta * tb * tiles.size()));
-        CK(ctx->cptr_r.ensure(4 * ptr_r.size()));
-        CK(ctx->cidx_r.ensure(4 * idx_r.size()));
-        CK(ctx->cptr_l.ensure(4 * ptr_l.size()));
-        CK(ctx->cidx_l.ensure(4 * idx_l.size()));
-        CK(cudaMemcpyAsync(ctx->cptr_r.p, ptr_r.data(), 4 * ptr_r.size(), cudaMemcpyHostToDevice, s));
-        CK(cudaMemcpyAsync(ctx->cidx_r.p, idx_r.data(), 4 * idx_r.size(), cudaMemcpyHostToDevice, s));
-        CK(cudaMemcpyAsync(ctx->cptr_l.p, ptr_l.data(), 4 * ptr_l.size(), cudaMemcpyHostToDevice, s));
-        CK(cudaMemcpyAsync(ctx->cidx_l.p, idx_l.data(), 4 * idx_l.size(), cudaMemcpyHostToDevice, s));
-    }
-    // ---- band Gram + epilogue ----
+        return join_up();
+    };
+
+    // ---- epilogue constants ----
     EpilogueArgs ep{};
-    ep.left = ctx->left.as<int64_t>();
     ep.n = st.n;
     ep.s = st.s;
     ep.qinv = st.qinv;
@@ -579,9 +669,112 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
     ep.n_inv_sq = (1.0 / N) * (1.0 / N);
     ep.sketch_d = (double)d;
     ep.err = ctx->err.as<unsigned int>();
-    ep.rtiles = (K > 1 && !tiles.empty()) ? ctx->rtiles.as<float>() : nullptr;
+
+    // Whole-file INT8 runs with one annotation column overlap the band Gram
+    // with the upload too: after chunk k is decoded and finalised, the tiles
+    // whose records all lie in chunks [0, k] run while later chunks copy.
+    const bool stream_gram = chunked && exact_i8 && K == 1;
+    if (stream_gram) {
+        int rc = plan();
+        if (rc != LDSC_OK) return rc;
+        ep.left = ctx->left.as<int64_t>();
+        ep.rtiles = nullptr;
+    }
+    if (chunked) {
+        int rc = feed->start(s);
+        if (rc != LDSC_OK) return rc;
+    }
+
+    Events ev(s);
+    const int e0 = ev.mark();
+
+    // ---- decode ----
+    const uint64_t ld_i8 = round_up(n_used, 128);
+    const uint64_t ld_sk = round_up(d ? d : 1, 32);  // 128-byte operand rows for TMA
+    int e_sk = -1;
+    if (exact_i8) CK(ctx->ops.ensure((size_t)2 * nmom * ld_i8));
+    if (chunked) {
+        // records [r0, r1) whose rows arrived with chunks [0, k]
+        int64_t r0 = 0;
+        size_t t0 = 0;
+        for (int k = 0; k < feed->nchunks; k++) {
+            const uint64_t rend = feed->row_end(k);
+            int64_t r1 = r0;
+            if (a->bed_idx)
+                r1 = std::lower_bound(a->bed_idx + r0, a->bed_idx + m, rend) - a->bed_idx;
+            else
+                r1 = std::min<int64_t>(m, (int64_t)rend);
+            int rc = feed->issue_until(k + 1, s);
+            if (rc != LDSC_OK) return rc;
+            if (r1 > r0) {
+                PanelView pc = pv;
+                if (!rr) pc.rows = pv.rows + (uint64_t)r0 * pv.pitch;
+                RecStats sc = st;
+                sc.n += r0;
+                sc.s += r0;
+                sc.q += r0;
+                uint8_t* oc = exact_i8 ? ctx->ops.as<uint8_t>() + (size_t)2 * r0 * ld_i8 : nullptr;
+                CK(launch_decode_i8(pc, rr ? rr + r0 : nullptr, r1 - r0, sel, oc, exact_i8 ? ld_i8 : 0, sc, 0, s));
+                ctx->kernels++;
+                if (stream_gram) {
+                    sc.maf += r0;
+                    sc.mean += r0;
+                    sc.inv_std += r0;
+                    sc.qinv += r0;
+                    CK(launch_finalize_stats(r1 - r0, n_used, sc, a->annot ? ctx->annot.as<double>() + r0 : nullptr,
+                                             1, a->has_pq_exp, a->pq_exp, ctx->aeff.as<double>() + r0, nullptr,
+                                             ctx->l2.as<double>() + r0, s));
+                    ctx->kernels++;
+                    // tiles are ordered by right block; take those whose right block is complete
+                    size_t t1 = t0;
+                    while (t1 < tiles.size() && (r1 == m || (int64_t)(tiles[t1].b_blk + 1) * tb <= r1)) t1++;
+                    if (t1 > t0) {
+                        CK(launch_gram_i8(ctx->ops.as<uint8_t>(), ld_i8, m, ctx->tiles.as<Tile>() + t0,
+                                          (int64_t)(t1 - t0), ep, nullptr, ctx->sms, s));
+                        ctx->kernels++;
+                    }
+                    t0 = t1;
+                }
+            }
+            r0 = r1;
+        }
+        ctx->kernels--;  // counted once below
+    } else if (exact_i8) {
+        CK(launch_decode_i8(pv, rr, m, sel, ctx->ops.as<uint8_t>(), ld_i8, st, 0, s));
+    } else if (d) {
+        // fused: moments + CountSketch rows in one pass over the permuted panel
+        CK(launch_sketch_seg(ctx->sk_pp.as<uint32_t>(), ctx->sk_pitch_words, rr, m, n_used,
+                             ctx->sk_seg.as<int32_t>(), ctx->sk_wseg.as<int32_t>(), d, st, maf_aware ? 1 : 0, 1,
+                             ctx->xsk.as<float>(), ld_sk, s));
+        e_sk = ev.mark();
+    } else {
+        CK(launch_decode_i8(pv, rr, m, sel, nullptr, 0, st, 0, s));
+    }
+    ctx->kernels++;
+    if (!stream_gram) {
+        CK(launch_finalize_stats(m, n_used, st, a->annot ? ctx->annot.as<double>() : nullptr, K, a->has_pq_exp,
+                                 a->pq_exp, ctx->aeff.as<double>(), K > 1 ? ctx->aeff32.as<float>() : nullptr,
+                                 ctx->l2.as<double>(), s));
+        ctx->kernels++;
+    }
+    const uint64_t ld_f64 = round_up(n_used, 128);
+    if (!d && !exact_i8) {
+        CK(ctx->xf64.ensure((size_t)8 * nmom * ld_f64));
+        CK(launch_decode_f64(pv, rr, m, sel, st, ctx->xf64.as<double>(), ld_f64, s));
+        ctx->kernels++;
+    }
+    const int e1 = ev.mark();
+
+    if (!stream_gram) {
+        // ---- host plan (runs while the decode kernels execute) ----
+        int rc = plan();
+        if (rc != LDSC_OK) return rc;
+        ep.left = ctx->left.as<int64_t>();
+        ep.rtiles = (K > 1 && !tiles.empty()) ? ctx->rtiles.as<float>() : nullptr;
+    }
+    // ---- band Gram + epilogue ----
     const int e2 = ev.mark();
-    if (!tiles.empty()) {
+    if (!tiles.empty() && !stream_gram) {
         if (d) {
             CK(launch_gram_tf32(ctx->xsk.as<float>(), ld_sk, m, ctx->tiles.as<Tile>(), (int64_t)tiles.size(), ep,
                                 maf_aware ? 1 : 0, nullptr, ctx->sms, s));
@@ -657,16 +850,39 @@ int ldsc_l2_from_bed(ldsc_ctx* ctx, const uint8_t* bed_file, uint64_t len, uint6
     int rc = ldsc_bed_validate(bed_file, len, n_indiv, rows, msg, sizeof msg);
     if (rc != LDSC_OK) return fail(ctx, rc, msg);
     if (need_rows > rows) return fail(ctx, LDSC_E_INVALID, "SNP records point past the BED rows");
-    const auto t0 = std::chrono::steady_clock::now();
-    ldsc_panel* p = nullptr;
-    rc = ldsc_panel_upload(ctx, bed_file + 3, len - 3, n_indiv, rows, &p);
-    if (rc != LDSC_OK) return rc;
-    const double up = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    {
-        std::lock_guard<std::mutex> g(ctx->mu);
-        rc = run_l2(ctx, p, args, l2_out, maf_out, perf, up);
+    std::lock_guard<std::mutex> g(ctx->mu);
+    CK(cudaSetDevice(ctx->device));
+    // the panel lives in context-owned memory for the duration of the call
+    ldsc_panel p;
+    p.ctx = ctx;
+    p.n_snp = rows;
+    p.n_indiv = n_indiv;
+    p.bpr = bpr;
+    p.pitch = round_up(bpr, 16);
+    p.id = g_panel_ids.fetch_add(1);
+    RowFeed feed;
+    feed.ctx = ctx;
+    feed.host = bed_file + 3;
+    feed.bpr = bpr;
+    feed.pitch = p.pitch;
+    feed.rows = rows;
+    if (rows > 0) {
+        rc = feed.prepare();
+        if (rc != LDSC_OK) return rc;
+        p.rows = feed.dst;
+    } else {
+        CK(ctx->bed_rows.ensure(16));
+        p.rows = ctx->bed_rows.as<uint8_t>();
     }
-    ldsc_panel_destroy(p);
+    rc = run_l2(ctx, &p, args, l2_out, maf_out, perf, 0.0, rows > 0 ? &feed : nullptr);
+    if (feed.started) {
+        // a run that failed part-way returns before the feed is drained: finish it here
+        int rc2 = feed.issue_all(ctx->stream);
+        cudaError_t e = cudaStreamSynchronize(ctx->stream);
+        if (rc == LDSC_OK && rc2 != LDSC_OK) rc = rc2;
+        if (rc == LDSC_OK && e != cudaSuccess) rc = cuda_fail(ctx, e, "BED upload");
+        if (rc == LDSC_OK && perf) perf->bed_read_secs = feed.upload_secs();
+    }
     return rc;
 }
 

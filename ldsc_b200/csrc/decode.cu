@@ -208,6 +208,26 @@ __global__ void __launch_bounds__(256) k_decode_f64(PanelView p, const uint64_t*
     }
 }
 
+// One thread per 4-byte word of the pitched rows; the source is the file's
+// unpadded rows, read byte-wise (their starts are not word aligned).
+__global__ void __launch_bounds__(256) k_repitch(const uint8_t* __restrict__ src, uint64_t bpr,
+                                                 uint8_t* __restrict__ dst, uint64_t pitch, uint64_t r0,
+                                                 uint64_t r1) {
+    const uint64_t wpr = pitch >> 2;
+    const uint64_t total = (r1 - r0) * wpr;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += stride) {
+        const uint64_t r = r0 + t / wpr;
+        const uint64_t x = (t % wpr) * 4;
+        const uint8_t* srow = src + r * bpr;
+        uint32_t w = 0;
+#pragma unroll
+        for (int b = 0; b < 4; b++)
+            if (x + b < bpr) w |= (uint32_t)__ldg(srow + x + b) << (8 * b);
+        *reinterpret_cast<uint32_t*>(dst + r * pitch + x) = w;
+    }
+}
+
 int decode_grid(int64_t m) {
     int64_t blocks = (m + 7) / 8;
     if (blocks > 148 * 16) blocks = 148 * 16;
@@ -222,6 +242,16 @@ cudaError_t launch_decode_i8(const PanelView& p, const uint64_t* rec_rows, int64
                              cudaStream_t stream) {
     if (m <= 0) return cudaSuccess;
     k_decode_i8<<<decode_grid(m), 256, 0, stream>>>(p, rec_rows, m, sel, ops, ld, st, want_moments);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_repitch(const uint8_t* src, uint64_t bpr, uint8_t* dst, uint64_t pitch, uint64_t r0,
+                           uint64_t r1, cudaStream_t stream) {
+    if (r1 <= r0) return cudaSuccess;
+    const uint64_t words = (r1 - r0) * (pitch >> 2);
+    uint64_t blocks = (words + 255) / 256;
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    k_repitch<<<(unsigned)blocks, 256, 0, stream>>>(src, bpr, dst, pitch, r0, r1);
     return cudaGetLastError();
 }
 

@@ -81,6 +81,11 @@ cudaError_t launch_finalize_stats(int64_t m, uint64_t n_indiv, RecStats st,
                                   cudaStream_t stream);
 
 // Standardised f64 columns, row r of `x` = record r, `ld` doubles per row.
+// Rows [r0, r1) of a packed BED body (bpr bytes per row, as in the file) to
+// the pitched panel layout; pad bytes are zeroed.
+cudaError_t launch_repitch(const uint8_t* src, uint64_t bpr, uint8_t* dst, uint64_t pitch, uint64_t r0,
+                           uint64_t r1, cudaStream_t stream);
+
 cudaError_t launch_decode_f64(const PanelView& p, const uint64_t* rec_rows, int64_t m,
                               IndivSel sel, RecStats st, double* x, uint64_t ld,
                               cudaStream_t stream);
