@@ -116,6 +116,10 @@ typedef struct {
     int32_t yes_really;           /* --yes-really: silence the whole-chromosome window warning */
     ldsc_progress_fn on_progress; /* optional */
     void *progress_user;
+    /* Extensions for a resident panel (no reference counterpart; zero = off). */
+    uint64_t row_begin;           /* with bed_idx NULL: record i is row row_begin + i */
+    int32_t annot_on_device;      /* annot points to device memory (read in place) */
+    uint64_t annot_ld;            /* rows between annot columns; 0 = n_snp */
 } ldsc_l2_args;
 
 /* Synthetic panel description (seeded founder mosaic; see ldsc_b200/synth.py). */
@@ -148,6 +152,13 @@ int ldsc_last_error(const ldsc_ctx *ctx, char *buf, size_t len);
 /* Number of kernels this context has launched since creation. */
 uint64_t ldsc_ctx_kernel_count(const ldsc_ctx *ctx);
 
+/* Number of cached CUDA-graph replays (regression pipelines) of this context. */
+uint64_t ldsc_ctx_graph_launches(const ldsc_ctx *ctx);
+
+/* Free the context's device workspace and cached graphs (they grow back on
+ * demand).  Waits for the context's work. */
+int ldsc_ctx_trim(ldsc_ctx *ctx);
+
 /* ---- BED validation and resident panels -------------------------------- */
 
 /* Bed::from_bytes header/length validation (src/bed.rs:53-128) on a whole
@@ -172,6 +183,9 @@ int ldsc_panel_download(ldsc_ctx *ctx, const ldsc_panel *panel, uint64_t snp_beg
 
 int ldsc_panel_destroy(ldsc_panel *panel);
 
+/* Individuals and SNP rows of a panel. */
+int ldsc_panel_shape(const ldsc_panel *panel, uint64_t *n_indiv, uint64_t *n_snp);
+
 /* ---- the l2 computation ------------------------------------------------ */
 
 /* compute_ldscore_global on a resident panel.  l2_out: n_snp x K column-major
@@ -186,6 +200,11 @@ int ldsc_l2_from_bed(ldsc_ctx *ctx, const uint8_t *bed_file, uint64_t len, uint6
 
 /* Number of off-diagonal pairs the call would accumulate (host only). */
 int ldsc_l2_pair_count(const ldsc_l2_args *args, uint64_t *n_pairs);
+
+/* Device workspace (bytes) ldsc_l2_run would hold for these arguments on a
+ * panel of n_indiv individuals, not counting the panel and its shared
+ * CountSketch layout (host only). */
+int ldsc_l2_workspace_bytes(const ldsc_l2_args *args, uint64_t n_indiv, uint64_t *bytes);
 
 /* Per-record left window limit L[i] (host only): record i pairs with every
  * record k, L[i] <= k < i.  Masked mode: the per-SNP block_left
@@ -269,6 +288,64 @@ typedef struct {
 } ldsc_rg_result;
 
 int ldsc_rg_batch(ldsc_ctx *ctx, const ldsc_rg_args *args, ldsc_rg_result *results);
+
+/* ---- serving: continuous batching over resident panels ------------------ */
+
+/* No counterpart in the reference (one computation per process there).  A
+ * server owns n_slots engine contexts, each with its own stream, workspace
+ * and worker thread.  Queued jobs are admitted in arrival order as a slot
+ * and device memory free up: a job fits when its workspace fits in the
+ * slot's, or when growing the slot keeps all slots' workspace within
+ * device_budget (0 = free memory at creation minus 4 GiB).  A later job may
+ * pass an older one that does not fit yet; idle slots give their workspace
+ * back when the oldest job needs it.  Admitted jobs run concurrently and
+ * their kernels overlap on the device; regression pipelines replay as cached
+ * CUDA graphs.  A job's result does not depend on what else runs. */
+typedef struct ldsc_server ldsc_server;
+
+enum { LDSC_JOB_L2 = 0, LDSC_JOB_H2 = 1, LDSC_JOB_RG = 2 };
+
+typedef struct {
+    int32_t kind;                 /* LDSC_JOB_* */
+    const ldsc_panel *panel;      /* L2: resident panel */
+    ldsc_l2_args l2;              /* L2 arguments (copied; the arrays they point to must stay valid
+                                     until the job completes) */
+    double *l2_out;               /* L2: n_snp x K column-major, host */
+    double *maf_out;              /* L2: n_snp, host, may be NULL */
+    ldsc_h2_args h2;              /* H2 */
+    ldsc_h2_result *h2_out;       /* H2: n_traits results */
+    ldsc_rg_args rg;              /* RG */
+    ldsc_rg_result *rg_out;       /* RG: n_pairs results */
+    uint64_t device_bytes;        /* workspace the job needs; 0 = estimated by the server */
+} ldsc_job;
+
+typedef struct {
+    int32_t status;               /* LDSC_OK or an error code */
+    uint32_t slot;                /* slot that ran the job */
+    double queue_ms;              /* submit -> start */
+    double run_ms;                /* start -> end */
+    double latency_ms;            /* submit -> end */
+    ldsc_perf perf;               /* L2 jobs */
+    char error[256];
+} ldsc_job_result;
+
+typedef struct {
+    uint64_t submitted, completed, running, queued;
+    uint64_t budget_bytes;        /* device workspace budget */
+    uint64_t reserved_bytes;      /* workspace the slots may hold now */
+    uint64_t graph_launches;      /* cached-graph replays over all slots */
+    uint64_t kernels;             /* kernels launched over all slots */
+} ldsc_server_stats;
+
+int ldsc_server_create(int device, uint32_t n_slots, uint64_t device_budget, ldsc_server **out);
+/* Queue a job; returns at once with its ticket.  LDSC_E_NOMEM if the job's
+ * workspace exceeds the whole budget. */
+int ldsc_server_submit(ldsc_server *srv, const ldsc_job *job, uint64_t *ticket);
+/* Block until the job ends; returns its status and releases the ticket. */
+int ldsc_server_wait(ldsc_server *srv, uint64_t ticket, ldsc_job_result *result);
+int ldsc_server_stats_get(ldsc_server *srv, ldsc_server_stats *stats);
+/* Finish running jobs, fail queued ones, free the slots. */
+int ldsc_server_destroy(ldsc_server *srv);
 
 /* ---- allocation-free entry point ---------------------------------------- */
 

@@ -61,6 +61,7 @@ class L2Args(C.Structure):
         ("n_keep", C.c_uint64), ("annot", C.c_void_p), ("n_annot", C.c_uint32),
         ("has_pq_exp", C.c_int32), ("pq_exp", C.c_double), ("yes_really", C.c_int32),
         ("on_progress", PROGRESS_FN), ("progress_user", C.c_void_p),
+        ("row_begin", C.c_uint64), ("annot_on_device", C.c_int32), ("annot_ld", C.c_uint64),
     ]
 
 
@@ -95,6 +96,26 @@ class RgResult(C.Structure):
                                           "h2_1_se", "h2_2", "h2_2_se", "mean_z1z2")]
 
 
+JOB_L2, JOB_H2, JOB_RG = 0, 1, 2
+
+
+class Job(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("panel", C.c_void_p), ("l2", L2Args), ("l2_out", C.c_void_p),
+                ("maf_out", C.c_void_p), ("h2", H2Args), ("h2_out", C.c_void_p), ("rg", RgArgs),
+                ("rg_out", C.c_void_p), ("device_bytes", C.c_uint64)]
+
+
+class JobResult(C.Structure):
+    _fields_ = [("status", C.c_int32), ("slot", C.c_uint32), ("queue_ms", C.c_double),
+                ("run_ms", C.c_double), ("latency_ms", C.c_double), ("perf", Perf),
+                ("error", C.c_char * 256)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [(f, C.c_uint64) for f in ("submitted", "completed", "running", "queued", "budget_bytes",
+                                          "reserved_bytes", "graph_launches", "kernels")]
+
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     "ldsc_abi_version": (C.c_int, []),
@@ -126,6 +147,15 @@ SIGNATURES = {
     "ldsc_l2_int8_noalloc": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p,
                                        C.c_void_p, C.c_void_p, C.c_void_p]),
     "ldsc_noalloc_last_error": (C.c_int, [C.c_char_p, C.c_size_t]),
+    "ldsc_ctx_graph_launches": (C.c_uint64, [C.c_void_p]),
+    "ldsc_ctx_trim": (C.c_int, [C.c_void_p]),
+    "ldsc_panel_shape": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    "ldsc_l2_workspace_bytes": (C.c_int, [C.POINTER(L2Args), C.c_uint64, C.POINTER(C.c_uint64)]),
+    "ldsc_server_create": (C.c_int, [C.c_int, C.c_uint32, C.c_uint64, C.POINTER(C.c_void_p)]),
+    "ldsc_server_submit": (C.c_int, [C.c_void_p, C.POINTER(Job), C.POINTER(C.c_uint64)]),
+    "ldsc_server_wait": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(JobResult)]),
+    "ldsc_server_stats_get": (C.c_int, [C.c_void_p, C.POINTER(ServerStats)]),
+    "ldsc_server_destroy": (C.c_int, [C.c_void_p]),
     "ldsc_h2_batch": (C.c_int, [C.c_void_p, C.POINTER(H2Args), C.c_void_p]),
     "ldsc_rg_batch": (C.c_int, [C.c_void_p, C.POINTER(RgArgs), C.c_void_p]),
 }

@@ -181,7 +181,8 @@ class _ArgPack:
 
     def __init__(self, snps: BimTable, mode: WindowMode, chunk_c: int, annot, iid_indices, pq_exp,
                  yes_really, use_f32, sketch, sketch_maf_aware, snp_level_masking, precision,
-                 global_pass, on_progress, records_are_rows: bool = False):
+                 global_pass, on_progress, records_are_rows: bool = False, row_begin: int = 0,
+                 annot_device=None):
         m = len(snps)
         self.chr = np.ascontiguousarray(snps.chr, dtype=np.uint8)
         self.cm = np.ascontiguousarray(snps.cm, dtype=np.float64)
@@ -199,6 +200,10 @@ class _ArgPack:
                                 f"Annotation matrix has {a.shape[0]} rows but BIM has {m} SNPs")
             self.annot = np.asfortranarray(a)
             K = a.shape[1]
+        annot_ptr, annot_ld = (None if self.annot is None else self.annot.ctypes.data), 0
+        if annot_device is not None:
+            # (device pointer, leading dimension in rows, K) of a resident annotation matrix
+            annot_ptr, annot_ld, K = int(annot_device[0]), int(annot_device[1]), int(annot_device[2])
         self.K = K
         self.cb = PROGRESS_NONE
         if on_progress is not None:
@@ -219,9 +224,10 @@ class _ArgPack:
             sketch_maf_aware=int(bool(sketch_maf_aware)),
             keep_iids=None if self.keep is None else self.keep.ctypes.data,
             n_keep=0 if self.keep is None else len(self.keep),
-            annot=None if self.annot is None else self.annot.ctypes.data, n_annot=K,
+            annot=annot_ptr, n_annot=K,
             has_pq_exp=int(pq_exp is not None), pq_exp=float(pq_exp or 0.0),
-            yes_really=int(bool(yes_really)), on_progress=self.cb, progress_user=None)
+            yes_really=int(bool(yes_really)), on_progress=self.cb, progress_user=None,
+            row_begin=int(row_begin), annot_on_device=int(annot_device is not None), annot_ld=annot_ld)
 
 
 PROGRESS_NONE = L.PROGRESS_FN()

@@ -59,6 +59,40 @@ struct DevBuf {
 
 uint64_t round_up(uint64_t x, uint64_t a) { return (x + a - 1) / a * a; }
 
+// Instantiated CUDA graphs of fixed launch sequences, keyed by everything
+// their kernels' parameters depend on (sizes and buffer addresses).
+struct GraphCache {
+    struct Entry {
+        std::vector<uint64_t> key;
+        cudaGraphExec_t exec = nullptr;
+        uint64_t tick = 0;
+    };
+    std::vector<Entry> e;
+    uint64_t tick = 0;
+    void clear() {
+        for (auto& x : e)
+            if (x.exec) cudaGraphExecDestroy(x.exec);
+        e.clear();
+    }
+};
+
+// Bucket-major CountSketch layout of a panel: the individuals' order, the
+// segment tables and the panel rows rewritten in that order.
+struct SketchCache {
+    DevBuf perm, seg, wseg, pp;
+    uint64_t n = 0, key = 0, pitch_words = 0;
+    uint32_t d = 0;
+    bool valid = false;
+    bool matches(uint64_t n_, uint32_t d_, uint64_t key_) const { return valid && n == n_ && d == d_ && key == key_; }
+    void release() {
+        perm.release();
+        seg.release();
+        wseg.release();
+        pp.release();
+        valid = false;
+    }
+};
+
 }  // namespace
 
 struct ldsc_ctx {
@@ -73,24 +107,42 @@ struct ldsc_ctx {
     // workspace (grow-only)
     DevBuf ops, xf64, xsk, recrows, keep, left, tiles, annot, aeff, aeff32, l2, maf, pq, err;
     DevBuf st_n, st_s, st_q, st_q3, st_q4, st_mean, st_inv, st_qinv, st_kappa, packed, tsum, dbg;
-    // CountSketch cache: bucket-major order and the permuted panel, keyed by
-    // (panel id, individuals used, d, keep-list hash)
-    DevBuf sk_perm, sk_seg, sk_wseg, sk_pp;
+    // private CountSketch layout (explicit bucket/sign arrays, or a panel
+    // whose shared layout is in use under another key)
+    SketchCache sk;
+    uint64_t sk_panel = 0;
+    GraphCache graphs;            // regression pipelines
+    uint64_t graph_launches = 0;  // replays of cached graphs
     DevBuf rtiles, cptr_r, cidx_r, cptr_l, cidx_l;  // K > 1 contraction: r2u tiles and CSR tile lists
     DevBuf rg_jobs, rg_states, rg_outs, rg_part, rg_tdel, rg_y, rg_y2, rg_n, rg_ld, rg_wld, rg_sel, rg_pairs, rg_res;
-    uint64_t sk_panel = 0, sk_n = 0, sk_key = 0, sk_pitch_words = 0;
-    uint32_t sk_d = 0;
     // whole-file entry: staged file rows, the pitched panel, per-chunk events
     DevBuf bed_stage, bed_rows;
     std::vector<cudaEvent_t> feed_ev;
     cudaEvent_t feed_t0 = nullptr, feed_t1 = nullptr, feed_go = nullptr, up_ev = nullptr;
+
+    std::vector<DevBuf*> workspace() {
+        return {&ops, &xf64, &xsk, &recrows, &keep, &left,
+                      &tiles, &annot, &aeff, &aeff32, &l2, &maf,
+                      &pq, &err, &st_n, &st_s, &st_q, &st_q3,
+                      &st_q4, &st_mean, &st_inv, &st_qinv, &st_kappa,
+                      &packed, &tsum, &dbg,
+                      &rtiles, &cptr_r, &cidx_r, &cptr_l, &cidx_l,
+                      &rg_jobs, &rg_states, &rg_outs, &rg_part, &rg_tdel,
+                      &rg_y, &rg_y2, &rg_n, &rg_ld, &rg_wld, &rg_sel,
+                      &rg_pairs, &rg_res, &bed_stage, &bed_rows};
+    }
 };
 
 struct ldsc_panel {
     ldsc_ctx* ctx = nullptr;
     uint8_t* rows = nullptr;
     uint64_t n_snp = 0, n_indiv = 0, bpr = 0, pitch = 0;
-    uint64_t id = 0;  // unique per panel, keys the CountSketch permuted-panel cache
+    uint64_t id = 0;  // unique per panel, keys the contexts' private sketch layouts
+    // shared CountSketch layout, usable by every context on the device;
+    // rebuilt only while no run is using it
+    mutable std::mutex mu;
+    mutable SketchCache sk;
+    mutable int sk_users = 0;
 };
 
 static std::atomic<uint64_t> g_panel_ids{1};
@@ -148,18 +200,11 @@ int ldsc_ctx_destroy(ldsc_ctx* ctx) {
     if (!ctx) return LDSC_OK;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
-    DevBuf* bufs[] = {&ctx->ops, &ctx->xf64, &ctx->xsk, &ctx->recrows, &ctx->keep, &ctx->left,
-                      &ctx->tiles, &ctx->annot, &ctx->aeff, &ctx->aeff32, &ctx->l2, &ctx->maf,
-                      &ctx->pq, &ctx->err, &ctx->st_n, &ctx->st_s, &ctx->st_q, &ctx->st_q3,
-                      &ctx->st_q4, &ctx->st_mean, &ctx->st_inv, &ctx->st_qinv, &ctx->st_kappa,
-                      &ctx->packed, &ctx->tsum, &ctx->dbg,
-                      &ctx->sk_perm, &ctx->sk_seg, &ctx->sk_wseg, &ctx->sk_pp,
-                      &ctx->rtiles, &ctx->cptr_r, &ctx->cidx_r, &ctx->cptr_l, &ctx->cidx_l,
-                      &ctx->rg_jobs, &ctx->rg_states, &ctx->rg_outs, &ctx->rg_part, &ctx->rg_tdel,
-                      &ctx->rg_y, &ctx->rg_y2, &ctx->rg_n, &ctx->rg_ld, &ctx->rg_wld, &ctx->rg_sel,
-                      &ctx->rg_pairs, &ctx->rg_res, &ctx->bed_stage, &ctx->bed_rows};
+    std::vector<DevBuf*> bufs = ctx->workspace();
     cudaStreamSynchronize(ctx->copy);
     for (DevBuf* b : bufs) b->release();
+    ctx->sk.release();
+    ctx->graphs.clear();
     for (cudaEvent_t e : ctx->feed_ev) cudaEventDestroy(e);
     for (cudaEvent_t e : {ctx->feed_t0, ctx->feed_t1, ctx->feed_go, ctx->up_ev})
         if (e) cudaEventDestroy(e);
@@ -184,6 +229,28 @@ int ldsc_last_error(const ldsc_ctx* ctx, char* buf, size_t len) {
 }
 
 uint64_t ldsc_ctx_kernel_count(const ldsc_ctx* ctx) { return ctx ? ctx->kernels : 0; }
+
+uint64_t ldsc_ctx_graph_launches(const ldsc_ctx* ctx) { return ctx ? ctx->graph_launches : 0; }
+
+int ldsc_ctx_trim(ldsc_ctx* ctx) {
+    if (!ctx) return LDSC_E_INVALID;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    cudaStreamSynchronize(ctx->copy);
+    ctx->graphs.clear();  // their kernels hold the buffers' addresses
+    for (DevBuf* b : ctx->workspace()) b->release();
+    ctx->sk.release();
+    ctx->sk_panel = 0;
+    return LDSC_OK;
+}
+
+int ldsc_panel_shape(const ldsc_panel* p, uint64_t* n_indiv, uint64_t* n_snp) {
+    if (!p) return LDSC_E_INVALID;
+    if (n_indiv) *n_indiv = p->n_indiv;
+    if (n_snp) *n_snp = p->n_snp;
+    return LDSC_OK;
+}
 
 int ldsc_bed_validate(const uint8_t* bed, uint64_t len, uint64_t n_indiv, uint64_t n_snp, char* err,
                       size_t errlen) {
@@ -289,6 +356,7 @@ int ldsc_panel_destroy(ldsc_panel* p) {
     if (!p) return LDSC_OK;
     if (p->ctx) cudaSetDevice(p->ctx->device);
     if (p->rows) cudaFree(p->rows);
+    p->sk.release();
     delete p;
     return LDSC_OK;
 }
@@ -307,6 +375,33 @@ int ldsc_l2_left_limits(const ldsc_l2_args* a, int64_t* left_out) {
                      a->chunk_size, a->snp_level_masking != 0, a->global_pass != 0, &L, &err))
         return LDSC_E_INVALID;
     if (a->n_snp) std::memcpy(left_out, L.left.data(), sizeof(int64_t) * a->n_snp);
+    return LDSC_OK;
+}
+
+int ldsc_l2_workspace_bytes(const ldsc_l2_args* a, uint64_t n_indiv, uint64_t* bytes) {
+    if (!a || !bytes) return LDSC_E_INVALID;
+    const uint64_t m = a->n_snp;
+    LeftLimits L;
+    std::string err;
+    if (!left_limits((int64_t)m, a->chr, a->cm, a->bp, a->window_mode, a->window_size, a->window_snps, a->chunk_size,
+                     a->snp_level_masking != 0, a->global_pass != 0, &L, &err))
+        return LDSC_E_INVALID;
+    const uint64_t n_used = a->keep_iids ? a->n_keep : n_indiv;
+    const uint64_t K = a->annot ? a->n_annot : 1;
+    const uint32_t d = a->sketch_d;
+    const bool exact_i8 = !d && a->precision == LDSC_PRECISION_INT8;
+    const int ta = (exact_i8 || d) ? 64 : 128, tb = 128;
+    const uint64_t ntiles = band_tiles(L.left, ta, tb).size();
+    uint64_t b = m * (12 + 32 + 16 * K) + 8 * m + 8 * (ntiles + 1) + 64;  // stats, l2/aeff, left, tiles
+    if (d && a->sketch_maf_aware) b += 16 * m;
+    if (K > 1) b += 4 * m * K + (uint64_t)4 * ta * tb * ntiles + 8 * ntiles + 4 * (m / 64 + m / 128 + 4);
+    if (a->annot && !a->annot_on_device) b += 8 * m * K;
+    if (a->bed_idx) b += 8 * m;
+    if (a->keep_iids) b += 8 * a->n_keep;
+    if (exact_i8) b += 2 * m * round_up(n_used, 128);
+    else if (d) b += 8 * m * round_up(d, 32);
+    else b += 8 * m * round_up(n_used, 128);
+    *bytes = b;
     return LDSC_OK;
 }
 
@@ -350,29 +445,31 @@ struct Events {
 };
 
 // Bucket-major order for a sketch, uploaded, and the panel rewritten in that
-// order (cached in the context until the panel / individuals / d change).
+// order into cache c.
 int sketch_prepare(ldsc_ctx* ctx, const ldsc_panel* panel, uint64_t n_used, uint32_t d, const uint32_t* bucket,
-                   const float* sign, const int64_t* keep) {
+                   const float* sign, const int64_t* keep, uint64_t key, SketchCache& c) {
     cudaStream_t s = ctx->stream;
     SketchOrder o = sketch_order(n_used, d, bucket, sign, keep);
     const uint64_t words = (n_used + 15) / 16;
     const uint64_t pitch_words = round_up(words, 4);
-    CK(ctx->sk_perm.ensure(4 * (size_t)n_used));
-    CK(ctx->sk_seg.ensure(4 * o.seg_off.size()));
-    CK(ctx->sk_wseg.ensure(4 * o.word_seg.size()));
-    CK(ctx->sk_pp.ensure((size_t)4 * pitch_words * (panel->n_snp ? panel->n_snp : 1)));
-    CK(cudaMemcpyAsync(ctx->sk_perm.p, o.perm.data(), 4 * (size_t)n_used, cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(ctx->sk_seg.p, o.seg_off.data(), 4 * o.seg_off.size(), cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(ctx->sk_wseg.p, o.word_seg.data(), 4 * o.word_seg.size(), cudaMemcpyHostToDevice, s));
+    c.valid = false;
+    CK(c.perm.ensure(4 * (size_t)n_used));
+    CK(c.seg.ensure(4 * o.seg_off.size()));
+    CK(c.wseg.ensure(4 * o.word_seg.size()));
+    CK(c.pp.ensure((size_t)4 * pitch_words * (panel->n_snp ? panel->n_snp : 1)));
+    CK(cudaMemcpyAsync(c.perm.p, o.perm.data(), 4 * (size_t)n_used, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(c.seg.p, o.seg_off.data(), 4 * o.seg_off.size(), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(c.wseg.p, o.word_seg.data(), 4 * o.word_seg.size(), cudaMemcpyHostToDevice, s));
     PanelView pv{panel->rows, panel->n_snp, panel->n_indiv, panel->bpr, panel->pitch};
-    CK(launch_sketch_permute(pv, ctx->sk_perm.as<int32_t>(), n_used, ctx->sk_pp.as<uint32_t>(), pitch_words, s));
+    CK(launch_sketch_permute(pv, c.perm.as<int32_t>(), n_used, c.pp.as<uint32_t>(), pitch_words, s));
     ctx->kernels++;
-    CK(cudaStreamSynchronize(s));  // host vectors go out of scope
-    ctx->sk_panel = panel->id;
-    ctx->sk_n = n_used;
-    ctx->sk_d = d;
-    ctx->sk_key = 0;
-    ctx->sk_pitch_words = pitch_words;
+    // host vectors go out of scope, and other streams may read the layout next
+    CK(cudaStreamSynchronize(s));
+    c.n = n_used;
+    c.d = d;
+    c.key = key;
+    c.pitch_words = pitch_words;
+    c.valid = true;
     return LDSC_OK;
 }
 
@@ -498,9 +595,11 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
             if (a->bed_idx[i] >= panel->n_snp)
                 return fail(ctx, LDSC_E_INVALID, "SNP index " + std::to_string(a->bed_idx[i]) +
                                                      " out of range (max " + std::to_string(panel->n_snp) + ")");
-    } else if ((uint64_t)m > panel->n_snp) {
+    } else if (a->row_begin > panel->n_snp || (uint64_t)m > panel->n_snp - a->row_begin) {
         return fail(ctx, LDSC_E_INVALID, "more SNP records than panel rows");
     }
+    if (a->annot && a->annot_ld && a->annot_ld < (uint64_t)m)
+        return fail(ctx, LDSC_E_INVALID, "annot_ld is smaller than the number of SNP records");
     if (m == 0) {
         if (perf) *perf = pf;
         return LDSC_OK;
@@ -533,7 +632,7 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
         CK(ctx->st_kappa.ensure(8 * nmom));
     }
     if (K > 1) CK(ctx->aeff32.ensure(4 * nmom * K));
-    if (a->annot) CK(ctx->annot.ensure(8 * nmom * K));
+    if (a->annot && !a->annot_on_device) CK(ctx->annot.ensure(8 * nmom * K));
     if (a->bed_idx) CK(ctx->recrows.ensure(8 * nmom));
     if (a->keep_iids) CK(ctx->keep.ensure(8 * a->n_keep));
 
@@ -552,12 +651,22 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
         CK(cudaEventRecord(ctx->up_ev, s));
         CK(cudaStreamWaitEvent(up, ctx->up_ev, 0));
     }
-    if (a->annot) CK(cudaMemcpyAsync(ctx->annot.p, a->annot, 8 * nmom * K, cudaMemcpyHostToDevice, up));
+    if (a->annot && !a->annot_on_device) {
+        const uint64_t ald = a->annot_ld ? a->annot_ld : nmom;
+        CK(cudaMemcpy2DAsync(ctx->annot.p, 8 * nmom, a->annot, 8 * ald, 8 * nmom, K, cudaMemcpyHostToDevice, up));
+    }
+    // annotations on the device: column c of record r at annot_dev[r + c * annot_ld_dev]
+    const double* annot_dev = !a->annot ? nullptr : (a->annot_on_device ? a->annot : ctx->annot.as<double>());
+    const uint64_t annot_ld_dev = !a->annot ? 0 : (a->annot_on_device && a->annot_ld ? a->annot_ld : nmom);
     if (a->bed_idx) CK(cudaMemcpyAsync(ctx->recrows.p, a->bed_idx, 8 * nmom, cudaMemcpyHostToDevice, up));
     if (a->keep_iids) CK(cudaMemcpyAsync(ctx->keep.p, a->keep_iids, 8 * a->n_keep, cudaMemcpyHostToDevice, up));
     CK(cudaMemsetAsync(ctx->err.p, 0, 16, s));
 
     PanelView pv{panel->rows, panel->n_snp, panel->n_indiv, panel->bpr, panel->pitch};
+    if (!a->bed_idx) {
+        pv.rows += a->row_begin * panel->pitch;
+        pv.n_snp -= a->row_begin;
+    }
     IndivSel sel{a->keep_iids ? ctx->keep.as<int64_t>() : nullptr, n_used};
     const uint64_t* rr = a->bed_idx ? ctx->recrows.as<uint64_t>() : nullptr;
     RecStats st{};
@@ -587,17 +696,51 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
         if (rc != LDSC_OK) return rc;
     }
 
+    // the sketch layout: the panel's shared one, or this context's own when the
+    // shared one is in use under another key
+    const SketchCache* skc = nullptr;
+    struct SketchUse {
+        const ldsc_panel* p = nullptr;
+        ~SketchUse() {
+            if (p) {
+                std::lock_guard<std::mutex> g(p->mu);
+                p->sk_users--;
+            }
+        }
+    } sk_use;
     if (d) {
         uint64_t key = 1469598103934665603ull;
         if (a->keep_iids)
             for (uint64_t i = 0; i < a->n_keep; i++) key = (key ^ (uint64_t)a->keep_iids[i]) * 1099511628211ull;
-        if (!(ctx->sk_panel == panel->id && ctx->sk_n == n_used && ctx->sk_d == d && ctx->sk_key == key)) {
-            std::vector<uint32_t> bucket(n_used);
-            std::vector<float> sign(n_used);
+        std::vector<uint32_t> bucket;
+        std::vector<float> sign;
+        auto hash = [&]() {
+            bucket.resize(n_used);
+            sign.resize(n_used);
             countsketch_hash(n_used, d, 42, bucket.data(), sign.data());  // the reference's seed-42 stream
-            int rc = sketch_prepare(ctx, panel, n_used, d, bucket.data(), sign.data(), a->keep_iids);
-            if (rc != LDSC_OK) return rc;
-            ctx->sk_key = key;
+        };
+        {
+            std::lock_guard<std::mutex> g(panel->mu);
+            if (!panel->sk.matches(n_used, d, key) && panel->sk_users == 0) {
+                hash();
+                int rc = sketch_prepare(ctx, panel, n_used, d, bucket.data(), sign.data(), a->keep_iids, key, panel->sk);
+                if (rc != LDSC_OK) return rc;
+            }
+            if (panel->sk.matches(n_used, d, key)) {
+                panel->sk_users++;
+                sk_use.p = panel;
+                skc = &panel->sk;
+            }
+        }
+        if (!skc) {
+            if (!(ctx->sk_panel == panel->id && ctx->sk.matches(n_used, d, key))) {
+                if (bucket.empty()) hash();
+                ctx->sk_panel = 0;
+                int rc = sketch_prepare(ctx, panel, n_used, d, bucket.data(), sign.data(), a->keep_iids, key, ctx->sk);
+                if (rc != LDSC_OK) return rc;
+                ctx->sk_panel = panel->id;
+            }
+            skc = &ctx->sk;
         }
         CK(ctx->xsk.ensure((size_t)4 * 2 * nmom * round_up(d, 32)));
     }
@@ -703,7 +846,7 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
             if (a->bed_idx)
                 r1 = std::lower_bound(a->bed_idx + r0, a->bed_idx + m, rend) - a->bed_idx;
             else
-                r1 = std::min<int64_t>(m, (int64_t)rend);
+                r1 = std::max<int64_t>(r0, std::min<int64_t>(m, (int64_t)rend - (int64_t)a->row_begin));
             int rc = feed->issue_until(k + 1, s);
             if (rc != LDSC_OK) return rc;
             if (r1 > r0) {
@@ -721,9 +864,9 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
                     sc.mean += r0;
                     sc.inv_std += r0;
                     sc.qinv += r0;
-                    CK(launch_finalize_stats(r1 - r0, n_used, sc, a->annot ? ctx->annot.as<double>() + r0 : nullptr,
-                                             1, a->has_pq_exp, a->pq_exp, ctx->aeff.as<double>() + r0, nullptr,
-                                             ctx->l2.as<double>() + r0, s));
+                    CK(launch_finalize_stats(r1 - r0, n_used, sc, annot_dev ? annot_dev + r0 : nullptr, 1,
+                                             a->has_pq_exp, a->pq_exp, ctx->aeff.as<double>() + r0, nullptr,
+                                             ctx->l2.as<double>() + r0, s, annot_ld_dev));
                     ctx->kernels++;
                     // tiles are ordered by right block; take those whose right block is complete
                     size_t t1 = t0;
@@ -743,18 +886,17 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
         CK(launch_decode_i8(pv, rr, m, sel, ctx->ops.as<uint8_t>(), ld_i8, st, 0, s));
     } else if (d) {
         // fused: moments + CountSketch rows in one pass over the permuted panel
-        CK(launch_sketch_seg(ctx->sk_pp.as<uint32_t>(), ctx->sk_pitch_words, rr, m, n_used,
-                             ctx->sk_seg.as<int32_t>(), ctx->sk_wseg.as<int32_t>(), d, st, maf_aware ? 1 : 0, 1,
-                             ctx->xsk.as<float>(), ld_sk, s));
+        CK(launch_sketch_seg(skc->pp.as<uint32_t>() + (rr ? 0 : a->row_begin * skc->pitch_words), skc->pitch_words,
+                             rr, m, n_used, skc->seg.as<int32_t>(), skc->wseg.as<int32_t>(), d, st,
+                             maf_aware ? 1 : 0, 1, ctx->xsk.as<float>(), ld_sk, s));
         e_sk = ev.mark();
     } else {
         CK(launch_decode_i8(pv, rr, m, sel, nullptr, 0, st, 0, s));
     }
     ctx->kernels++;
     if (!stream_gram) {
-        CK(launch_finalize_stats(m, n_used, st, a->annot ? ctx->annot.as<double>() : nullptr, K, a->has_pq_exp,
-                                 a->pq_exp, ctx->aeff.as<double>(), K > 1 ? ctx->aeff32.as<float>() : nullptr,
-                                 ctx->l2.as<double>(), s));
+        CK(launch_finalize_stats(m, n_used, st, annot_dev, K, a->has_pq_exp, a->pq_exp, ctx->aeff.as<double>(),
+                                 K > 1 ? ctx->aeff32.as<float>() : nullptr, ctx->l2.as<double>(), s, annot_ld_dev));
         ctx->kernels++;
     }
     const uint64_t ld_f64 = round_up(n_used, 128);
@@ -875,6 +1017,7 @@ int ldsc_l2_from_bed(ldsc_ctx* ctx, const uint8_t* bed_file, uint64_t len, uint6
         p.rows = ctx->bed_rows.as<uint8_t>();
     }
     rc = run_l2(ctx, &p, args, l2_out, maf_out, perf, 0.0, rows > 0 ? &feed : nullptr);
+    p.sk.release();  // the call's panel layout does not outlive the call
     if (feed.started) {
         // a run that failed part-way returns before the feed is drained: finish it here
         int rc2 = feed.issue_all(ctx->stream);
@@ -902,8 +1045,8 @@ int ldsc_sketch_project(ldsc_ctx* ctx, const ldsc_panel* panel, uint64_t b, uint
     }
     cudaStream_t s = ctx->stream;
     CK(cudaSetDevice(ctx->device));
-    int rc = sketch_prepare(ctx, panel, n_used, d, bucket, sign, keep);
-    ctx->sk_panel = 0;  // explicit bucket/sign arrays: do not reuse for l2 runs
+    ctx->sk_panel = 0;  // explicit bucket/sign arrays: the layout is not reused by l2 runs
+    int rc = sketch_prepare(ctx, panel, n_used, d, bucket, sign, keep, 0, ctx->sk);
     if (rc != LDSC_OK) return rc;
     std::vector<uint64_t> rows((size_t)m);
     for (int64_t i = 0; i < m; i++) rows[i] = b + (uint64_t)i;
@@ -917,8 +1060,8 @@ int ldsc_sketch_project(ldsc_ctx* ctx, const ldsc_panel* panel, uint64_t b, uint
     st.n = ctx->st_n.as<int32_t>();
     st.s = ctx->st_s.as<int32_t>();
     st.q = ctx->st_q.as<int32_t>();
-    CK(launch_sketch_seg(ctx->sk_pp.as<uint32_t>(), ctx->sk_pitch_words, ctx->recrows.as<uint64_t>(), m, n_used,
-                         ctx->sk_seg.as<int32_t>(), ctx->sk_wseg.as<int32_t>(), d, st, 0, 0, ctx->xsk.as<float>(), d,
+    CK(launch_sketch_seg(ctx->sk.pp.as<uint32_t>(), ctx->sk.pitch_words, ctx->recrows.as<uint64_t>(), m, n_used,
+                         ctx->sk.seg.as<int32_t>(), ctx->sk.wseg.as<int32_t>(), d, st, 0, 0, ctx->xsk.as<float>(), d,
                          s));
     ctx->kernels += 1;
     CK(cudaMemcpyAsync(out, ctx->xsk.p, 4 * (size_t)m * d, cudaMemcpyDeviceToHost, s));
@@ -996,6 +1139,48 @@ int ldsc_debug_gram_i8_tile(ldsc_ctx* ctx, const ldsc_panel* panel, uint64_t k0,
 // ---------------------------------------------------------------------------
 
 namespace {
+
+// Launches body(s) through a cached graph: captured and instantiated on the
+// first call with this key, replayed afterwards.
+template <typename F>
+cudaError_t graph_launch(ldsc_ctx* ctx, const std::vector<uint64_t>& key, cudaStream_t s, F&& body) {
+    GraphCache& gc = ctx->graphs;
+    for (auto& x : gc.e)
+        if (x.key == key) {
+            x.tick = ++gc.tick;
+            ctx->graph_launches++;
+            return cudaGraphLaunch(x.exec, s);
+        }
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return e;
+    const cudaError_t eb = body(s);
+    e = cudaStreamEndCapture(s, &g);
+    if (eb != cudaSuccess || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return eb != cudaSuccess ? eb : e;
+    }
+    cudaGraphExec_t ex = nullptr;
+    e = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return e;
+    if (gc.e.size() >= 16) {
+        size_t old = 0;
+        for (size_t i = 1; i < gc.e.size(); i++)
+            if (gc.e[i].tick < gc.e[old].tick) old = i;
+        cudaGraphExecDestroy(gc.e[old].exec);
+        gc.e.erase(gc.e.begin() + (long)old);
+    }
+    gc.e.push_back(GraphCache::Entry{key, ex, ++gc.tick});
+    ctx->graph_launches++;
+    return cudaGraphLaunch(ex, s);
+}
+
+static uint64_t dbits(double v) {
+    uint64_t b;
+    std::memcpy(&b, &v, 8);
+    return b;
+}
 
 // Device copies (or views) of the inputs shared by every job of a batch.
 int reg_inputs(ldsc_ctx* ctx, int device_pointers, uint64_t n, const double* ld, const double* wld,
@@ -1076,15 +1261,22 @@ extern "C" int ldsc_h2_batch(ldsc_ctx* ctx, const ldsc_h2_args* a, ldsc_h2_resul
     CK(ctx->rg_part.ensure(sizeof(double) * 5 * (size_t)T * nb));
     CK(ctx->rg_sel.ensure(sizeof(double) * 2 * T));
     CK(cudaMemcpyAsync(ctx->rg_jobs.p, jobs.data(), sizeof(RegJob) * T, cudaMemcpyHostToDevice, s));
-    CK(launch_regressions(ctx->rg_jobs.as<RegJob>(), ctx->rg_states.as<RegState>(), ctx->rg_outs.as<RegOut>(),
-                          nullptr, ctx->rg_part.as<double>(), nullptr, d_ld, d_wld, n, nb, a->m_snps, T, s));
-    ctx->kernels += 8;
-    if (a->want_lambda_gc) {
+    // the whole pipeline (8 regression kernels + the median) replays as one graph
+    const std::vector<uint64_t> gkey{1, (uint64_t)T, n, (uint64_t)nb, dbits(a->m_snps), (uint64_t)a->want_lambda_gc,
+                                     (uint64_t)d_ld, (uint64_t)d_wld, (uint64_t)ctx->rg_jobs.p,
+                                     (uint64_t)ctx->rg_states.p, (uint64_t)ctx->rg_outs.p, (uint64_t)ctx->rg_part.p,
+                                     (uint64_t)ctx->rg_sel.p};
+    CK(graph_launch(ctx, gkey, s, [&](cudaStream_t gs) -> cudaError_t {
+        cudaError_t e2 = launch_regressions(ctx->rg_jobs.as<RegJob>(), ctx->rg_states.as<RegState>(),
+                                            ctx->rg_outs.as<RegOut>(), nullptr, ctx->rg_part.as<double>(), nullptr,
+                                            d_ld, d_wld, n, nb, a->m_snps, T, gs);
+        if (e2 != cudaSuccess || !a->want_lambda_gc) return e2;
         // median (src/h2.rs:394-414): middle order statistic, mean of the two for even n
-        CK(launch_select(ctx->rg_jobs.as<RegJob>(), n, n / 2, ctx->rg_sel.as<double>(), T, s));
-        if (n % 2 == 0) CK(launch_select(ctx->rg_jobs.as<RegJob>(), n, n / 2 - 1, ctx->rg_sel.as<double>() + T, T, s));
-        ctx->kernels += n % 2 == 0 ? 2 : 1;
-    }
+        e2 = launch_select(ctx->rg_jobs.as<RegJob>(), n, n / 2, ctx->rg_sel.as<double>(), T, gs);
+        if (e2 != cudaSuccess || n % 2) return e2;
+        return launch_select(ctx->rg_jobs.as<RegJob>(), n, n / 2 - 1, ctx->rg_sel.as<double>() + T, T, gs);
+    }));
+    ctx->kernels += 8 + (a->want_lambda_gc ? (n % 2 == 0 ? 2 : 1) : 0);
     std::vector<RegOut> outs(T);
     std::vector<double> sel(2 * T, NAN);
     CK(cudaMemcpyAsync(outs.data(), ctx->rg_outs.p, sizeof(RegOut) * T, cudaMemcpyDeviceToHost, s));
@@ -1192,13 +1384,22 @@ extern "C" int ldsc_rg_batch(ldsc_ctx* ctx, const ldsc_rg_args* a, ldsc_rg_resul
     RegState* dst = ctx->rg_states.as<RegState>();
     RegOut* dout = ctx->rg_outs.as<RegOut>();
     double* dtd = ctx->rg_tdel.as<double>();
-    // stage 1: the h2 fits; stage 2: the covariance fits, whose weights use them
-    CK(launch_regressions(dj, dst, dout, nullptr, ctx->rg_part.as<double>(), dtd, d_ld, d_wld, n, nb, a->m_snps,
-                          2 * P, s));
-    CK(launch_regressions(dj + 2 * P, dst + 2 * P, dout + 2 * P, dout,
-                          ctx->rg_part.as<double>() + (size_t)2 * P * nb * 5, dtd + (size_t)2 * P * nb, d_ld, d_wld,
-                          n, nb, a->m_snps, P, s));
-    CK(launch_rg_finish(ctx->rg_pairs.as<RgPairIdx>(), dout, dtd, nb, ctx->rg_res.as<RgOut>(), P, s));
+    // stage 1: the h2 fits; stage 2: the covariance fits, whose weights use
+    // them; then the ratio jackknife -- 17 kernels replayed as one graph
+    const std::vector<uint64_t> gkey{2, (uint64_t)P, n, (uint64_t)nb, dbits(a->m_snps), (uint64_t)d_ld,
+                                     (uint64_t)d_wld, (uint64_t)dj, (uint64_t)dst, (uint64_t)dout,
+                                     (uint64_t)ctx->rg_part.p, (uint64_t)dtd, (uint64_t)ctx->rg_pairs.p,
+                                     (uint64_t)ctx->rg_res.p};
+    CK(graph_launch(ctx, gkey, s, [&](cudaStream_t gs) -> cudaError_t {
+        cudaError_t e2 = launch_regressions(dj, dst, dout, nullptr, ctx->rg_part.as<double>(), dtd, d_ld, d_wld, n,
+                                            nb, a->m_snps, 2 * P, gs);
+        if (e2 != cudaSuccess) return e2;
+        e2 = launch_regressions(dj + 2 * P, dst + 2 * P, dout + 2 * P, dout,
+                                ctx->rg_part.as<double>() + (size_t)2 * P * nb * 5, dtd + (size_t)2 * P * nb, d_ld,
+                                d_wld, n, nb, a->m_snps, P, gs);
+        if (e2 != cudaSuccess) return e2;
+        return launch_rg_finish(ctx->rg_pairs.as<RgPairIdx>(), dout, dtd, nb, ctx->rg_res.as<RgOut>(), P, gs);
+    }));
     ctx->kernels += 17;
     std::vector<RgOut> outs(P);
     CK(cudaMemcpyAsync(outs.data(), ctx->rg_res.p, sizeof(RgOut) * P, cudaMemcpyDeviceToHost, s));

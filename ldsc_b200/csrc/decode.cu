@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(256) k_decode_i8(PanelView p, const uint64_t* 
 // src/l2/compute.rs:1406-1412,1595-1603).  Also seeds l2 with the diagonal
 // term r2u_jj * a_j = a_j.
 __global__ void k_finalize(int64_t m, uint64_t n_indiv, RecStats st, const double* __restrict__ annot,
-                           int32_t K, int has_pq, double pq_exp, double* __restrict__ aeff,
+                           uint64_t annot_ld, int32_t K, int has_pq, double pq_exp, double* __restrict__ aeff,
                            float* __restrict__ aeff32, double* __restrict__ l2_init) {
     int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= m) return;
@@ -170,7 +170,7 @@ __global__ void k_finalize(int64_t m, uint64_t n_indiv, RecStats st, const doubl
         st.kappa[r] = kap;
     }
     for (int32_t c = 0; c < K; c++) {
-        double a = annot ? annot[r + (int64_t)c * m] : 1.0;
+        double a = annot ? annot[r + c * annot_ld] : 1.0;
         a *= pq;
         aeff[r + (int64_t)c * m] = a;
         if (aeff32) aeff32[r * K + c] = (float)a;
@@ -257,9 +257,10 @@ cudaError_t launch_repitch(const uint8_t* src, uint64_t bpr, uint8_t* dst, uint6
 
 cudaError_t launch_finalize_stats(int64_t m, uint64_t n_indiv, RecStats st, const double* annot,
                                   int32_t K, int has_pq, double pq_exp, double* aeff, float* aeff32,
-                                  double* l2_init, cudaStream_t stream) {
+                                  double* l2_init, cudaStream_t stream, uint64_t annot_ld) {
     if (m <= 0) return cudaSuccess;
-    k_finalize<<<(unsigned)((m + 255) / 256), 256, 0, stream>>>(m, n_indiv, st, annot, K, has_pq,
+    k_finalize<<<(unsigned)((m + 255) / 256), 256, 0, stream>>>(m, n_indiv, st, annot,
+                                                              annot_ld ? annot_ld : (uint64_t)m, K, has_pq,
                                                               pq_exp, aeff, aeff32, l2_init);
     return cudaGetLastError();
 }

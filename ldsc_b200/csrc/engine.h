@@ -78,7 +78,7 @@ cudaError_t launch_decode_i8(const PanelView& p, const uint64_t* rec_rows, int64
 cudaError_t launch_finalize_stats(int64_t m, uint64_t n_indiv, RecStats st,
                                   const double* annot, int32_t K, int has_pq, double pq_exp,
                                   double* aeff, float* aeff32, double* l2_init,
-                                  cudaStream_t stream);
+                                  cudaStream_t stream, uint64_t annot_ld = 0);
 
 // Standardised f64 columns, row r of `x` = record r, `ld` doubles per row.
 // Rows [r0, r1) of a packed BED body (bpr bytes per row, as in the file) to
