@@ -278,6 +278,184 @@ def run_partitioned_workload(args, ctx, stream):
     panel.close()
 
 
+def run_serving_workload(args, ctx, duration_s: float, rate: float, seed: int = 7):
+    """Serving mix on a resident N=20,000 x M=1,200,000 panel (22
+    chromosomes, 3,500 cM).  Poisson arrivals at `rate` requests/s for
+    `duration_s` seconds: 70% LD-score requests (region M log-uniform in
+    [2,000, 200,000], K in {1, 10, 97} from resident annotations, exact INT8
+    or sketch d=1000, 1 cM, per-SNP masking), 20% h2 over 1,000 traits and 10%
+    rg over 200 trait pairs, both against the resident LD scores of every 6th
+    SNP (200,000 regression SNPs, 200-block jackknife).  Returns the latency
+    and throughput summary."""
+    import threading
+    import queue as pyqueue
+    import torch
+    from ldsc_b200 import synth
+    from ldsc_b200.api import WindowMode, run_l2
+    from ldsc_b200.plink import BimTable
+    from ldsc_b200.serve import Server
+    t_setup = time.perf_counter()
+    spec = synth.spec_resident()
+    chr_, cm, bp = synth.positions(spec)
+    M = spec.m
+    names = [f"rs{i}" for i in range(M)]
+    snps = BimTable(chr_, names, cm, bp, np.arange(M, dtype=np.int64))
+    panel = ctx.synth(spec.n_indiv, M, spec.founders, spec.switch_p, spec.miss, spec.seed)
+    wm = WindowMode.Cm(1.0)
+    # resident LD-score store (K = 1, INT8, masked) and regression inputs
+    l2_all, _, _ = run_l2(ctx, snps, panel, wm, 200, snp_level_masking=True, precision="int8", yes_really=True)
+    reg_idx = np.arange(0, M, 6)
+    n_reg = len(reg_idx)
+    dev = torch.device("cuda")
+    d_ld = torch.from_numpy(np.ascontiguousarray(l2_all[reg_idx, 0])).to(dev)
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    T = 1000
+
+    def uni(lo, hi, n):
+        return lo + (hi - lo) * torch.rand(n, generator=g, device=dev, dtype=torch.float64)
+
+    def randn(r, c):
+        return torch.randn(r, c, generator=g, device=dev, dtype=torch.float64)
+
+    h2 = uni(0.05, 0.5, T)
+    n_t = torch.exp(uni(np.log(1e4), np.log(5e5), T))
+    lm = d_ld.clamp_min(0)[None, :]
+    z = torch.sqrt(n_t[:, None] * h2[:, None] * lm / M) * randn(T, n_reg) + randn(T, n_reg)
+    d_chi2 = z * z
+    del z
+    # trait pairs with genetic correlation rg ~ U(-0.8, 0.8)
+    Pn = 1000
+    rgv = uni(-0.8, 0.8, Pn)
+    h1p, h2p = uni(0.05, 0.5, Pn), uni(0.05, 0.5, Pn)
+    n1p = torch.exp(uni(np.log(1e4), np.log(5e5), Pn))
+    n2p = torch.exp(uni(np.log(1e4), np.log(5e5), Pn))
+    b1 = randn(Pn, n_reg)
+    b2 = rgv[:, None] * b1 + torch.sqrt(1 - rgv[:, None] ** 2) * randn(Pn, n_reg)
+    d_z1 = torch.sqrt(n1p[:, None] * h1p[:, None] * lm / M) * b1 + randn(Pn, n_reg)
+    d_z2 = torch.sqrt(n2p[:, None] * h2p[:, None] * lm / M) * b2 + randn(Pn, n_reg)
+    del b1, b2
+    annot = synth.partitioned_annot(M, seed=seed)
+    d_annot = torch.from_numpy(np.ascontiguousarray(annot.T)).to(dev)   # column c of SNP r at c * M + r
+    del annot
+    torch.cuda.synchronize()
+
+    rng = np.random.default_rng(seed)
+    n_req = max(1, int(rate * duration_s))
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
+    reqs = []
+    for _ in range(n_req):
+        u = rng.random()
+        if u < 0.7:
+            mreg = int(np.exp(rng.uniform(np.log(2000), np.log(200000))))
+            b = int(rng.integers(0, M - mreg))
+            reqs.append(("l2", dict(b=b, e=b + mreg, K=int(rng.choice([1, 10, 97])),
+                                    sketch=None if rng.random() < 0.5 else 1000)))
+        elif u < 0.9:
+            reqs.append(("h2", {}))
+        else:
+            reqs.append(("rg", dict(p0=int(rng.integers(0, Pn - 200)))))
+
+    def region(b, e):
+        return BimTable(chr_[b:e], names[b:e], cm[b:e], bp[b:e], np.arange(b, e, dtype=np.int64))
+
+    def submit(srv, kind, p):
+        if kind == "l2":
+            ad = None if p["K"] == 1 else (d_annot.data_ptr() + 8 * p["b"], M, p["K"])
+            return srv.submit_l2(panel, region(p["b"], p["e"]), wm, 200, row_begin=p["b"], annot_device=ad,
+                                 sketch=p["sketch"], precision="int8", snp_level_masking=True)
+        if kind == "h2":
+            return srv.submit_h2(d_chi2, n_t, d_ld, d_ld, float(M), 200)
+        p0 = p["p0"]
+        return srv.submit_rg(d_z1[p0:p0 + 200], d_z2[p0:p0 + 200], n1p[p0:p0 + 200], n2p[p0:p0 + 200], d_ld, d_ld,
+                             float(M), 200)
+
+    n_slots = args.serve_slots
+    srv = Server(torch.cuda.current_device(), n_slots=n_slots)
+    # warm-up: the shared sketch layout, then every slot grown to the largest
+    # request of each kind (one wave per kind, one job per slot)
+    srv.wait(submit(srv, "l2", dict(b=0, e=5000, K=1, sketch=1000)))
+    for wave in ([("l2", dict(b=i * 150000, e=i * 150000 + 200000, K=97, sketch=None)) for i in range(n_slots)],
+                 [("l2", dict(b=i * 150000, e=i * 150000 + 200000, K=97, sketch=1000)) for i in range(n_slots)],
+                 [("h2", {})] * n_slots + [("rg", dict(p0=0))] * n_slots):
+        for t in [submit(srv, k, p) for k, p in wave]:
+            srv.wait(t)
+    setup_s = time.perf_counter() - t_setup
+
+    done = []
+    q = pyqueue.Queue()
+
+    def waiter():
+        while True:
+            item = q.get()
+            if item is None:
+                return
+            kind, p, t = item
+            try:
+                res, timing = srv.wait(t)
+                pairs = res[2].n_pairs if kind == "l2" else 0
+                done.append((kind, p, timing, pairs, None))
+            except Exception as e:  # noqa: BLE001
+                done.append((kind, p, None, 0, str(e)))
+
+    waiters = [threading.Thread(target=waiter) for _ in range(n_slots + 2)]
+    for w in waiters:
+        w.start()
+    st0 = srv.stats()
+    t0 = time.perf_counter()
+    late = []
+    for (kind, p), ta in zip(reqs, arrivals):
+        now = time.perf_counter() - t0
+        if ta > now:
+            time.sleep(ta - now)
+        else:
+            late.append(now - ta)
+        q.put((kind, p, submit(srv, kind, p)))
+    for _ in waiters:
+        q.put(None)
+    for w in waiters:
+        w.join()
+    wall = time.perf_counter() - t0
+    st1 = srv.stats()
+    srv.close()
+    panel.close()
+
+    ok = [d for d in done if d[4] is None]
+    lat = np.array([d[2].latency_ms for d in ok])
+    que = np.array([d[2].queue_ms for d in ok])
+    run = np.array([d[2].run_ms for d in ok])
+
+    def pct(a):
+        return {"p50": float(np.percentile(a, 50)), "p99": float(np.percentile(a, 99)), "mean": float(np.mean(a)),
+                "max": float(np.max(a)), "n": int(len(a))} if len(a) else None
+
+    def label(kind, p):
+        if kind != "l2":
+            return kind
+        return f"l2_{'sketch1000' if p['sketch'] else 'int8'}_K{p['K']}"
+
+    by = {}
+    for d in ok:
+        by.setdefault(label(d[0], d[1]), []).append(d[2].latency_ms)
+    pairs = float(sum(d[3] for d in ok))
+    return {"workload": "serving", "metric": "request latency (ms) and throughput at a stated Poisson rate",
+            "rate_req_s": rate, "duration_s": duration_s, "requests": n_req, "completed": len(ok),
+            "failed": len(done) - len(ok), "errors": sorted({d[4] for d in done if d[4]})[:3],
+            "wall_s": wall, "throughput_req_s": len(ok) / wall, "l2_pairs_per_s": pairs / wall,
+            "latency_ms": pct(lat), "queue_ms": pct(que), "run_ms": pct(run),
+            "by_kind_latency_ms": {k: pct(np.array(v)) for k, v in sorted(by.items())},
+            "arrival_lag_ms_p99": float(np.percentile(late, 99) * 1e3) if late else 0.0,
+            "slots": n_slots, "graph_launches": st1["graph_launches"] - st0["graph_launches"],
+            "gpu_launches": st1["kernels"] - st0["kernels"], "setup_s": setup_s,
+            "config": {"panel": "N=20,000 x M=1,200,000, 22 chromosomes, 3,500 cM, 1% missing",
+                       "l2": "70%: region M log-uniform [2k, 200k], K in {1,10,97} (resident annotations), "
+                             "INT8 exact or sketch d=1000, 1 cM, per-SNP masking",
+                       "h2": "20%: 1,000 traits x 200,000 regression SNPs, 200 blocks",
+                       "rg": "10%: 200 trait pairs x 200,000 regression SNPs, 200 blocks",
+                       "traits": "z = sqrt(N h2 l2 / M) b + e, h2 ~ U(0.05, 0.5), N log-uniform [1e4, 5e5], "
+                                 "chi2 = z^2; rg ~ U(-0.8, 0.8)"}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -287,7 +465,11 @@ def main():
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="biobank", choices=["biobank", "profile", "sketch", "partitioned"])
+    ap.add_argument("--workload", default="biobank",
+                    choices=["biobank", "profile", "sketch", "partitioned", "serving"])
+    ap.add_argument("--serve-rate", type=float, default=40.0, help="serving: Poisson arrivals per second")
+    ap.add_argument("--serve-seconds", type=float, default=30.0, help="serving: length of the arrival window")
+    ap.add_argument("--serve-slots", type=int, default=6, help="serving: concurrent job slots")
     ap.add_argument("--sketch-d", default="200,1000,5000")
     ap.add_argument("--sketch-snps", type=int, default=0, help="truncate the sketch panel (profiling)")
     args = ap.parse_args()
@@ -329,6 +511,9 @@ def main():
         return
     if args.workload == "partitioned":
         run_partitioned_workload(args, ctx, stream)
+        return
+    if args.workload == "serving":
+        print(json.dumps(run_serving_workload(args, ctx, args.serve_seconds, args.serve_rate)), flush=True)
         return
 
     spec = workload_spec(seed_offset=rank, workload=args.workload)

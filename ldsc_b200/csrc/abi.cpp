@@ -36,18 +36,30 @@ namespace {
 struct DevBuf {
     void* p = nullptr;
     size_t cap = 0;
+    // Context workspace is allocated stream-ordered on the context's stream
+    // (from the device's memory pool): growing or freeing it then does not
+    // wait for other contexts' work, as cudaFree would.
+    cudaStream_t* owner = nullptr;
     cudaError_t ensure(size_t bytes) {
         if (bytes <= cap && p) return cudaSuccess;
-        if (p) cudaFree(p);
-        p = nullptr;
-        cap = 0;
+        release();
         if (bytes == 0) bytes = 16;
-        cudaError_t e = cudaMalloc(&p, bytes);
-        if (e == cudaSuccess) cap = bytes;
+        cudaError_t e = owner ? cudaMallocAsync(&p, bytes, *owner) : cudaMalloc(&p, bytes);
+        if (e == cudaSuccess) {
+            cap = bytes;
+        } else {
+            p = nullptr;
+            cudaGetLastError();
+        }
         return e;
     }
     void release() {
-        if (p) cudaFree(p);
+        if (p) {
+            if (owner)
+                cudaFreeAsync(p, *owner);
+            else
+                cudaFree(p);
+        }
         p = nullptr;
         cap = 0;
     }
@@ -192,6 +204,15 @@ int ldsc_ctx_create(int device, uint32_t flags, ldsc_ctx** out) {
         return LDSC_E_CUDA;
     }
     c->stream = c->own;
+    for (DevBuf* b : c->workspace()) b->owner = &c->stream;
+    for (DevBuf* b : {&c->sk.perm, &c->sk.seg, &c->sk.wseg, &c->sk.pp}) b->owner = &c->stream;
+    // keep freed workspace in the pool for the next call instead of returning it
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t keep_all = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep_all);
+    }
+    cudaGetLastError();
     *out = c;
     return LDSC_OK;
 }
@@ -205,6 +226,7 @@ int ldsc_ctx_destroy(ldsc_ctx* ctx) {
     for (DevBuf* b : bufs) b->release();
     ctx->sk.release();
     ctx->graphs.clear();
+    cudaStreamSynchronize(ctx->stream);
     for (cudaEvent_t e : ctx->feed_ev) cudaEventDestroy(e);
     for (cudaEvent_t e : {ctx->feed_t0, ctx->feed_t1, ctx->feed_go, ctx->up_ev})
         if (e) cudaEventDestroy(e);
