@@ -91,7 +91,7 @@ struct GraphCache {
 // Bucket-major CountSketch layout of a panel: the individuals' order, the
 // segment tables and the panel rows rewritten in that order.
 struct SketchCache {
-    DevBuf perm, seg, wseg, pp;
+    DevBuf perm, seg, pp;
     uint64_t n = 0, key = 0, pitch_words = 0;
     uint32_t d = 0;
     bool valid = false;
@@ -99,7 +99,6 @@ struct SketchCache {
     void release() {
         perm.release();
         seg.release();
-        wseg.release();
         pp.release();
         valid = false;
     }
@@ -205,7 +204,7 @@ int ldsc_ctx_create(int device, uint32_t flags, ldsc_ctx** out) {
     }
     c->stream = c->own;
     for (DevBuf* b : c->workspace()) b->owner = &c->stream;
-    for (DevBuf* b : {&c->sk.perm, &c->sk.seg, &c->sk.wseg, &c->sk.pp}) b->owner = &c->stream;
+    for (DevBuf* b : {&c->sk.perm, &c->sk.seg, &c->sk.pp}) b->owner = &c->stream;
     // keep freed workspace in the pool for the next call instead of returning it
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
@@ -477,11 +476,9 @@ int sketch_prepare(ldsc_ctx* ctx, const ldsc_panel* panel, uint64_t n_used, uint
     c.valid = false;
     CK(c.perm.ensure(4 * (size_t)n_used));
     CK(c.seg.ensure(4 * o.seg_off.size()));
-    CK(c.wseg.ensure(4 * o.word_seg.size()));
     CK(c.pp.ensure((size_t)4 * pitch_words * (panel->n_snp ? panel->n_snp : 1)));
     CK(cudaMemcpyAsync(c.perm.p, o.perm.data(), 4 * (size_t)n_used, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(c.seg.p, o.seg_off.data(), 4 * o.seg_off.size(), cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(c.wseg.p, o.word_seg.data(), 4 * o.word_seg.size(), cudaMemcpyHostToDevice, s));
     PanelView pv{panel->rows, panel->n_snp, panel->n_indiv, panel->bpr, panel->pitch};
     CK(launch_sketch_permute(pv, c.perm.as<int32_t>(), n_used, c.pp.as<uint32_t>(), pitch_words, s));
     ctx->kernels++;
@@ -605,6 +602,8 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
                                              " is out of bounds (must be 3 <= d < n_indiv=" +
                                              std::to_string(n_used) + ")");
     if (d > 12288) return fail(ctx, LDSC_E_UNSUPPORTED, "--sketch d > 12288 is not supported on the GPU");
+    if (d && !sketch_supported(n_used, d))
+        return fail(ctx, LDSC_E_UNSUPPORTED, "--sketch: too many individuals for the sketch kernel's shared memory");
     if (a->precision != LDSC_PRECISION_FP64 && a->precision != LDSC_PRECISION_INT8)
         return fail(ctx, LDSC_E_INVALID, "unknown precision");
     if (a->window_mode < 0 || a->window_mode > 2) return fail(ctx, LDSC_E_INVALID, "invalid window mode");
@@ -909,7 +908,7 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
     } else if (d) {
         // fused: moments + CountSketch rows in one pass over the permuted panel
         CK(launch_sketch_seg(skc->pp.as<uint32_t>() + (rr ? 0 : a->row_begin * skc->pitch_words), skc->pitch_words,
-                             rr, m, n_used, skc->seg.as<int32_t>(), skc->wseg.as<int32_t>(), d, st,
+                             rr, m, n_used, skc->seg.as<int32_t>(), d, st,
                              maf_aware ? 1 : 0, 1, ctx->xsk.as<float>(), ld_sk, s));
         e_sk = ev.mark();
     } else {
@@ -1060,6 +1059,8 @@ int ldsc_sketch_project(ldsc_ctx* ctx, const ldsc_panel* panel, uint64_t b, uint
     if (m == 0) return LDSC_OK;
     const uint64_t n_used = keep ? n_keep : panel->n_indiv;
     if (n_used == 0) return fail(ctx, LDSC_E_INVALID, "no individuals");
+    if (!sketch_supported(n_used, d))
+        return fail(ctx, LDSC_E_UNSUPPORTED, "too many individuals for the sketch kernel's shared memory");
     for (uint64_t i = 0; i < n_used; i++) {
         if (bucket[i] >= d) return fail(ctx, LDSC_E_INVALID, "bucket index >= d");
         if (keep && (keep[i] < 0 || (uint64_t)keep[i] >= panel->n_indiv))
@@ -1083,7 +1084,7 @@ int ldsc_sketch_project(ldsc_ctx* ctx, const ldsc_panel* panel, uint64_t b, uint
     st.s = ctx->st_s.as<int32_t>();
     st.q = ctx->st_q.as<int32_t>();
     CK(launch_sketch_seg(ctx->sk.pp.as<uint32_t>(), ctx->sk.pitch_words, ctx->recrows.as<uint64_t>(), m, n_used,
-                         ctx->sk.seg.as<int32_t>(), ctx->sk.wseg.as<int32_t>(), d, st, 0, 0, ctx->xsk.as<float>(), d,
+                         ctx->sk.seg.as<int32_t>(), d, st, 0, 0, ctx->xsk.as<float>(), d,
                          s));
     ctx->kernels += 1;
     CK(cudaMemcpyAsync(out, ctx->xsk.p, 4 * (size_t)m * d, cudaMemcpyDeviceToHost, s));

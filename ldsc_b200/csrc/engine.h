@@ -112,13 +112,14 @@ cudaError_t launch_sketch_permute(const PanelView& p, const int32_t* perm, uint6
 // CountSketch, step 2 (per call): per record, run sums over the permuted row,
 // per-SNP moments into st.n/s/q (and q3/q4 when want_moments), standardised
 // and renormalised bucket values.  seg_off: 2d+1 run starts (run k = bucket
-// k/2, sign + for even k); word_seg[w]: run containing position 16w.
+// k/2, sign + for even k).
 // out: m rows of `ld` floats, or with split = 1 the tensor-core operand form:
 // rows 2r = tf32(v) and 2r+1 = tf32(v - tf32(v)), `ld` floats each.
 cudaError_t launch_sketch_seg(const uint32_t* pp, uint64_t pp_pitch_words, const uint64_t* rec_rows, int64_t m,
-                              uint64_t n_used, const int32_t* seg_off, const int32_t* word_seg, uint32_t d,
-                              RecStats st, int want_moments, int split, float* out, uint64_t ld,
-                              cudaStream_t stream);
+                              uint64_t n_used, const int32_t* seg_off, uint32_t d, RecStats st,
+                              int want_moments, int split, float* out, uint64_t ld, cudaStream_t stream);
+// Whether the sketch kernel's shared memory holds n_used individuals and d buckets.
+bool sketch_supported(uint64_t n_used, uint32_t d);
 
 // CountSketch band Gram on tcgen05 kind::tf32 over split rows (hi/lo
 // interleaved, `ld` floats per row, ld*4 a multiple of 128) + quadratic

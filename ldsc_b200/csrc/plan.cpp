@@ -155,14 +155,6 @@ SketchOrder sketch_order(uint64_t n_used, uint32_t d, const uint32_t* bucket, co
         const uint32_t k = 2 * bucket[i] + (sign[i] < 0 ? 1 : 0);
         o.perm[fill[k]++] = (int32_t)(keep ? keep[i] : (int64_t)i);
     }
-    const uint64_t words = (n_used + 15) / 16;
-    o.word_seg.assign(words + 4, (int32_t)nseg);
-    uint32_t k = 0;
-    for (uint64_t w = 0; w < words; w++) {
-        const int64_t pos = (int64_t)w * 16;
-        while (k + 1 < nseg + 1 && o.seg_off[k + 1] <= pos) k++;
-        o.word_seg[w] = (int32_t)k;
-    }
     return o;
 }
 

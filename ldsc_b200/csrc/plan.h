@@ -45,7 +45,6 @@ void countsketch_hash(uint64_t n, uint32_t d, uint64_t seed, uint32_t* bucket, f
 struct SketchOrder {
     std::vector<int32_t> perm;      // FAM index at each permuted position
     std::vector<int32_t> seg_off;   // 2d + 1 run starts
-    std::vector<int32_t> word_seg;  // run containing position 16 w
 };
 SketchOrder sketch_order(uint64_t n_used, uint32_t d, const uint32_t* bucket, const float* sign,
                          const int64_t* keep);

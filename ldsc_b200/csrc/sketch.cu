@@ -13,8 +13,8 @@
 // k_sketch_permute rewrites every panel row in that order (2-bit codes, 16 per
 // word), after which each (bucket, sign) group is a contiguous run of
 // positions.  k_sketch_seg then streams a permuted row once and forms the
-// bucket sums with popcounts on 32-bit words (16 genotypes at a time); the
-// same popcounts give the per-SNP moments.
+// bucket sums from popcount prefix sums at the run boundaries (16 genotypes
+// per 32-bit word); the same popcounts give the per-SNP moments.
 //
 // mean / inv_std are the reference's f32-rounded values; each bucket value is
 // formed exactly and rounded to f32 once (the reference accumulates f32 in
@@ -81,167 +81,214 @@ __global__ void __launch_bounds__(NT) k_sketch_permute(PanelView p, const int32_
     }
 }
 
-__device__ __forceinline__ uint32_t span_mask(uint32_t a, uint32_t b) {  // even bits of positions [a, b)
-    const uint32_t hi = b >= 16 ? 0xFFFFFFFFu : ((1u << (2 * b)) - 1u);
-    const uint32_t lo = (1u << (2 * a)) - 1u;
-    return hi & ~lo & kEven;
+// Bucket sums from prefix sums.  Position p of the permuted row has
+//     g = 2 - (lo + hi) - miss,   present = 1 - miss
+// (codes 00 -> 2, 10 -> 1, 11 -> 0, 01 = missing -> 0), so over any span of
+// positions  sum g = 2 len - popc(bits) - popc(miss)  and  present = len -
+// popc(miss).  With the prefix (sum g, present) at every run boundary k,
+// bucket b is
+//     S1_b = (PF[2b+1] - PF[2b]) - (PF[2b+2] - PF[2b+1])   (g sums; S0_b with present)
+// and row moments come from the totals:
+//     n = present, s = sum g, q = s + 2 #2, q3 = s + 6 #2, q4 = s + 14 #2
+// (#2 = number of genotype-2 codes).
+//
+// Two phases per record.  (1) Streaming: each warp owns a contiguous block of
+// the row's 16-byte quads and walks it 64 quads at a time, two adjacent quads
+// per lane (coalesced loads, branch-free popcounts); a warp scan gives the
+// prefix (popc, missing) at the start of every quad, kept in shared memory.
+// (2) Boundaries: after a block scan over the warps, thread t takes the
+// buckets [d t / NT, d (t+1) / NT) and walks their boundaries in order; each
+// prefix is the quad prefix plus popcounts inside one quad (re-read from
+// L1/L2, once per quad per thread), and each bucket's value is formed on the
+// spot.  No atomics, and nothing needs clearing between records.
+__device__ __forceinline__ uint32_t miss_bits(uint32_t x) { return x & ~(x >> 1) & kEven; }
+__device__ __forceinline__ uint32_t two_bits(uint32_t x) { return ~(x | (x >> 1)) & kEven; }
+
+template <typename T>
+__device__ __forceinline__ T warp_incl_scan(T v, int lane) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const T u = __shfl_up_sync(0xFFFFFFFFu, v, o);
+        if (lane >= o) v += u;
+    }
+    return v;
 }
 
-// One CTA per record, one pass over the permuted row: per-SNP moments and
-// per-bucket sums S1 (sum sign * g) and S0 (sum sign * present), then the
-// standardised, renormalised bucket values.  Each thread takes a contiguous
-// range of words (loaded QB x 16 bytes at a time into registers); a bucket
-// that lies wholly inside one thread's range is written with a plain store,
-// only the two buckets at the ends of a range use shared-memory atomics.
-// Output row r: `ld` floats (zero padded past d), or with split the hi/lo
-// tensor-core rows 2r / 2r+1.
-__global__ void __launch_bounds__(NT, 4) k_sketch_seg(const uint32_t* __restrict__ pp, uint64_t pp_pitch_words,
-                                                   const uint64_t* __restrict__ rec_rows, int64_t m, uint64_t n_used,
-                                                   const int32_t* __restrict__ seg_off,
-                                                   const int32_t* __restrict__ word_seg, uint32_t d, RecStats st,
-                                                   int want_moments, int split, float* __restrict__ out,
-                                                   uint64_t ld) {
-    extern __shared__ int32_t sh[];
-    int32_t* Z = sh;       // S1 per bucket
-    int32_t* P = sh + d;   // S0 per bucket
-    __shared__ int64_t red[5][NT / 32];
-    __shared__ double dred[NT / 32];
-    __shared__ double s_mean, s_inv;
-    const uint64_t words = (n_used + 15) / 16;
-    const uint32_t nseg = 2 * d;
-    const uint64_t quads = (words + 3) / 4;
-    const uint64_t q0 = quads * threadIdx.x / NT, q1 = quads * (threadIdx.x + 1) / NT;
+constexpr int SNT = 128;       // threads of the sketch kernel
+constexpr int SNW = SNT / 32;  // warps
+constexpr int CHUNK_Q = 64;    // quads per warp step (2 per lane)
+
+__host__ __device__ inline uint64_t sketch_quads(uint64_t n_used) { return ((n_used + 15) / 16 + 3) / 4; }
+
+// Dynamic shared memory of the sketch kernel: per-quad prefixes and the d
+// bucket values.
+__host__ __device__ inline size_t sketch_smem(uint64_t n_used, uint32_t d) {
+    return 8 * sketch_quads(n_used) + 4 * (size_t)d + 16;
+}
+
+// One CTA per record (grid-stride over records).  Output row r: `ld` floats
+// (zero padded past d), or with split the hi/lo tensor-core rows 2r / 2r+1.
+__global__ void __launch_bounds__(SNT, 8) k_sketch_seg(const uint32_t* __restrict__ pp, uint64_t pp_pitch_words,
+                                                    const uint64_t* __restrict__ rec_rows, int64_t m, uint64_t n_used,
+                                                    const int32_t* __restrict__ seg_off, uint32_t d, RecStats st,
+                                                    int want_moments, int split, float* __restrict__ out,
+                                                    uint64_t ld) {
+    extern __shared__ __align__(16) int32_t sh[];
+    const uint32_t quads = (uint32_t)sketch_quads(n_used);  // the permuted pitch is 4 quads' worth of words, padded
+    int2* Pq = reinterpret_cast<int2*>(sh);                  // (popc, missing) before each quad, warp-relative
+    float* ob = reinterpret_cast<float*>(sh + 2 * quads);    // bucket values
+    __shared__ int32_t wa[SNW], wm[SNW], wt[SNW];
+    __shared__ double dred[SNW];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t wq0 = (uint32_t)((uint64_t)quads * warp / SNW), wq1 = (uint32_t)((uint64_t)quads * (warp + 1) / SNW);
+    const uint32_t b0 = (uint32_t)((uint64_t)d * threadIdx.x / SNT), b1 = (uint32_t)((uint64_t)d * (threadIdx.x + 1) / SNT);
+    const int32_t row_len = (int32_t)(64 * quads);
+    __shared__ uint32_t wstart[SNW];  // first quad of each warp's block
+    if (threadIdx.x < SNW) wstart[threadIdx.x] = (uint32_t)((uint64_t)quads * threadIdx.x / SNW);
+    __syncthreads();
     for (int64_t r = blockIdx.x; r < m; r += gridDim.x) {
         const uint64_t brow = rec_rows ? rec_rows[r] : (uint64_t)r;
         const uint4* row = reinterpret_cast<const uint4*>(pp + brow * pp_pitch_words);
-        for (uint32_t b = threadIdx.x; b < 2 * d; b += NT) sh[b] = 0;
-        __syncthreads();
-        // counts over the row: present, genotype 1, genotype 2 (sum g^k = #1 + 2^k #2)
-        uint32_t cn = 0, c1 = 0, c2 = 0;
-        if (q0 < q1) {
-            uint32_t k = (uint32_t)__ldg(word_seg + q0 * 4);
-            int32_t cut = __ldg(seg_off + k + 1);
-            int32_t sg = (k & 1u) ? -1 : 1;
-            const uint32_t first_b = k >> 1;
-            uint32_t cur_b = first_b;
-            uint32_t zr = 0, pr = 0;       // sums over the current run
-            int32_t zacc = 0, pacc = 0;    // signed sums over the current bucket
-            int32_t base = (int32_t)(q0 * 64);
-            uint4 nxt = __ldg(row + q0);
-            for (uint64_t q = q0; q < q1; q++) {
-                const uint4 v = nxt;
-                if (q + 1 < q1) nxt = __ldg(row + q + 1);
-                const uint32_t wv[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-                for (int t = 0; t < 4; t++, base += 16) {
-                    const uint32_t x = wv[t];
-                    const uint32_t lo = x & kEven, hi = (x >> 1) & kEven;
-                    const uint32_t one = hi & ~lo, two = ~(lo | hi) & kEven, pres = (~lo | hi) & kEven;
-                    const uint32_t p1 = __popc(one), p2 = __popc(two), pn = __popc(pres);
-                    cn += pn;
-                    c1 += p1;
-                    c2 += p2;
-                    if (cut > base + 16) {  // the whole word lies in run k (or past the last run)
-                        zr += p1 + 2 * p2;
-                        pr += pn;
-                        continue;
-                    }
-                    uint32_t a = 0;
-                    while (true) {
-                        const uint32_t b = cut < base + 16 ? (uint32_t)(cut - base) : 16u;
-                        const uint32_t msk = span_mask(a, b);
-                        zr += __popc(one & msk) + 2 * __popc(two & msk);
-                        pr += __popc(pres & msk);
-                        // run k ends at position base + b
-                        zacc += sg * (int32_t)zr;
-                        pacc += sg * (int32_t)pr;
-                        zr = pr = 0;
-                        k++;
-                        if ((k >> 1) != cur_b || k >= nseg) {
-                            if (cur_b == first_b) {
-                                if (zacc) atomicAdd(&Z[cur_b], zacc);
-                                if (pacc) atomicAdd(&P[cur_b], pacc);
-                            } else {
-                                Z[cur_b] = zacc;
-                                P[cur_b] = pacc;
-                            }
-                            zacc = pacc = 0;
-                            cur_b = k >> 1;
-                        }
-                        if (k >= nseg) {
-                            cut = 0x7FFFFFFF;
-                            break;
-                        }
-                        cut = __ldg(seg_off + k + 1);
-                        sg = (k & 1u) ? -1 : 1;
-                        a = b;
-                        if (a >= 16) break;
-                        if (cut > base + 16) {  // the new run covers the rest of the word
-                            const uint32_t rest = span_mask(a, 16);
-                            zr += __popc(one & rest) + 2 * __popc(two & rest);
-                            pr += __popc(pres & rest);
-                            break;
-                        }
-                    }
-                }
-            }
-            if (k < nseg) {  // bucket continuing past this thread's range
-                zacc += sg * (int32_t)zr;
-                pacc += sg * (int32_t)pr;
-                if (zacc) atomicAdd(&Z[cur_b], zacc);
-                if (pacc) atomicAdd(&P[cur_b], pacc);
-            }
+        // ---- phase 1: stream the warp's quads ----
+        int32_t carryA = 0, carryM = 0;
+        uint32_t T2 = 0;
+        uint4 n0 = make_uint4(0, 0, 0, 0), n1 = n0;
+        if (wq0 + 2 * lane < wq1) n0 = __ldg(row + wq0 + 2 * lane);
+        if (wq0 + 2 * lane + 1 < wq1) n1 = __ldg(row + wq0 + 2 * lane + 1);
+        for (uint32_t c0 = wq0; c0 < wq1; c0 += CHUNK_Q) {
+            const uint32_t qa = c0 + 2 * lane;
+            const bool l0 = qa < wq1, l1 = qa + 1 < wq1;
+            const uint4 v0 = n0, v1 = n1;
+            if (qa + CHUNK_Q < wq1) n0 = __ldg(row + qa + CHUNK_Q);
+            if (qa + CHUNK_Q + 1 < wq1) n1 = __ldg(row + qa + CHUNK_Q + 1);
+            const int32_t a0 = __popc(v0.x) + __popc(v0.y) + __popc(v0.z) + __popc(v0.w);
+            const int32_t a1 = __popc(v1.x) + __popc(v1.y) + __popc(v1.z) + __popc(v1.w);
+            const int32_t m0 = __popc(miss_bits(v0.x) | (miss_bits(v0.y) << 1)) +
+                               __popc(miss_bits(v0.z) | (miss_bits(v0.w) << 1));
+            const int32_t m1 = __popc(miss_bits(v1.x) | (miss_bits(v1.y) << 1)) +
+                               __popc(miss_bits(v1.z) | (miss_bits(v1.w) << 1));
+            const uint32_t t0 = __popc(two_bits(v0.x) | (two_bits(v0.y) << 1)) +
+                                __popc(two_bits(v0.z) | (two_bits(v0.w) << 1));
+            const uint32_t t1 = __popc(two_bits(v1.x) | (two_bits(v1.y) << 1)) +
+                                __popc(two_bits(v1.z) | (two_bits(v1.w) << 1));
+            const int32_t la = (l0 ? a0 : 0) + (l1 ? a1 : 0), lm = (l0 ? m0 : 0) + (l1 ? m1 : 0);
+            T2 += (l0 ? t0 : 0u) + (l1 ? t1 : 0u);
+            const int32_t ia = warp_incl_scan(la, lane), im = warp_incl_scan(lm, lane);
+            const int32_t ea = carryA + ia - la, em = carryM + im - lm;
+            if (l0) Pq[qa] = make_int2(ea, em);
+            if (l1) Pq[qa + 1] = make_int2(ea + a0, em + m0);
+            carryA += __shfl_sync(0xFFFFFFFFu, ia, 31);
+            carryM += __shfl_sync(0xFFFFFFFFu, im, 31);
         }
-        const uint32_t cs = c1 + 2 * c2, cq = c1 + 4 * c2, c3 = c1 + 8 * c2, c4 = c1 + 16 * c2;
-        int64_t mom[5] = {warp_sum(cn), warp_sum(cs), warp_sum(cq), warp_sum(c3), warp_sum(c4)};
-        if ((threadIdx.x & 31) == 0)
-            for (int i = 0; i < 5; i++) red[i][threadIdx.x >> 5] = mom[i];
-        __syncthreads();
-        if (threadIdx.x < 32) {
-            int64_t t[5];
-#pragma unroll
-            for (int i = 0; i < 5; i++) t[i] = warp_sum(threadIdx.x < NT / 32 ? red[i][threadIdx.x] : (int64_t)0);
-            if (threadIdx.x == 0) {
-                const int64_t n = t[0], s = t[1], q = t[2];
-                st.n[r] = (int32_t)n;
-                st.s[r] = (int32_t)s;
-                st.q[r] = (int32_t)q;
-                if (want_moments && st.q3) {
-                    st.q3[r] = (int32_t)t[3];
-                    st.q4[r] = (int32_t)t[4];
-                }
-                // normalize_col_f32_with_stats constants (src/l2/normalize.rs:115-154)
-                const double mean = n > 0 ? (double)s / (double)n : 0.0;
-                const double css = (double)q - (double)n * mean * mean;
-                const double sd = sqrt(css / (double)n_used);
-                s_mean = (double)(float)mean;
-                s_inv = sd > 0.0 ? (double)(float)(1.0 / sd) : 0.0;
-            }
+        const int32_t t2w = warp_sum((int32_t)T2);
+        if (lane == 0) {
+            wa[warp] = carryA;
+            wm[warp] = carryM;
+            wt[warp] = t2w;
         }
         __syncthreads();
-        const double mean = s_mean, inv = s_inv;
+        // ---- block scan over the warps: offsets and row totals ----
+        int32_t A = 0, MS = 0, TT = 0;
+#pragma unroll
+        for (int w = 0; w < SNW; w++) {
+            A += wa[w];
+            MS += wm[w];
+            TT += wt[w];
+        }
+        const int32_t G = 2 * row_len - A - MS, N = row_len - MS;  // padding positions are missing: no effect
+        if (threadIdx.x == 0) {
+            st.n[r] = N;
+            st.s[r] = G;
+            st.q[r] = G + 2 * TT;
+            if (want_moments && st.q3) {
+                st.q3[r] = G + 6 * TT;
+                st.q4[r] = G + 14 * TT;
+            }
+        }
+        // normalize_col_f32_with_stats constants (src/l2/normalize.rs:115-154)
+        const double dmean = N > 0 ? (double)G / (double)N : 0.0;
+        const double css = (double)(G + 2 * TT) - (double)N * dmean * dmean;
+        const double sd = sqrt(css / (double)n_used);
+        const double mean = (double)(float)dmean;
+        const double inv = sd > 0.0 ? (double)(float)(1.0 / sd) : 0.0;
+        // ---- phase 2: this thread's buckets ----
+        // Boundaries 2 b0 .. 2 b1 in groups of four: the group's positions are
+        // loaded one group ahead and its four quads are loaded together.
         double part = 0.0;
-        float* ov = reinterpret_cast<float*>(Z);  // bucket values replace S1 in shared memory
-        for (uint32_t b = threadIdx.x; b < d; b += NT) {
-            const float o = (float)(inv * ((double)Z[b] - mean * (double)P[b]));
-            ov[b] = o;
-            part += (double)o * (double)o;
+        if (b0 < b1) {
+            const uint32_t kb = 2 * b0, ke = 2 * b1 + 1;
+            int32_t pn[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) pn[u] = kb + u < ke ? __ldg(seg_off + kb + u) : row_len;
+            int32_t g1 = 0, n1w = 0, g2 = 0, n2w = 0;  // prefixes at the previous two boundaries
+            for (uint32_t k = kb; k < ke; k += 4) {
+                int32_t pc[4];
+                uint4 qv[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    pc[u] = pn[u];
+                    pn[u] = k + 4 + u < ke ? __ldg(seg_off + k + 4 + u) : row_len;
+                }
+#pragma unroll
+                for (int u = 0; u < 4; u++) qv[u] = pc[u] < row_len ? __ldg(row + (pc[u] >> 6)) : make_uint4(0, 0, 0, 0);
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    if (k + u >= ke) break;
+                    const int32_t p = pc[u];
+                    int32_t pg = G, pnr = N;  // at or past the row end: the totals
+                    if (p < row_len) {
+                        const uint32_t q = (uint32_t)p >> 6;
+                        // plus the offset of the warp that owns quad q
+                        const int2 pq = Pq[q];
+                        int32_t pa = pq.x, pm = pq.y;
+#pragma unroll
+                        for (int o = 0; o < SNW - 1; o++)
+                            if (q >= wstart[o + 1]) {
+                                pa += wa[o];
+                                pm += wm[o];
+                            }
+                        const uint4 v = qv[u];
+                        const int t = (p >> 4) & 3, j = p & 15;
+                        const uint32_t msk = j ? (0xFFFFFFFFu >> (32 - 2 * j)) : 0u;
+                        const uint32_t mk0 = t > 0 ? 0xFFFFFFFFu : (t == 0 ? msk : 0u);
+                        const uint32_t mk1 = t > 1 ? 0xFFFFFFFFu : (t == 1 ? msk : 0u);
+                        const uint32_t mk2 = t > 2 ? 0xFFFFFFFFu : (t == 2 ? msk : 0u);
+                        const uint32_t mk3 = t == 3 ? msk : 0u;
+                        pa += __popc(v.x & mk0) + __popc(v.y & mk1) + __popc(v.z & mk2) + __popc(v.w & mk3);
+                        pm += __popc(miss_bits(v.x) & mk0) + __popc(miss_bits(v.y) & mk1) +
+                              __popc(miss_bits(v.z) & mk2) + __popc(miss_bits(v.w) & mk3);
+                        pg = 2 * p - pa - pm;
+                        pnr = p - pm;
+                    }
+                    const uint32_t idx = k + u - kb;
+                    if (idx >= 2 && !(idx & 1)) {  // bucket b0 + idx/2 - 1 is complete
+                        const int32_t s1 = (g1 - g2) - (pg - g1), s0 = (n1w - n2w) - (pnr - n1w);
+                        const float o = (float)(inv * ((double)s1 - mean * (double)s0));
+                        ob[b0 + idx / 2 - 1] = o;
+                        part += (double)o * (double)o;
+                    }
+                    g2 = g1;
+                    n2w = n1w;
+                    g1 = pg;
+                    n1w = pnr;
+                }
+            }
         }
         part = warp_sum(part);
-        if ((threadIdx.x & 31) == 0) dred[threadIdx.x >> 5] = part;
+        if (lane == 0) dred[warp] = part;
         __syncthreads();
         double nrm = 0.0;
 #pragma unroll
-        for (int w = 0; w < NT / 32; w++) nrm += dred[w];
+        for (int w = 0; w < SNW; w++) nrm += dred[w];
         const float scale = nrm > 0.0 ? (float)sqrt((double)n_used / nrm) : 1.0f;
         float* orow = out + (uint64_t)r * (split ? 2 : 1) * ld;
         if (split) {
             // tensor-core operand rows: 2r = tf32(v), 2r+1 = tf32(v - tf32(v))
             float* lrow = orow + ld;
-            for (uint64_t b = threadIdx.x; b < ld; b += NT) {
+            for (uint64_t b = threadIdx.x; b < ld; b += SNT) {
                 float hi = 0.f, lo = 0.f;
                 if (b < d) {
-                    const float v = nrm > 0.0 ? ov[b] * scale : ov[b];
+                    const float v = nrm > 0.0 ? ob[b] * scale : ob[b];
                     hi = to_tf32(v);
                     lo = to_tf32(v - hi);
                 }
@@ -249,10 +296,9 @@ __global__ void __launch_bounds__(NT, 4) k_sketch_seg(const uint32_t* __restrict
                 lrow[b] = lo;
             }
         } else {
-            for (uint64_t b = threadIdx.x; b < ld; b += NT)
-                orow[b] = b < d ? (nrm > 0.0 ? ov[b] * scale : ov[b]) : 0.f;
+            for (uint64_t b = threadIdx.x; b < ld; b += SNT) orow[b] = b < d ? (nrm > 0.0 ? ob[b] * scale : ob[b]) : 0.f;
         }
-        __syncthreads();
+        __syncthreads();  // Pq, ob, wa and dred are rewritten by the next record
     }
 }
 
@@ -273,19 +319,21 @@ cudaError_t launch_sketch_permute(const PanelView& p, const int32_t* perm, uint6
 }
 
 cudaError_t launch_sketch_seg(const uint32_t* pp, uint64_t pp_pitch_words, const uint64_t* rec_rows, int64_t m,
-                              uint64_t n_used, const int32_t* seg_off, const int32_t* word_seg, uint32_t d,
-                              RecStats st, int want_moments, int split, float* out, uint64_t ld,
-                              cudaStream_t stream) {
+                              uint64_t n_used, const int32_t* seg_off, uint32_t d, RecStats st, int want_moments,
+                              int split, float* out, uint64_t ld, cudaStream_t stream) {
     if (m <= 0) return cudaSuccess;
-    const size_t smem = sizeof(int32_t) * 2 * (size_t)d;
+    const size_t smem = sketch_smem(n_used, d);
+    if (smem > 200 * 1024) return cudaErrorInvalidValue;  // rejected by the caller first (ldsc_sketch_supported)
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(k_sketch_seg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
-    int64_t grid = m < 148 * 8 ? m : 148 * 8;
-    k_sketch_seg<<<(unsigned)grid, NT, smem, stream>>>(pp, pp_pitch_words, rec_rows, m, n_used, seg_off, word_seg, d,
-                                                       st, want_moments, split, out, ld);
+    int64_t grid = m < 148 * 16 ? m : 148 * 16;
+    k_sketch_seg<<<(unsigned)grid, SNT, smem, stream>>>(pp, pp_pitch_words, rec_rows, m, n_used, seg_off, d, st,
+                                                       want_moments, split, out, ld);
     return cudaGetLastError();
 }
+
+bool sketch_supported(uint64_t n_used, uint32_t d) { return sketch_smem(n_used, d) <= 200 * 1024; }
 
 }  // namespace ldsc
