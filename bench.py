@@ -470,6 +470,7 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=40.0, help="serving: Poisson arrivals per second")
     ap.add_argument("--serve-seconds", type=float, default=30.0, help="serving: length of the arrival window")
     ap.add_argument("--serve-slots", type=int, default=6, help="serving: concurrent job slots")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving summary of the default run")
     ap.add_argument("--sketch-d", default="200,1000,5000")
     ap.add_argument("--sketch-snps", type=int, default=0, help="truncate the sketch panel (profiling)")
     args = ap.parse_args()
@@ -612,8 +613,8 @@ def main():
     ops = 8.0 * spec.n_indiv * npairs   # 4 integer products x 2 ops x N per in-band pair
     achieved = ops / gram_avg / 1e12
     roofline = {"bound": "tensor", "achieved": achieved, "peak": int8_peak, "unit": "TFLOP/s",
-                "frac": achieved / int8_peak, "traffic": committed_traffic("k_gram_i8"),
-                "kernel": "k_gram_i8 (tcgen05.mma kind::i8)",
+                "frac": achieved / int8_peak, "traffic": committed_traffic("k_gram_tc"),
+                "kernel": "k_gram_tc<4,0> (tcgen05.mma kind::i8)",
                 "note": f"int8 ops counted like flops (2 per MAC, 4 products per pair); peak = 2 x {src} "
                         "bf16 dense burst (MEASURED_PEAKS.json), nominal int8 dense 4500"}
 
@@ -624,13 +625,25 @@ def main():
         cpu = {"value": v, "unit": "r2 pairs/s", "cores": cores, "kind": "port",
                "sample": f"first {CPU_SAMPLE_SNPS} SNPs of the panel ({pairs_s} pairs, {dt:.1f} s), same flags, f64"}
 
+    # ---- serving latency at a stated rate (the metric's second half), 1 GPU ----
+    serving = None
+    if world == 1 and args.serve_seconds > 0 and not args.no_serving:
+        try:
+            sv = run_serving_workload(args, ctx, min(args.serve_seconds, 10.0), args.serve_rate)
+            serving = {k: sv[k] for k in ("rate_req_s", "duration_s", "requests", "completed", "failed",
+                                          "throughput_req_s", "l2_pairs_per_s", "latency_ms", "queue_ms",
+                                          "by_kind_latency_ms", "slots", "graph_launches")}
+            serving["config"] = sv["config"]
+        except Exception as e:  # noqa: BLE001 -- reported in the line, the headline numbers stand
+            serving = {"error": str(e)[:300]}
+
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": "r2 pairs/s", "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": "int8 (int32 accumulate, f64 epilogue)",
                "data": "synthetic (seeded founder-mosaic panel generated on the device)",
                "config": config_dict(spec), "e2e": e2e, "gpu_launches": int(launches),
-               "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
+               "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks, "serving": serving,
                "forms": {"int8_pairs_per_s": value / world, "fp64_pairs_per_s": fp64_value,
                          "int8_over_fp64": (value / world) / fp64_value if fp64_value else None,
                          "int8_gram_ms": 1e3 * gram_avg, "fp64_gram_ms": 1e3 * float(np.mean(fp64_gram)),
