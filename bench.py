@@ -561,9 +561,12 @@ def main():
     gram_avg = float(np.mean(gram_s))
 
     # ---- FP64 plain form, same panel ----
-    fp64_value, fp64_gram = None, [float("nan")]
+    fp64_value, fp64_gram, int8_err = None, [float("nan")], None
     if args.fp64_steps > 0:
-        step("fp64")
+        l2_64 = step("fp64")[0]
+        l2_i8 = step("int8")[0]
+        # l2 of the INT8 form against the FP64 form on the same panel: max |a - b| / max(|b|, 1)
+        int8_err = float(np.max(np.abs(l2_i8 - l2_64) / np.maximum(np.abs(l2_64), 1.0)))
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -649,7 +652,8 @@ def main():
                          "int8_gram_ms": 1e3 * gram_avg, "fp64_gram_ms": 1e3 * float(np.mean(fp64_gram)),
                          "int8_decode_ms": 1e3 * float(np.mean(dec_s)),
                          "int8_device_ms_per_pass": float(np.mean(dev_ms)),
-                         "n_pairs_per_rank": npairs}}
+                         "n_pairs_per_rank": npairs,
+                         "int8_vs_fp64_l2_max_rel_err": int8_err}}
         print(json.dumps(out))
     panel.close()
     ctx.close()
