@@ -87,6 +87,7 @@ typedef struct {
     uint32_t kernel_launches;   /* kernels launched by this call */
     uint32_t gram_kind;         /* 0 fp64, 1 int8 tcgen05, 2 fp32 sketch */
     double device_ms;           /* whole call, device time */
+    double contract_secs;       /* K > 1: the annotation contraction passes (inside ab_dot_secs) */
 } ldsc_perf;
 
 /* Arguments of one l2 computation.  Record i of the call is BED row
@@ -120,6 +121,7 @@ typedef struct {
     uint64_t row_begin;           /* with bed_idx NULL: record i is row row_begin + i */
     int32_t annot_on_device;      /* annot points to device memory (read in place) */
     uint64_t annot_ld;            /* rows between annot columns; 0 = n_snp */
+    int32_t out_on_device;        /* l2_out / maf_out are device pointers */
 } ldsc_l2_args;
 
 /* Synthetic panel description (seeded founder mosaic; see ldsc_b200/synth.py). */

@@ -48,7 +48,7 @@ class Perf(C.Structure):
                 ("bb_dot_secs", C.c_double), ("ab_dot_secs", C.c_double),
                 ("ring_store_secs", C.c_double), ("n_pairs", C.c_uint64),
                 ("n_tiles", C.c_uint64), ("kernel_launches", C.c_uint32),
-                ("gram_kind", C.c_uint32), ("device_ms", C.c_double)]
+                ("gram_kind", C.c_uint32), ("device_ms", C.c_double), ("contract_secs", C.c_double)]
 
 
 class L2Args(C.Structure):
@@ -62,6 +62,7 @@ class L2Args(C.Structure):
         ("has_pq_exp", C.c_int32), ("pq_exp", C.c_double), ("yes_really", C.c_int32),
         ("on_progress", PROGRESS_FN), ("progress_user", C.c_void_p),
         ("row_begin", C.c_uint64), ("annot_on_device", C.c_int32), ("annot_ld", C.c_uint64),
+        ("out_on_device", C.c_int32),
     ]
 
 

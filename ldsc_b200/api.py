@@ -64,6 +64,7 @@ class L2Perf:
     kernel_launches: int
     gram_kind: str
     device_ms: float
+    contract_secs: float = 0.0
 
 
 def _perf(p: L.Perf) -> L2Perf:
@@ -71,7 +72,7 @@ def _perf(p: L.Perf) -> L2Perf:
                   None if p.sketch_secs < 0 else p.sketch_secs, p.bb_dot_secs, p.ab_dot_secs,
                   p.ring_store_secs, int(p.n_pairs), int(p.n_tiles), int(p.kernel_launches),
                   {0: "fp64", 1: "int8", 2: "fp32-sketch"}.get(int(p.gram_kind), "?"),
-                  p.device_ms)
+                  p.device_ms, p.contract_secs)
 
 
 class Context:
@@ -233,7 +234,17 @@ class _ArgPack:
 PROGRESS_NONE = L.PROGRESS_FN()
 
 
-def _run(ctx: Context, panel: Panel, pack: _ArgPack, m: int):
+def _run(ctx: Context, panel: Panel, pack: _ArgPack, m: int, out_device=None):
+    if out_device is not None:
+        # (l2, maf) CUDA tensors: l2 of shape (K, m) row-major = m x K column-major; maf (m,)
+        l2, maf = out_device
+        if tuple(l2.shape) != (pack.K, m) or tuple(maf.shape) != (m,) or not l2.is_contiguous():
+            raise LdscError(L.LDSC_E_INVALID, "out_device wants contiguous (K, m) and (m,) float64 tensors")
+        pack.args.out_on_device = 1
+        perf = L.Perf()
+        ctx.check(ctx.lib.ldsc_l2_run(ctx.h, panel.h, C.byref(pack.args), l2.data_ptr(), maf.data_ptr(),
+                                      C.byref(perf)))
+        return l2, maf, _perf(perf)
     l2 = np.zeros((m, pack.K), dtype=np.float64, order="F")
     maf = np.zeros(m, dtype=np.float64)
     perf = L.Perf()
@@ -264,13 +275,15 @@ def compute_ldscore_global(ctx: Context, all_snps: BimTable, panel: Panel, n_ind
 def run_l2(ctx: Context, all_snps: BimTable, panel: Panel, mode: WindowMode, chunk_c: int = 200,
            annot=None, iid_indices=None, pq_exp=None, yes_really=False, use_f32=False,
            sketch=None, sketch_maf_aware=False, snp_level_masking=False, global_pass=False,
-           precision="fp64", on_progress=None):
+           precision="fp64", on_progress=None, annot_device=None, out_device=None):
     """The compute part of ``l2::run``: per-chromosome chunking (default) or
-    one global pass (src/l2/mod.rs:439-575)."""
+    one global pass (src/l2/mod.rs:439-575).  ``annot_device`` = (device
+    pointer, leading dimension, K) of resident annotations; ``out_device`` =
+    (l2, maf) CUDA tensors that receive the results in place of host arrays."""
     pack = _ArgPack(all_snps, mode, chunk_c, annot, iid_indices, pq_exp, yes_really, use_f32,
                     sketch, sketch_maf_aware, snp_level_masking, precision, global_pass,
-                    on_progress)
-    return _run(ctx, panel, pack, len(all_snps))
+                    on_progress, annot_device=annot_device)
+    return _run(ctx, panel, pack, len(all_snps), out_device)
 
 
 def l2_from_bed_bytes(ctx: Context, bed_file: np.ndarray, n_indiv: int, snps: BimTable,

@@ -937,6 +937,7 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
     }
     // ---- band Gram + epilogue ----
     const int e2 = ev.mark();
+    int e_c = -1;
     if (!tiles.empty() && !stream_gram) {
         if (d) {
             CK(launch_gram_tf32(ctx->xsk.as<float>(), ld_sk, m, ctx->tiles.as<Tile>(), (int64_t)tiles.size(), ep,
@@ -949,6 +950,7 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
                                ep, ctx->sms, s));
         }
         ctx->kernels++;
+        e_c = ev.mark();
         if (K > 1) {
             CK(launch_contract(ctx->rtiles.as<float>(), ta, tb, ctx->tiles.as<Tile>(), ctx->cptr_r.as<int32_t>(),
                                ctx->cidx_r.as<int32_t>(), n_right, true, ep, s));
@@ -958,8 +960,9 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
         }
     }
     const int e3 = ev.mark();
-    CK(cudaMemcpyAsync(l2_out, ctx->l2.p, 8 * nmom * K, cudaMemcpyDeviceToHost, s));
-    if (maf_out) CK(cudaMemcpyAsync(maf_out, ctx->maf.p, 8 * nmom, cudaMemcpyDeviceToHost, s));
+    const cudaMemcpyKind okind = a->out_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    CK(cudaMemcpyAsync(l2_out, ctx->l2.p, 8 * nmom * K, okind, s));
+    if (maf_out) CK(cudaMemcpyAsync(maf_out, ctx->maf.p, 8 * nmom, okind, s));
     unsigned int herr[4] = {0, 0, 0, 0};
     CK(cudaMemcpyAsync(herr, ctx->err.p, 16, cudaMemcpyDeviceToHost, s));
     const int e4 = ev.mark();
@@ -970,6 +973,7 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
     pf.norm_secs = ev.ms(d ? e_sk : e0, e1) / 1e3;
     if (d) pf.sketch_secs = ev.ms(e0, e_sk) / 1e3;
     pf.ab_dot_secs = ev.ms(e2, e3) / 1e3;
+    if (e_c >= 0 && K > 1) pf.contract_secs = ev.ms(e_c, e3) / 1e3;
     pf.device_ms = ev.ms(e0, e4);
     pf.kernel_launches = (uint32_t)(ctx->kernels - kernels0);
     if (perf) *perf = pf;
