@@ -200,6 +200,13 @@ int ldsc_l2_run(ldsc_ctx *ctx, const ldsc_panel *panel, const ldsc_l2_args *args
 int ldsc_l2_from_bed(ldsc_ctx *ctx, const uint8_t *bed_file, uint64_t len, uint64_t n_indiv,
                      const ldsc_l2_args *args, double *l2_out, double *maf_out, ldsc_perf *perf);
 
+/* compute_snp_stats (src/l2/snp_stats.rs:5-195), the --maf / --pq-exp
+ * prefilter: per record of `args` (n_snp, bed_idx or row_begin, keep_iids),
+ * MAF = min(f, 1 - f) with f = sum / (2 count), and het_miss_ok = 1 when
+ * het + missing < n (0 for an all-het-or-missing SNP).  One decode pass. */
+int ldsc_snp_stats(ldsc_ctx *ctx, const ldsc_panel *panel, const ldsc_l2_args *args, double *maf_out,
+                   uint8_t *het_miss_ok_out);
+
 /* Number of off-diagonal pairs the call would accumulate (host only). */
 int ldsc_l2_pair_count(const ldsc_l2_args *args, uint64_t *n_pairs);
 

@@ -137,6 +137,7 @@ SIGNATURES = {
     "ldsc_l2_from_bed": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64,
                                    C.POINTER(L2Args), C.c_void_p, C.c_void_p, C.POINTER(Perf)]),
     "ldsc_l2_pair_count": (C.c_int, [C.POINTER(L2Args), C.POINTER(C.c_uint64)]),
+    "ldsc_snp_stats": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(L2Args), C.c_void_p, C.c_void_p]),
     "ldsc_l2_left_limits": (C.c_int, [C.POINTER(L2Args), C.c_void_p]),
     "ldsc_countsketch_hash": (C.c_int, [C.c_uint64, C.c_uint32, C.c_uint64, C.c_void_p,
                                         C.c_void_p]),

@@ -486,3 +486,15 @@ def rg_batch(ctx: Context, z1, z2, n1, n2, ref_l2, w_l2, m_snps: float,
     names = [f for f, _ in L.RgResult._fields_]
     return np.array([tuple(getattr(r, f) for f in names) for r in out],
                     dtype=[(f, np.float64) for f in names])
+
+
+def snp_stats(ctx: Context, snps: BimTable, panel: Panel, iid_indices=None):
+    """compute_snp_stats (src/l2/snp_stats.rs:5-195): (MAF, het_miss_ok) per
+    record, the --maf / --pq-exp prefilter."""
+    pack = _ArgPack(snps, WindowMode.Cm(1.0), 200, None, iid_indices, None, True, False, None, False,
+                    False, "fp64", False, None)
+    m = len(snps)
+    maf = np.zeros(m, dtype=np.float64)
+    ok = np.zeros(m, dtype=np.uint8)
+    ctx.check(ctx.lib.ldsc_snp_stats(ctx.h, panel.h, C.byref(pack.args), maf.ctypes.data, ok.ctypes.data))
+    return maf, ok.astype(bool)

@@ -994,6 +994,73 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
 
 extern "C" {
 
+int ldsc_snp_stats(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double* maf_out,
+                   uint8_t* het_miss_ok_out) {
+    if (!ctx || !panel || !a) return LDSC_E_INVALID;
+    const int64_t m = (int64_t)a->n_snp;
+    if (m > 0 && (!maf_out || !het_miss_ok_out)) return LDSC_E_INVALID;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    const uint64_t n_file = panel->n_indiv;
+    const uint64_t n_used = a->keep_iids ? a->n_keep : n_file;
+    if (a->keep_iids) {
+        if (a->n_keep == 0) return fail(ctx, LDSC_E_INVALID, "--keep: no individuals retained");
+        for (uint64_t i = 0; i < a->n_keep; i++)
+            if (a->keep_iids[i] < 0 || (uint64_t)a->keep_iids[i] >= n_file)
+                return fail(ctx, LDSC_E_INVALID, "index " + std::to_string(a->keep_iids[i]) +
+                                                     " out of range (max " + std::to_string(n_file) + ")");
+    }
+    if (a->bed_idx) {
+        for (int64_t i = 0; i < m; i++)
+            if (a->bed_idx[i] >= panel->n_snp)
+                return fail(ctx, LDSC_E_INVALID, "SNP index " + std::to_string(a->bed_idx[i]) +
+                                                     " out of range (max " + std::to_string(panel->n_snp) + ")");
+    } else if (a->row_begin > panel->n_snp || (uint64_t)m > panel->n_snp - a->row_begin) {
+        return fail(ctx, LDSC_E_INVALID, "more SNP records than panel rows");
+    }
+    if (m == 0) return LDSC_OK;
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->stream;
+    CK(ctx->st_n.ensure(4 * (size_t)m));
+    CK(ctx->st_s.ensure(4 * (size_t)m));
+    CK(ctx->st_q.ensure(4 * (size_t)m));
+    if (a->bed_idx) {
+        CK(ctx->recrows.ensure(8 * (size_t)m));
+        CK(cudaMemcpyAsync(ctx->recrows.p, a->bed_idx, 8 * (size_t)m, cudaMemcpyHostToDevice, s));
+    }
+    if (a->keep_iids) {
+        CK(ctx->keep.ensure(8 * a->n_keep));
+        CK(cudaMemcpyAsync(ctx->keep.p, a->keep_iids, 8 * a->n_keep, cudaMemcpyHostToDevice, s));
+    }
+    PanelView pv{panel->rows, panel->n_snp, panel->n_indiv, panel->bpr, panel->pitch};
+    if (!a->bed_idx) {
+        pv.rows += a->row_begin * panel->pitch;
+        pv.n_snp -= a->row_begin;
+    }
+    IndivSel sel{a->keep_iids ? ctx->keep.as<int64_t>() : nullptr, n_used};
+    RecStats st{};
+    st.n = ctx->st_n.as<int32_t>();
+    st.s = ctx->st_s.as<int32_t>();
+    st.q = ctx->st_q.as<int32_t>();
+    CK(launch_decode_i8(pv, a->bed_idx ? ctx->recrows.as<uint64_t>() : nullptr, m, sel, nullptr, 0, st, 0, s));
+    ctx->kernels++;
+    std::vector<int32_t> hn((size_t)m), hs((size_t)m), hq((size_t)m);
+    CK(cudaMemcpyAsync(hn.data(), st.n, 4 * (size_t)m, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(hs.data(), st.s, 4 * (size_t)m, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(hq.data(), st.q, 4 * (size_t)m, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    // compute_snp_stats (src/l2/snp_stats.rs:150-163): freq = sum / (2 count),
+    // MAF = min(freq, 1 - freq); keep when het + missing < n.  With s = #1 + 2 #2
+    // and q = #1 + 4 #2, het = #1 = 2 s - q.
+    for (int64_t i = 0; i < m; i++) {
+        const int64_t n = hn[i], sm = hs[i], q = hq[i];
+        const double freq = n > 0 ? (double)sm / (2.0 * (double)n) : 0.0;
+        maf_out[i] = freq < 1.0 - freq ? freq : 1.0 - freq;
+        const int64_t het = 2 * sm - q, missing = (int64_t)n_used - n;
+        het_miss_ok_out[i] = (uint8_t)(het + missing < (int64_t)n_used);
+    }
+    return LDSC_OK;
+}
+
 int ldsc_l2_run(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* args, double* l2_out,
                 double* maf_out, ldsc_perf* perf) {
     if (!ctx || !panel || !args) return LDSC_E_INVALID;

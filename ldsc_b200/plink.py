@@ -133,7 +133,7 @@ def write_plink(prefix: str, body: np.ndarray, chr_: np.ndarray, cm: np.ndarray,
     ids = snp_ids or [f"rs{j + 1}" for j in range(m)]
     with open(prefix + ".bim", "w") as f:
         for j in range(m):
-            f.write(f"{int(chr_[j])}\t{ids[j]}\t{cm[j]!r}\t{int(bp[j])}\tA\tG\n")
+            f.write(f"{int(chr_[j])}\t{ids[j]}\t{float(cm[j])!r}\t{int(bp[j])}\tA\tG\n")
     with open(prefix + ".fam", "w") as f:
         for i in range(n_indiv):
             f.write(f"F{i + 1}\tI{i + 1}\t0\t0\t1\t-9\n")

@@ -12,4 +12,5 @@ from .oracle import (  # noqa: F401
     wyrand_stream,
     scatter_column_f32,
     max_threads,
+    oracle_snp_stats,
 )

@@ -185,3 +185,23 @@ def scatter_column_f32(row: np.ndarray, n_indiv: int, bucket, sign, mean: float,
 
 def max_threads() -> int:
     return int(_load().oracle_max_threads())
+
+
+def oracle_snp_stats(bed_body: np.ndarray, n_file_indiv: int, bed_idx: np.ndarray,
+                     iid_idx: Optional[np.ndarray] = None):
+    """compute_snp_stats (src/l2/snp_stats.rs:5-195): per record, MAF from
+    sum / (2 count) over the kept individuals, and het + missing < n.
+    Codes: 00 -> 2, 01 -> missing, 10 -> 1 (het), 11 -> 0."""
+    bpr = (n_file_indiv + 3) // 4
+    rows = np.asarray(bed_body, dtype=np.uint8).reshape(-1, bpr)[np.asarray(bed_idx, dtype=np.int64)]
+    codes = np.stack([(rows >> (2 * k)) & 3 for k in range(4)], axis=-1).reshape(len(rows), -1)[:, :n_file_indiv]
+    if iid_idx is not None:
+        codes = codes[:, np.asarray(iid_idx, dtype=np.int64)]
+    n = codes.shape[1]
+    count = (codes != 1).sum(axis=1)
+    s = 2 * (codes == 0).sum(axis=1) + (codes == 2).sum(axis=1)
+    het = (codes == 2).sum(axis=1)
+    freq = np.where(count > 0, s / np.maximum(2.0 * count, 1), 0.0)
+    maf = np.minimum(freq, 1.0 - freq)
+    ok = het + (n - count) < n
+    return maf, ok
