@@ -259,6 +259,8 @@ typedef struct {
     double intercept;
     int32_t want_lambda_gc;       /* median(chi2) / 0.4549 (exact order statistics) */
     int32_t device_pointers;      /* 1: the arrays above are device pointers */
+    int32_t two_step;             /* --two-step: fit the intercept on chi2 < two_step_cutoff first */
+    double two_step_cutoff;
 } ldsc_h2_args;
 
 typedef struct {

@@ -76,7 +76,8 @@ class H2Args(C.Structure):
                 ("chi2", C.c_void_p), ("n_per_snp", C.c_void_p), ("n_scalar", C.c_void_p),
                 ("ref_l2", C.c_void_p), ("w_l2", C.c_void_p), ("m_snps", C.c_double),
                 ("fixed_intercept", C.c_int32), ("intercept", C.c_double),
-                ("want_lambda_gc", C.c_int32), ("device_pointers", C.c_int32)]
+                ("want_lambda_gc", C.c_int32), ("device_pointers", C.c_int32), ("two_step", C.c_int32),
+                ("two_step_cutoff", C.c_double)]
 
 
 class H2Result(C.Structure):

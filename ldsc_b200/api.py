@@ -449,7 +449,8 @@ def _f64(a):
 
 
 def h2_batch(ctx: Context, chi2, n, ref_l2, w_l2, m_snps: float, n_blocks: int = 200,
-             intercept: Optional[float] = None, lambda_gc: bool = True) -> np.ndarray:
+             intercept: Optional[float] = None, lambda_gc: bool = True,
+             two_step: Optional[float] = None) -> np.ndarray:
     """run_h2_ldsc for many traits (K = 1, no --two-step).  chi2: T x n_snp;
     n: T scalars or T x n_snp.  Returns a structured array with the fields of
     ldsc_h2_result."""
@@ -463,7 +464,8 @@ def h2_batch(ctx: Context, chi2, n, ref_l2, w_l2, m_snps: float, n_blocks: int =
                     n_scalar=None if per_snp else n.ctypes.data,
                     ref_l2=ref_l2.ctypes.data, w_l2=w_l2.ctypes.data, m_snps=float(m_snps),
                     fixed_intercept=int(intercept is not None), intercept=float(intercept or 0.0),
-                    want_lambda_gc=int(lambda_gc), device_pointers=0)
+                    want_lambda_gc=int(lambda_gc), device_pointers=0, two_step=int(two_step is not None),
+                    two_step_cutoff=float(two_step or 0.0))
     out = (L.H2Result * T)()
     ctx.check(ctx.lib.ldsc_h2_batch(ctx.h, C.byref(args), C.cast(out, C.c_void_p)))
     names = [f for f, _ in L.H2Result._fields_]

@@ -126,6 +126,7 @@ struct ldsc_ctx {
     uint64_t graph_launches = 0;  // replays of cached graphs
     DevBuf rtiles, cptr_r, cidx_r, cptr_l, cidx_l;  // K > 1 contraction: r2u tiles and CSR tile lists
     DevBuf rg_jobs, rg_states, rg_outs, rg_part, rg_tdel, rg_y, rg_y2, rg_n, rg_ld, rg_wld, rg_sel, rg_pairs, rg_res;
+    DevBuf ts_seps, ts_n1, ts_cnt, ts_dv, ts_outs;  // --two-step
     // whole-file entry: staged file rows, the pitched panel, per-chunk events
     DevBuf bed_stage, bed_rows;
     std::vector<cudaEvent_t> feed_ev;
@@ -140,7 +141,7 @@ struct ldsc_ctx {
                       &rtiles, &cptr_r, &cidx_r, &cptr_l, &cidx_l,
                       &rg_jobs, &rg_states, &rg_outs, &rg_part, &rg_tdel,
                       &rg_y, &rg_y2, &rg_n, &rg_ld, &rg_wld, &rg_sel,
-                      &rg_pairs, &rg_res, &bed_stage, &bed_rows};
+                      &rg_pairs, &rg_res, &bed_stage, &bed_rows, &ts_seps, &ts_n1, &ts_cnt, &ts_dv, &ts_outs};
     }
 };
 
@@ -1319,6 +1320,9 @@ extern "C" int ldsc_h2_batch(ldsc_ctx* ctx, const ldsc_h2_args* a, ldsc_h2_resul
     const int nb = (int)std::min<uint64_t>(a->n_blocks, n);
     if (nb < 2) return fail(ctx, LDSC_E_INVALID, "n_blocks must be >= 2");
     if (!(a->m_snps > 0)) return fail(ctx, LDSC_E_INVALID, "M must be > 0");
+    const bool two = a->two_step != 0;
+    if (two && a->fixed_intercept)
+        return fail(ctx, LDSC_E_INVALID, "twostep is not compatible with constrained intercept");
     CK(cudaSetDevice(ctx->device));
     cudaStream_t s = ctx->stream;
     const double *d_ld, *d_wld;
@@ -1341,6 +1345,7 @@ extern "C" int ldsc_h2_batch(ldsc_ctx* ctx, const ldsc_h2_args* a, ldsc_h2_resul
         jb.fixed = a->fixed_intercept;
         jb.fixed_int = a->intercept;
         jb.hsq1 = jb.hsq2 = -1;
+        jb.int_from = -1;
     }
     if (a->device_pointers && !d_n) {
         // scalar sample sizes live on the device: fetch them (T doubles)
@@ -1349,33 +1354,83 @@ extern "C" int ldsc_h2_batch(ldsc_ctx* ctx, const ldsc_h2_args* a, ldsc_h2_resul
         CK(cudaStreamSynchronize(s));
         for (int t = 0; t < T; t++) jobs[t].n1s = ns[t];
     }
-    CK(ctx->rg_jobs.ensure(sizeof(RegJob) * T));
-    CK(ctx->rg_states.ensure(sizeof(RegState) * T));
+    // --two-step (src/h2.rs:319-393): jobs [0, T) fit both parameters on the
+    // SNPs with chi2 below the cutoff, jobs [T, 2T) refit the slope on all SNPs
+    // with that intercept held, over the same jackknife blocks
+    const int J = two ? 2 * T : T;
+    const int nch = (int)((n + 4095) / 4096);
+    if (two) {
+        CK(ctx->ts_seps.ensure(sizeof(int32_t) * (size_t)T * (nb + 1)));
+        CK(ctx->ts_n1.ensure(sizeof(int32_t) * (size_t)T));
+        CK(ctx->ts_cnt.ensure(sizeof(int32_t) * (size_t)T * nch));
+        CK(ctx->ts_dv.ensure(sizeof(double) * 2 * (size_t)J * nb));
+        CK(ctx->ts_outs.ensure(sizeof(RegOut) * (size_t)J));
+        jobs.resize(J);
+        for (int t = 0; t < T; t++) {
+            RegJob& s1 = jobs[t];
+            s1.seps = ctx->ts_seps.as<int32_t>() + (size_t)t * (nb + 1);
+            s1.use_mask = 1;
+            s1.mask_max = a->two_step_cutoff;
+            s1.ld_from_x = 1;
+            RegJob& s2 = jobs[T + t];
+            s2 = jobs[t];
+            s2.use_mask = 0;
+            s2.ld_from_x = 0;
+            s2.fixed = 1;
+            s2.int_from = t;
+        }
+    }
+    CK(ctx->rg_jobs.ensure(sizeof(RegJob) * J));
+    CK(ctx->rg_states.ensure(sizeof(RegState) * J));
     CK(ctx->rg_outs.ensure(sizeof(RegOut) * T));
-    CK(ctx->rg_part.ensure(sizeof(double) * 5 * (size_t)T * nb));
+    CK(ctx->rg_part.ensure(sizeof(double) * 5 * (size_t)J * nb));
     CK(ctx->rg_sel.ensure(sizeof(double) * 2 * T));
-    CK(cudaMemcpyAsync(ctx->rg_jobs.p, jobs.data(), sizeof(RegJob) * T, cudaMemcpyHostToDevice, s));
-    // the whole pipeline (8 regression kernels + the median) replays as one graph
+    CK(cudaMemcpyAsync(ctx->rg_jobs.p, jobs.data(), sizeof(RegJob) * J, cudaMemcpyHostToDevice, s));
+    // the whole pipeline (8 regression kernels + the median; 2 x 8 + 3 for
+    // --two-step) replays as one graph
     const std::vector<uint64_t> gkey{1, (uint64_t)T, n, (uint64_t)nb, dbits(a->m_snps), (uint64_t)a->want_lambda_gc,
                                      (uint64_t)d_ld, (uint64_t)d_wld, (uint64_t)ctx->rg_jobs.p,
                                      (uint64_t)ctx->rg_states.p, (uint64_t)ctx->rg_outs.p, (uint64_t)ctx->rg_part.p,
-                                     (uint64_t)ctx->rg_sel.p};
+                                     (uint64_t)ctx->rg_sel.p, (uint64_t)two, (uint64_t)ctx->ts_seps.p,
+                                     (uint64_t)ctx->ts_dv.p, (uint64_t)ctx->ts_outs.p};
     CK(graph_launch(ctx, gkey, s, [&](cudaStream_t gs) -> cudaError_t {
-        cudaError_t e2 = launch_regressions(ctx->rg_jobs.as<RegJob>(), ctx->rg_states.as<RegState>(),
-                                            ctx->rg_outs.as<RegOut>(), nullptr, ctx->rg_part.as<double>(), nullptr,
-                                            d_ld, d_wld, n, nb, a->m_snps, T, gs);
+        RegJob* dj = ctx->rg_jobs.as<RegJob>();
+        RegState* dst = ctx->rg_states.as<RegState>();
+        cudaError_t e2;
+        if (!two) {
+            e2 = launch_regressions(dj, dst, ctx->rg_outs.as<RegOut>(), nullptr, ctx->rg_part.as<double>(), nullptr,
+                                    d_ld, d_wld, n, nb, a->m_snps, T, gs);
+        } else {
+            RegOut* o12 = ctx->ts_outs.as<RegOut>();
+            double* dv = ctx->ts_dv.as<double>();
+            e2 = launch_twostep_seps(dj, n, nb, ctx->ts_seps.as<int32_t>(), ctx->ts_n1.as<int32_t>(),
+                                     ctx->ts_cnt.as<int32_t>(), T, gs);
+            if (e2 == cudaSuccess)
+                e2 = launch_regressions(dj, dst, o12, nullptr, ctx->rg_part.as<double>(), nullptr, d_ld, d_wld, n,
+                                        nb, a->m_snps, T, gs, dv);
+            if (e2 == cudaSuccess)
+                e2 = launch_regressions(dj + T, dst + T, o12 + T, o12, ctx->rg_part.as<double>() + (size_t)5 * T * nb,
+                                        nullptr, d_ld, d_wld, n, nb, a->m_snps, T, gs, dv + (size_t)2 * T * nb);
+            if (e2 == cudaSuccess)
+                e2 = launch_twostep_combine(o12, o12 + T, dst + T, dv, dv + (size_t)2 * T * nb, nb, a->m_snps,
+                                            ctx->rg_outs.as<RegOut>(), T, gs);
+        }
         if (e2 != cudaSuccess || !a->want_lambda_gc) return e2;
         // median (src/h2.rs:394-414): middle order statistic, mean of the two for even n
         e2 = launch_select(ctx->rg_jobs.as<RegJob>(), n, n / 2, ctx->rg_sel.as<double>(), T, gs);
         if (e2 != cudaSuccess || n % 2) return e2;
         return launch_select(ctx->rg_jobs.as<RegJob>(), n, n / 2 - 1, ctx->rg_sel.as<double>() + T, T, gs);
     }));
-    ctx->kernels += 8 + (a->want_lambda_gc ? (n % 2 == 0 ? 2 : 1) : 0);
+    ctx->kernels += (two ? 19 : 8) + (a->want_lambda_gc ? (n % 2 == 0 ? 2 : 1) : 0);
     std::vector<RegOut> outs(T);
     std::vector<double> sel(2 * T, NAN);
+    std::vector<int32_t> n1(two ? T : 0);
     CK(cudaMemcpyAsync(outs.data(), ctx->rg_outs.p, sizeof(RegOut) * T, cudaMemcpyDeviceToHost, s));
     if (a->want_lambda_gc) CK(cudaMemcpyAsync(sel.data(), ctx->rg_sel.p, 8 * 2 * (size_t)T, cudaMemcpyDeviceToHost, s));
+    if (two) CK(cudaMemcpyAsync(n1.data(), ctx->ts_n1.p, 4 * (size_t)T, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    for (int t = 0; t < (two ? T : 0); t++)  // jackknife_fast on the step-1 SNPs (src/h2.rs:121-123)
+        if (n1[t] < nb) return fail(ctx, LDSC_E_INVALID, "More blocks than data points.");
     for (int t = 0; t < T; t++) {
         const RegOut& o = outs[t];
         ldsc_h2_result& r = res[t];
@@ -1442,6 +1497,7 @@ extern "C" int ldsc_rg_batch(ldsc_ctx* ctx, const ldsc_rg_args* a, ldsc_rg_resul
             RegJob& jb = jobs[q == 2 ? 2 * P + p : 2 * p + q];
             std::memset(&jb, 0, sizeof(jb));
             jb.hsq1 = jb.hsq2 = -1;
+            jb.int_from = -1;
         }
         RegJob& h1 = jobs[2 * p];
         h1.ya = d_z1 + (size_t)p * n;

@@ -21,6 +21,12 @@ struct RegJob {
     int32_t fixed;      // intercept constrained
     double fixed_int;
     int32_t hsq1, hsq2; // REG_GENCOV: job indices of the two h2 fits
+    // --two-step (src/h2.rs:319-393)
+    const int32_t* seps;  // nb + 1 block starts in SNP index space, or null: floor(b n / nb)
+    int32_t use_mask;     // least-squares sums over SNPs with y < mask_max only (step 1)
+    double mask_max;
+    int32_t ld_from_x;    // re-weighting uses the regressor x0 in place of the LD score (step 1)
+    int32_t int_from;     // fixed intercept = est[1] of ref_outs[int_from] (step 2), or -1
 };
 
 // Running parameters of a job between passes.
@@ -29,6 +35,9 @@ struct RegState {
     double slope;       // hsq (REG_HSQ) or rho_g (REG_GENCOV) used by the weights
     double intercept;
     double h1, h2, int_h1, int_h2;  // REG_GENCOV weight constants
+    double fixed_int;               // intercept of the least squares when jb.fixed
+    double c_num, c_den;            // sum w0 x0, sum w0 x0^2 under the initial weights
+    int32_t n_updates;
 };
 
 struct RegOut {
@@ -52,10 +61,25 @@ struct RgOut {
 // Aggregate pass, two IRWLS updates and the block jackknife for all jobs.
 // outs[j] receives job j's result; ref_outs holds the h2 results that
 // REG_GENCOV jobs refer to by index.  part: njobs * nb * 5 doubles of
-// scratch; tot_delete (optional): njobs * nb.
+// scratch; tot_delete (optional): njobs * nb; dv (optional): njobs * nb * 2
+// delete values.
 cudaError_t launch_regressions(const RegJob* jobs, RegState* states, RegOut* outs, const RegOut* ref_outs,
                                double* part, double* tot_delete, const double* ld, const double* wld, uint64_t n,
-                               int nb, double m, int njobs, cudaStream_t s);
+                               int nb, double m, int njobs, cudaStream_t s, double* dv = nullptr);
+
+// --two-step block starts: for each job, mask = y < mask_max, n1 = its size,
+// and seps[b] = index of the kept SNP of rank floor(b n1 / nb) (0 and n at
+// the ends): get_separators on the kept SNPs mapped back by update_separators
+// (src/h2.rs:31-58).  seps: njobs * (nb + 1); n1: njobs; cnt: scratch of
+// njobs * ceil(n / 4096) ints.
+cudaError_t launch_twostep_seps(const RegJob* jobs, uint64_t n, int nb, int32_t* seps, int32_t* n1, int32_t* cnt,
+                                int njobs, cudaStream_t s);
+
+// combine_twostep (src/h2.rs:220-256) + the h2 result: step 1 jobs s1[t],
+// step 2 jobs s2[t] (the fixed-intercept fit on all SNPs), their delete
+// values dv1 / dv2 (nb * 2 per job) -> outs[t].
+cudaError_t launch_twostep_combine(const RegOut* out1, const RegOut* out2, const RegState* st2, const double* dv1,
+                                   const double* dv2, int nb, double m, RegOut* outs, int ntraits, cudaStream_t s);
 
 cudaError_t launch_rg_finish(const RgPairIdx* pairs, const RegOut* outs, const double* tot_delete, int nb,
                              RgOut* res, int npairs, cudaStream_t s);

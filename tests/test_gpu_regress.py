@@ -155,3 +155,32 @@ def test_regression_errors(ctx):
         h2_batch(ctx, np.ones((1, 10)), [1e4], ld, ld, 10.0, 1)
     with pytest.raises(LdscError, match="M must be"):
         h2_batch(ctx, np.ones((1, 10)), [1e4], ld, ld, 0.0, 5)
+
+
+@pytest.mark.parametrize("cutoff", [30.0, 8.0])
+def test_h2_batch_two_step(ctx, cutoff):
+    """--two-step (src/h2.rs:319-393): intercept from chi2 < cutoff, slope
+    refit on all SNPs, combined delete values."""
+    from ldsc_b200.api import h2_batch
+    from ldsc_b200.synth import gwas_traits
+    m = 40_000
+    ld, wld = _ld(m, 15)
+    chi2, n, _ = gwas_traits(ld, 2e5, 4, seed=16)
+    got = h2_batch(ctx, chi2, n, ld, wld, 2e5, 200, two_step=cutoff)
+    for t in range(4):
+        want = R.run_h2(chi2[t], ld, wld, n[t], 2e5, 200, two_step=cutoff)
+        for k in ("h2", "h2_se", "intercept", "intercept_se", "mean_chi2", "ratio", "ratio_se"):
+            assert _close(got[t][k], want[k], atol=1e-12), (t, k, got[t][k], want[k])
+        assert got[t]["lambda_gc"] == want["lambda_gc"]
+
+
+def test_h2_batch_two_step_errors(ctx):
+    from ldsc_b200.api import LdscError, h2_batch
+    m = 1000
+    ld, wld = _ld(m, 17)
+    chi2 = np.full((1, m), 50.0)
+    chi2[0, :100] = 1.0                                  # 100 SNPs below the cutoff, 200 blocks asked
+    with pytest.raises(LdscError, match="More blocks than data points"):
+        h2_batch(ctx, chi2, [1e5], ld, wld, 1e6, 200, two_step=30.0)
+    with pytest.raises(LdscError, match="constrained intercept"):
+        h2_batch(ctx, chi2, [1e5], ld, wld, 1e6, 50, two_step=30.0, intercept=1.0)
