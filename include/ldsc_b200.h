@@ -242,9 +242,9 @@ int ldsc_sketch_project(ldsc_ctx *ctx, const ldsc_panel *panel, uint64_t snp_beg
  * (ldsc_weights, src/h2.rs:185-206), two IRWLS re-weightings (irwls_ldsc,
  * src/h2.rs:435-458) and the block jackknife (jackknife_fast,
  * src/h2.rs:100-183; jackknife_se_cov, src/jackknife.rs:10-59), as in
- * run_h2_ldsc / run_hsq_ldsc (src/h2.rs:258-433, src/regressions.rs:1648-1825)
- * without --two-step.  One regression per trait; all traits share the SNPs,
- * ref_l2 and w_l2. */
+ * run_h2_ldsc / run_hsq_ldsc (src/h2.rs:258-433, src/regressions.rs:1648-1825),
+ * with --two-step when asked.  One regression per trait; all traits share the
+ * SNPs, ref_l2 and w_l2. */
 typedef struct {
     uint64_t n_snp;
     uint32_t n_traits;
@@ -299,6 +299,51 @@ typedef struct {
 } ldsc_rg_result;
 
 int ldsc_rg_batch(ldsc_ctx *ctx, const ldsc_rg_args *args, ldsc_rg_result *results);
+
+/* Partitioned h2 (fit_h2_partitioned, src/regressions.rs:1121-1226; the
+ * K > 1 branch of run_h2, src/regressions.rs:561-630): one weighted least
+ * squares of chi2 on K LD-score columns scaled by N / nbar, plus an intercept
+ * unless constrained, with weights ldsc_weights(sum of the K columns, w_l2,
+ * N, sum(M), aggregate h2) and the block jackknife over min(kept SNPs,
+ * n_blocks) blocks.  SNPs whose chi2 is not below the trait's chisq_max (NaN
+ * included) are dropped first; run_h2's default for K > 1 is
+ * max(0.001 max(N), 80), N over the SNPs with a chi2.
+ * One regression per trait; traits share ref_l2, w_l2 and m_vec.
+ * P = K + 1 with a free intercept, K with a fixed one; P <= 160. */
+typedef struct {
+    uint64_t n_snp;
+    uint32_t n_traits;
+    uint32_t n_annot;             /* K */
+    uint32_t n_blocks;            /* --n-blocks (200) */
+    const double *chi2;           /* n_traits x n_snp, row-major */
+    const double *n_per_snp;      /* n_traits x n_snp sample sizes, or NULL */
+    const double *n_scalar;       /* n_traits sample sizes (when n_per_snp is NULL) */
+    const double *ref_l2;         /* n_snp x K LD scores, column-major, column stride ref_ld */
+    uint64_t ref_ld;              /* 0: n_snp */
+    const double *w_l2;           /* n_snp regression-weight LD scores */
+    const double *m_vec;          /* K per-annotation M (host) */
+    int32_t fixed_intercept;      /* --intercept-h2 (or --no-intercept: 1.0) */
+    double intercept;
+    const double *chisq_max;      /* n_traits cut-offs (host); INFINITY keeps every finite chi2 */
+    int32_t device_pointers;      /* 1: chi2, n_per_snp, n_scalar, ref_l2, w_l2 are device pointers */
+    double *est;                  /* out, host, may be NULL: n_traits x P jackknife estimates
+                                     (coefficient x nbar per annotation, then the intercept) */
+    double *cov;                  /* out, host, may be NULL: n_traits x P x P jackknife covariance */
+    double *delete_values;        /* out, host, may be NULL: n_traits x n_blocks x P (NaN past
+                                     a trait's block count) */
+    double *h2_annot;             /* out, host, may be NULL: n_traits x K, coefficient x M_k */
+} ldsc_h2p_args;
+
+typedef struct {
+    double h2_total, h2_total_se;    /* sum of h2_annot; SE from the coefficients' covariance
+                                        (total_from_jknife, src/regressions.rs:1565-1610) */
+    double intercept, intercept_se;  /* intercept_se NaN when fixed */
+    double n_mean, mean_chi2;        /* over the kept SNPs */
+    uint64_t n_obs;                  /* kept SNPs */
+    uint32_t n_blocks;               /* jackknife blocks used */
+} ldsc_h2p_result;
+
+int ldsc_h2_partitioned(ldsc_ctx *ctx, const ldsc_h2p_args *args, ldsc_h2p_result *results);
 
 /* ---- serving: continuous batching over resident panels ------------------ */
 

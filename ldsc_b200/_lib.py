@@ -85,6 +85,22 @@ class H2Result(C.Structure):
                                           "lambda_gc", "ratio", "ratio_se", "coef", "coef_se")]
 
 
+class H2PArgs(C.Structure):
+    _fields_ = [("n_snp", C.c_uint64), ("n_traits", C.c_uint32), ("n_annot", C.c_uint32),
+                ("n_blocks", C.c_uint32), ("chi2", C.c_void_p), ("n_per_snp", C.c_void_p),
+                ("n_scalar", C.c_void_p), ("ref_l2", C.c_void_p), ("ref_ld", C.c_uint64),
+                ("w_l2", C.c_void_p), ("m_vec", C.c_void_p), ("fixed_intercept", C.c_int32),
+                ("intercept", C.c_double), ("chisq_max", C.c_void_p), ("device_pointers", C.c_int32),
+                ("est", C.c_void_p), ("cov", C.c_void_p), ("delete_values", C.c_void_p),
+                ("h2_annot", C.c_void_p)]
+
+
+class H2PResult(C.Structure):
+    _fields_ = [(f, C.c_double) for f in ("h2_total", "h2_total_se", "intercept", "intercept_se",
+                                          "n_mean", "mean_chi2")] + \
+               [("n_obs", C.c_uint64), ("n_blocks", C.c_uint32)]
+
+
 class RgArgs(C.Structure):
     _fields_ = [("n_snp", C.c_uint64), ("n_pairs", C.c_uint32), ("n_blocks", C.c_uint32),
                 ("z1", C.c_void_p), ("z2", C.c_void_p), ("n1", C.c_void_p), ("n2", C.c_void_p),
@@ -161,6 +177,7 @@ SIGNATURES = {
     "ldsc_server_destroy": (C.c_int, [C.c_void_p]),
     "ldsc_h2_batch": (C.c_int, [C.c_void_p, C.POINTER(H2Args), C.c_void_p]),
     "ldsc_rg_batch": (C.c_int, [C.c_void_p, C.POINTER(RgArgs), C.c_void_p]),
+    "ldsc_h2_partitioned": (C.c_int, [C.c_void_p, C.POINTER(H2PArgs), C.c_void_p]),
 }
 
 NOALLOC_SCRATCH_BYTES = 64 * 1024 * 1024

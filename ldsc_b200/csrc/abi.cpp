@@ -127,6 +127,9 @@ struct ldsc_ctx {
     DevBuf rtiles, cptr_r, cidx_r, cptr_l, cidx_l;  // K > 1 contraction: r2u tiles and CSR tile lists
     DevBuf rg_jobs, rg_states, rg_outs, rg_part, rg_tdel, rg_y, rg_y2, rg_n, rg_ld, rg_wld, rg_sel, rg_pairs, rg_res;
     DevBuf ts_seps, ts_n1, ts_cnt, ts_dv, ts_outs;  // --two-step
+    // partitioned h2
+    DevBuf p_l2, p_w, p_y, p_n, p_m, p_rjobs, p_seps, p_n1, p_cnt, p_jobs, p_st, p_xtot, p_part, p_gram, p_tot,
+        p_sol, p_res;
     // whole-file entry: staged file rows, the pitched panel, per-chunk events
     DevBuf bed_stage, bed_rows;
     std::vector<cudaEvent_t> feed_ev;
@@ -141,7 +144,9 @@ struct ldsc_ctx {
                       &rtiles, &cptr_r, &cidx_r, &cptr_l, &cidx_l,
                       &rg_jobs, &rg_states, &rg_outs, &rg_part, &rg_tdel,
                       &rg_y, &rg_y2, &rg_n, &rg_ld, &rg_wld, &rg_sel,
-                      &rg_pairs, &rg_res, &bed_stage, &bed_rows, &ts_seps, &ts_n1, &ts_cnt, &ts_dv, &ts_outs};
+                      &rg_pairs, &rg_res, &bed_stage, &bed_rows, &ts_seps, &ts_n1, &ts_cnt, &ts_dv, &ts_outs,
+                      &p_l2, &p_w, &p_y, &p_n, &p_m, &p_rjobs, &p_seps, &p_n1, &p_cnt, &p_jobs,
+                      &p_st, &p_xtot, &p_part, &p_gram, &p_tot, &p_sol, &p_res};
     }
 };
 
@@ -1452,6 +1457,181 @@ extern "C" int ldsc_h2_batch(ldsc_ctx* ctx, const ldsc_h2_args* a, ldsc_h2_resul
         } else {
             r.ratio = NAN;
             r.ratio_se = NAN;
+        }
+    }
+    return LDSC_OK;
+}
+
+extern "C" int ldsc_h2_partitioned(ldsc_ctx* ctx, const ldsc_h2p_args* a, ldsc_h2p_result* res) {
+    if (!ctx || !a || !res) return LDSC_E_INVALID;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    const uint64_t n = a->n_snp;
+    const int T = (int)a->n_traits, K = (int)a->n_annot;
+    if (T == 0) return LDSC_OK;
+    if (n == 0 || K == 0 || !a->chi2 || !a->ref_l2 || !a->w_l2 || !a->m_vec || !a->chisq_max ||
+        (!a->n_per_snp && !a->n_scalar))
+        return fail(ctx, LDSC_E_INVALID, "ldsc_h2_partitioned: missing inputs");
+    if (n > (uint64_t)INT32_MAX) return fail(ctx, LDSC_E_INVALID, "ldsc_h2_partitioned: more than 2^31-1 SNPs");
+    const bool fixed = a->fixed_intercept != 0;
+    const int P = part_params(K, fixed), Q = P + 1;
+    if (P > 160)
+        return fail(ctx, LDSC_E_INVALID, "ldsc_h2_partitioned: too many annotations (P = K + 1 must be <= 160)");
+    const uint64_t ld = a->ref_ld ? a->ref_ld : n;
+    if (ld < n) return fail(ctx, LDSC_E_INVALID, "ldsc_h2_partitioned: ref_ld < n_snp");
+    if (a->n_blocks < 2) return fail(ctx, LDSC_E_INVALID, "n_blocks must be >= 2");
+    double m_tot = 0.0;
+    for (int k = 0; k < K; k++) m_tot += a->m_vec[k];
+    if (!(m_tot > 0)) return fail(ctx, LDSC_E_INVALID, "sum of M must be > 0");
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->stream;
+    cudaError_t e;
+    // inputs on the device
+    const double* d_l2 = a->ref_l2;
+    uint64_t d_ld = ld;
+    if (!a->device_pointers) {
+        CK(ctx->p_l2.ensure(8 * n * (uint64_t)K));
+        CK(cudaMemcpy2DAsync(ctx->p_l2.p, 8 * n, a->ref_l2, 8 * ld, 8 * n, (size_t)K, cudaMemcpyHostToDevice, s));
+        d_l2 = ctx->p_l2.as<double>();
+        d_ld = n;
+    }
+    const double* d_w = dev_array(ctx, ctx->p_w, a->w_l2, n, a->device_pointers, &e);
+    CK(e);
+    const double* d_y = dev_array(ctx, ctx->p_y, a->chi2, (size_t)T * n, a->device_pointers, &e);
+    CK(e);
+    const double* d_n = dev_array(ctx, ctx->p_n, a->n_per_snp, (size_t)T * n, a->device_pointers, &e);
+    CK(e);
+    std::vector<double> ns(T, 0.0);
+    if (!d_n) {
+        if (a->device_pointers) {
+            CK(cudaMemcpyAsync(ns.data(), a->n_scalar, 8 * (size_t)T, cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+        } else {
+            for (int t = 0; t < T; t++) ns[t] = a->n_scalar[t];
+        }
+    }
+    CK(ctx->p_m.ensure(8 * (size_t)K));
+    CK(cudaMemcpyAsync(ctx->p_m.p, a->m_vec, 8 * (size_t)K, cudaMemcpyHostToDevice, s));
+    // kept SNPs (chi2 < chisq_max) and the jackknife block starts over them
+    // (get_separators on the filtered SNPs, src/h2.rs:31-41)
+    const int nb = (int)a->n_blocks;
+    const int nch = (int)((n + 4095) / 4096);
+    std::vector<RegJob> rj(T);
+    for (int t = 0; t < T; t++) {
+        std::memset(&rj[t], 0, sizeof(RegJob));
+        rj[t].ya = d_y + (size_t)t * n;
+        rj[t].ymode = REG_Y_DIRECT;
+        rj[t].use_mask = 1;
+        rj[t].mask_max = a->chisq_max[t];
+        rj[t].int_from = -1;
+    }
+    CK(ctx->p_rjobs.ensure(sizeof(RegJob) * T));
+    CK(ctx->p_seps.ensure(sizeof(int32_t) * 2 * (size_t)T * (nb + 1)));
+    CK(ctx->p_n1.ensure(sizeof(int32_t) * T));
+    CK(ctx->p_cnt.ensure(sizeof(int32_t) * (size_t)T * nch));
+    CK(cudaMemcpyAsync(ctx->p_rjobs.p, rj.data(), sizeof(RegJob) * T, cudaMemcpyHostToDevice, s));
+    RegJob* drj = ctx->p_rjobs.as<RegJob>();
+    int32_t* seps = ctx->p_seps.as<int32_t>();
+    CK(launch_twostep_seps(drj, n, nb, seps, ctx->p_n1.as<int32_t>(), ctx->p_cnt.as<int32_t>(), T, s));
+    ctx->kernels += 2;
+    std::vector<int32_t> n1(T);
+    CK(cudaMemcpyAsync(n1.data(), ctx->p_n1.p, 4 * (size_t)T, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    for (int t = 0; t < T; t++)
+        if (n1[t] < 2) return fail(ctx, LDSC_E_INVALID, "fewer than 2 SNPs below the chi2 cut");
+    // traits with at least nb kept SNPs run together; a trait with fewer runs
+    // alone with nb = its SNP count (src/regressions.rs:1151)
+    std::vector<std::vector<int>> groups(1);
+    for (int t = 0; t < T; t++) {
+        if (n1[t] >= nb)
+            groups[0].push_back(t);
+        else
+            groups.push_back({t});
+    }
+    std::vector<PartJob> pj(T);
+    std::vector<int> gnb(groups.size()), gofs(groups.size());
+    size_t res_len = 0;
+    for (size_t gi = 0, o = 0; gi < groups.size(); gi++) {
+        gnb[gi] = gi == 0 ? nb : n1[groups[gi][0]];
+        gofs[gi] = (int)o;
+        for (int t : groups[gi]) {
+            PartJob& jb = pj[o++];
+            jb.chi2 = d_y + (size_t)t * n;
+            jb.nv = d_n ? d_n + (size_t)t * n : nullptr;
+            jb.ns = ns[t];
+            // group 0 uses the block starts above; others get their own below
+            jb.seps = gi == 0 ? seps + (size_t)t * (nb + 1) : nullptr;
+            jb.mask_max = a->chisq_max[t];
+            jb.n_obs = (double)n1[t];
+            jb.fixed = fixed;
+            jb.fixed_int = fixed ? a->intercept : 0.0;
+            res_len += part_result_len(gnb[gi], K, P);
+        }
+    }
+    // block starts of the small traits (fewer than nb + 1 each), after the
+    // T x (nb + 1) of the first pass
+    size_t off = (size_t)T * (nb + 1);
+    for (size_t gi = 1; gi < groups.size(); gi++) {
+        const int t = groups[gi][0];
+        int32_t* sp = seps + off;
+        CK(launch_twostep_seps(drj + t, n, gnb[gi], sp, ctx->p_n1.as<int32_t>() + t, ctx->p_cnt.as<int32_t>(), 1, s));
+        ctx->kernels += 2;
+        pj[gofs[gi]].seps = sp;
+        off += (size_t)gnb[gi] + 1;
+    }
+    size_t max_gj = 0;
+    for (auto& gr : groups) max_gj = std::max(max_gj, gr.size());
+    CK(ctx->p_jobs.ensure(sizeof(PartJob) * T));
+    CK(ctx->p_st.ensure(sizeof(PartState) * T));
+    CK(ctx->p_xtot.ensure(8 * n));
+    CK(ctx->p_part.ensure(8 * 3 * max_gj * (size_t)nb));
+    CK(ctx->p_gram.ensure(8 * max_gj * (size_t)nb * Q * Q));
+    CK(ctx->p_tot.ensure(8 * max_gj * (size_t)Q * Q));
+    CK(ctx->p_sol.ensure(8 * max_gj * (size_t)(nb + 1) * P));
+    CK(ctx->p_res.ensure(8 * res_len));
+    CK(cudaMemcpyAsync(ctx->p_jobs.p, pj.data(), sizeof(PartJob) * T, cudaMemcpyHostToDevice, s));
+    std::vector<double> hres(res_len);
+    size_t ro = 0;
+    for (size_t gi = 0; gi < groups.size(); gi++) {
+        const int nj = (int)groups[gi].size();
+        if (nj == 0) continue;
+        const int gb = gnb[gi];
+        CK(launch_partitioned(ctx->p_jobs.as<PartJob>() + gofs[gi], ctx->p_st.as<PartState>() + gofs[gi], d_l2, d_ld,
+                              K, fixed, d_w, n, gb, m_tot, ctx->p_m.as<double>(), ctx->p_xtot.as<double>(), ro == 0,
+                              ctx->p_part.as<double>(), ctx->p_gram.as<double>(), ctx->p_tot.as<double>(),
+                              ctx->p_sol.as<double>(), ctx->p_res.as<double>() + ro, nj, s));
+        ctx->kernels += ro == 0 ? 7 : 6;
+        ro += (size_t)nj * part_result_len(gb, K, P);
+    }
+    CK(cudaMemcpyAsync(hres.data(), ctx->p_res.p, 8 * res_len, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    ro = 0;
+    for (size_t gi = 0; gi < groups.size(); gi++) {
+        const int gb = gnb[gi];
+        for (int t : groups[gi]) {
+            const double* R = hres.data() + ro;
+            ro += part_result_len(gb, K, P);
+            const double* est = R;
+            const double* cov = est + P;
+            const double* dv = cov + (size_t)P * P;
+            const double* h2a = dv + (size_t)gb * P;
+            const double* sc = h2a + K;
+            if (a->est) std::memcpy(a->est + (size_t)t * P, est, 8 * (size_t)P);
+            if (a->cov) std::memcpy(a->cov + (size_t)t * P * P, cov, 8 * (size_t)P * P);
+            if (a->delete_values) {
+                double* o = a->delete_values + (size_t)t * nb * P;
+                std::memcpy(o, dv, 8 * (size_t)gb * P);
+                for (size_t x = (size_t)gb * P; x < (size_t)nb * P; x++) o[x] = NAN;
+            }
+            if (a->h2_annot) std::memcpy(a->h2_annot + (size_t)t * K, h2a, 8 * (size_t)K);
+            ldsc_h2p_result& r = res[t];
+            r.h2_total = sc[0];
+            r.h2_total_se = sc[1];
+            r.intercept = sc[2];
+            r.intercept_se = sc[3];
+            r.n_mean = sc[4];
+            r.mean_chi2 = sc[5];
+            r.n_obs = (uint64_t)sc[6];
+            r.n_blocks = (uint32_t)gb;
         }
     }
     return LDSC_OK;

@@ -1,0 +1,403 @@
+// partitioned.cu -- partitioned (stratified) h2 on device-resident LD scores:
+// one weighted least squares on K annotation LD-score columns plus an
+// intercept, with the block jackknife.  Restates fit_h2_partitioned
+// (src/regressions.rs:1121-1226): weights from the summed LD score
+// (aggregate, ldsc_weights, src/h2.rs:185-218), the weighted design
+// (weight_xy, src/h2.rs:60-80), jackknife_fast's per-block X'X / X'y and LU
+// solves (src/h2.rs:100-183) and jackknife_se_cov (src/jackknife.rs:10-59).
+//
+// The design is augmented with y as its last column, Z = [x_1..x_K, 1, y],
+// so one symmetric Gram per jackknife block, sum_i w_i z_i z_i', holds X'X,
+// X'y and y'y.  Per-SNP weights enter squared-root-free: the reference scales
+// rows by sqrt(w_i) / sum_j sqrt(w_j), whose square's global factor cancels
+// in every solve.  SNPs dropped by the chi2 cut contribute nothing and the
+// jackknife blocks are the reference's blocks over the kept SNPs (block starts
+// mapped back to SNP indices).  Block partial sums are combined in block
+// order, so results do not depend on scheduling.
+#include <cuda_runtime.h>
+
+#include <cmath>
+
+#include "regress.h"
+
+namespace ldsc {
+
+namespace {
+
+constexpr int NT = 256;
+constexpr int TILE = 64;       // Gram output tile (64 x 64, 4 x 4 per thread)
+constexpr int ROWS = 32;       // SNPs staged per step
+constexpr int SROW = TILE + 2; // staged row stride in doubles (16-byte aligned rows)
+
+__device__ __forceinline__ double part_n(const PartJob& jb, uint64_t i) { return jb.nv ? jb.nv[i] : jb.ns; }
+__device__ __forceinline__ bool part_kept(const PartJob& jb, uint64_t i) { return jb.chi2[i] < jb.mask_max; }
+
+template <typename T>
+__device__ __forceinline__ T block_sum(T v, T* red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    T t = 0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < NT / 32; w++) t += red[w];
+    __syncthreads();
+    return t;
+}
+
+// x_tot[i] = sum_j l2[i, j], columns added in order (src/regressions.rs:1158-1165)
+__global__ void __launch_bounds__(NT) k_p_xtot(const double* __restrict__ l2, uint64_t ld, int k, uint64_t n,
+                                              double* __restrict__ xtot) {
+    for (uint64_t i = (uint64_t)blockIdx.x * NT + threadIdx.x; i < n; i += (uint64_t)gridDim.x * NT) {
+        double s = 0.0;
+        for (int j = 0; j < k; j++) s += l2[(size_t)j * ld + i];
+        xtot[i] = s;
+    }
+}
+
+// Per (jackknife block, job): sum chi2, sum x_tot * N, sum N over kept SNPs.
+__global__ void __launch_bounds__(NT) k_p_sums(const PartJob* __restrict__ jobs, const double* __restrict__ xtot,
+                                              int nb, double* __restrict__ part) {
+    __shared__ double red[NT / 32];
+    const int b = blockIdx.x, j = blockIdx.y;
+    const PartJob jb = jobs[j];
+    const uint64_t lo = (uint64_t)jb.seps[b], hi = (uint64_t)jb.seps[b + 1];
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    for (uint64_t i = lo + threadIdx.x; i < hi; i += NT) {
+        if (!part_kept(jb, i)) continue;
+        const double nn = part_n(jb, i);
+        s0 += jb.chi2[i];
+        s1 += xtot[i] * nn;
+        s2 += nn;
+    }
+    double* out = part + ((size_t)j * nb + b) * 3;
+    s0 = block_sum(s0, red);
+    s1 = block_sum(s1, red);
+    s2 = block_sum(s2, red);
+    if (threadIdx.x == 0) {
+        out[0] = s0;
+        out[1] = s1;
+        out[2] = s2;
+    }
+}
+
+// nbar, mean chi2 and the aggregate h2 that seeds the weights
+// (src/regressions.rs:1189-1191).
+__global__ void k_p_aggregate(const PartJob* __restrict__ jobs, const double* __restrict__ part, int nb,
+                              double m_tot, PartState* __restrict__ st, int njobs) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= njobs) return;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    for (int b = 0; b < nb; b++) {
+        const double* p = part + ((size_t)j * nb + b) * 3;
+        s0 += p[0];
+        s1 += p[1];
+        s2 += p[2];
+    }
+    const double nobs = jobs[j].n_obs;
+    PartState& o = st[j];
+    o.n_obs = nobs;
+    o.nbar = s2 / nobs;
+    o.mean_chi2 = s0 / nobs;
+    o.agg_int = jobs[j].fixed ? jobs[j].fixed_int : 1.0;
+    o.hsq = m_tot * (o.mean_chi2 - o.agg_int) / (s1 / nobs);
+}
+
+// Gram of the augmented weighted design over one jackknife block, one 64 x 64
+// tile pair (ti <= tj) per CTA.  Columns: K scaled LD scores N_i l2_ij / nbar,
+// the intercept column (free intercept only), y = chi2 - fixed intercept.
+__global__ void __launch_bounds__(NT) k_p_gram(const PartJob* __restrict__ jobs, const PartState* __restrict__ st,
+                                              const double* __restrict__ l2, uint64_t ld, int k,
+                                              const double* __restrict__ xtot, const double* __restrict__ wld,
+                                              double m_tot, int nb, int q, double* __restrict__ gram) {
+    __shared__ __align__(16) double As[ROWS * SROW];
+    __shared__ __align__(16) double Bs[ROWS * SROW];
+    __shared__ double rw[ROWS], rs[ROWS], ry[ROWS];
+    __shared__ int rk[ROWS];
+    const int b = blockIdx.x, j = blockIdx.z;
+    // tile pair index -> (ti, tj), ti <= tj, row-major over the upper triangle
+    const int nt = (q + TILE - 1) / TILE;
+    int ti = 0, rem = blockIdx.y;
+    while (rem >= nt - ti) {
+        rem -= nt - ti;
+        ti++;
+    }
+    const int tj = ti + rem;
+    const PartJob jb = jobs[j];
+    const PartState s = st[j];
+    const bool free_int = !jb.fixed;
+    const double yoff = jb.fixed ? jb.fixed_int : 0.0;
+    const double hsq = fmin(fmax(s.hsq, 0.0), 1.0);
+    const uint64_t lo = (uint64_t)jb.seps[b], hi = (uint64_t)jb.seps[b + 1];
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    double acc[4][4];
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+#pragma unroll
+        for (int v = 0; v < 4; v++) acc[u][v] = 0.0;
+
+    for (uint64_t r0 = lo; r0 < hi; r0 += ROWS) {
+        if (threadIdx.x < ROWS) {
+            const uint64_t i = r0 + threadIdx.x;
+            double w = 0.0, sc = 0.0, y = 0.0;
+            const bool kept = i < hi && part_kept(jb, i);
+            if (kept) {
+                // ldsc_weights (src/h2.rs:185-206) on x_tot with M = sum(M_k)
+                const double nn = part_n(jb, i);
+                const double c = hsq * nn / m_tot;
+                const double t = s.agg_int + c * fmax(xtot[i], 1.0);
+                w = 1.0 / (2.0 * t * t) / fmax(wld[i], 1.0);
+                sc = nn / s.nbar;
+                y = jb.chi2[i] - yoff;
+            }
+            rw[threadIdx.x] = w;
+            rs[threadIdx.x] = sc;
+            ry[threadIdx.x] = y;
+            rk[threadIdx.x] = kept;
+        }
+        __syncthreads();
+        // stage: lane = row (32 consecutive SNPs of one column per warp)
+        for (int e = threadIdx.x; e < 2 * ROWS * TILE; e += NT) {
+            const int side = e / (ROWS * TILE);
+            const int c = (e % (ROWS * TILE)) / ROWS, r = e % ROWS;
+            const int g = (side ? tj : ti) * TILE + c;
+            const uint64_t i = r0 + r;
+            double z = 0.0;
+            if (rk[r]) {
+                if (g < k)
+                    z = l2[(size_t)g * ld + i] * rs[r];
+                else if (g == k && free_int)
+                    z = 1.0;
+                else if (g == q - 1)
+                    z = ry[r];
+            }
+            if (side)
+                Bs[r * SROW + c] = z;
+            else
+                As[r * SROW + c] = z * rw[r];
+        }
+        __syncthreads();
+        const int nr = (int)(hi - r0 < (uint64_t)ROWS ? hi - r0 : (uint64_t)ROWS);
+        for (int r = 0; r < nr; r++) {
+            const double2 a01 = *reinterpret_cast<const double2*>(&As[r * SROW + ty * 4]);
+            const double2 a23 = *reinterpret_cast<const double2*>(&As[r * SROW + ty * 4 + 2]);
+            const double2 b01 = *reinterpret_cast<const double2*>(&Bs[r * SROW + tx * 4]);
+            const double2 b23 = *reinterpret_cast<const double2*>(&Bs[r * SROW + tx * 4 + 2]);
+            const double av[4] = {a01.x, a01.y, a23.x, a23.y};
+            const double bv[4] = {b01.x, b01.y, b23.x, b23.y};
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+#pragma unroll
+                for (int v = 0; v < 4; v++) acc[u][v] = fma(av[u], bv[v], acc[u][v]);
+        }
+        __syncthreads();
+    }
+    // write row <= col and its mirror, so the stored matrix is exactly symmetric
+    double* G = gram + ((size_t)j * nb + b) * (size_t)q * q;
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+            const int rr = ti * TILE + ty * 4 + u, cc = tj * TILE + tx * 4 + v;
+            if (rr < q && cc < q && rr <= cc) {
+                G[(size_t)rr * q + cc] = acc[u][v];
+                G[(size_t)cc * q + rr] = acc[u][v];
+            }
+        }
+}
+
+// tot[j] = sum over blocks in order of the block Grams.
+__global__ void __launch_bounds__(NT) k_p_total(const double* __restrict__ gram, int nb, int qq,
+                                               double* __restrict__ tot) {
+    const int j = blockIdx.y;
+    const int e = blockIdx.x * NT + threadIdx.x;
+    if (e >= qq) return;
+    const double* g = gram + (size_t)j * nb * qq + e;
+    double s = 0.0;
+    for (int b = 0; b < nb; b++) s += g[(size_t)b * qq];
+    tot[(size_t)j * qq + e] = s;
+}
+
+// One solve per CTA: (X'X_tot - X'X_b) beta = X'y_tot - X'y_b for b < nb
+// (the delete values), the total system for b == nb.  Gaussian elimination
+// with partial pivoting (largest |pivot|, first on ties) on the augmented
+// p x (p+1) system in shared memory, then back substitution.
+__global__ void __launch_bounds__(NT) k_p_solve(const double* __restrict__ gram, const double* __restrict__ tot,
+                                               int nb, int q, double* __restrict__ sol) {
+    extern __shared__ __align__(16) double M[];  // p x (p + 1), row-major
+    __shared__ double rv[NT / 32];
+    __shared__ int ri[NT / 32];
+    __shared__ int piv;
+    const int b = blockIdx.x, j = blockIdx.y;
+    const int p = q - 1, w = p + 1;
+    const size_t qq = (size_t)q * q;
+    const double* T = tot + (size_t)j * qq;
+    const double* G = b < nb ? gram + ((size_t)j * nb + b) * qq : nullptr;
+    for (int e = threadIdx.x; e < p * w; e += NT) {
+        const int r = e / w, c = e % w;
+        const int src = r * q + (c < p ? c : q - 1);  // last column: X'y
+        M[e] = G ? T[src] - G[src] : T[src];
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int c = 0; c < p; c++) {
+        // pivot row: largest |M[r][c]|, r >= c, first index on ties
+        double best = -1.0;
+        int bi = p;
+        for (int r = c + threadIdx.x; r < p; r += NT) {
+            const double v = fabs(M[r * w + c]);
+            if (v > best) {
+                best = v;
+                bi = r;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ov = __shfl_xor_sync(0xFFFFFFFFu, best, o);
+            const int oi = __shfl_xor_sync(0xFFFFFFFFu, bi, o);
+            if (ov > best || (ov == best && oi < bi)) {
+                best = ov;
+                bi = oi;
+            }
+        }
+        if (lane == 0) {
+            rv[warp] = best;
+            ri[warp] = bi;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double bv = rv[0];
+            int bidx = ri[0];
+            for (int x = 1; x < NT / 32; x++)
+                if (rv[x] > bv || (rv[x] == bv && ri[x] < bidx)) {
+                    bv = rv[x];
+                    bidx = ri[x];
+                }
+            piv = bidx < p ? bidx : c;  // NaN column: keep the row
+        }
+        __syncthreads();
+        const int pr = piv;
+        if (pr != c)
+            for (int x = c + threadIdx.x; x < w; x += NT) {
+                const double t = M[c * w + x];
+                M[c * w + x] = M[pr * w + x];
+                M[pr * w + x] = t;
+            }
+        __syncthreads();
+        // multipliers, then the trailing update
+        const double d = M[c * w + c];
+        for (int r = c + 1 + threadIdx.x; r < p; r += NT) M[r * w + c] = M[r * w + c] / d;
+        __syncthreads();
+        const int rows = p - c - 1, cols = w - c - 1;
+        for (int e = threadIdx.x; e < rows * cols; e += NT) {
+            const int r = c + 1 + e / cols, x = c + 1 + e % cols;
+            M[r * w + x] = fma(-M[r * w + c], M[c * w + x], M[r * w + x]);
+        }
+        __syncthreads();
+    }
+    // back substitution into the last column
+    for (int c = p - 1; c >= 0; c--) {
+        if (threadIdx.x == 0) M[c * w + p] = M[c * w + p] / M[c * w + c];
+        __syncthreads();
+        const double xc = M[c * w + p];
+        for (int r = threadIdx.x; r < c; r += NT) M[r * w + p] = fma(-M[r * w + c], xc, M[r * w + p]);
+        __syncthreads();
+    }
+    double* out = sol + ((size_t)j * (nb + 1) + b) * p;
+    for (int r = threadIdx.x; r < p; r += NT) out[r] = M[r * w + p];
+}
+
+// Estimates, delete values, jackknife covariance and the h2 figures of each
+// job.  res[j]: [est p][cov p x p][delete values nb x p][h2 per annotation k]
+// [h2_total, h2_total_se, intercept, intercept_se, nbar, mean_chi2, n_obs].
+__global__ void __launch_bounds__(NT) k_p_finish(const PartJob* __restrict__ jobs, const PartState* __restrict__ st,
+                                                const double* __restrict__ sol, const double* __restrict__ m_vec,
+                                                int nb, int k, int p, double* __restrict__ res) {
+    extern __shared__ double mean[];  // p pseudo-value means
+    __shared__ double red[NT / 32];
+    const int j = blockIdx.x;
+    const PartJob jb = jobs[j];
+    const PartState s = st[j];
+    const double* S = sol + (size_t)j * (nb + 1) * p;
+    const double* est = S + (size_t)nb * p;
+    double* R = res + (size_t)j * part_result_len(nb, k, p);
+    double* o_est = R;
+    double* o_cov = o_est + p;
+    double* o_dv = o_cov + (size_t)p * p;
+    double* o_h2 = o_dv + (size_t)nb * p;
+    double* o_sc = o_h2 + k;
+    const double fnb = (double)nb;
+    for (int c = threadIdx.x; c < p; c += NT) {
+        o_est[c] = est[c];
+        double sm = 0.0;
+        for (int b = 0; b < nb; b++) sm += fnb * est[c] - (fnb - 1.0) * S[(size_t)b * p + c];
+        mean[c] = sm / fnb;
+    }
+    for (size_t e = threadIdx.x; e < (size_t)nb * p; e += NT) o_dv[e] = S[e];
+    __syncthreads();
+    // jackknife_se_cov: centred pseudo-values, cov = C'C / ((nb - 1) nb)
+    const double scale = (fnb - 1.0) * fnb;
+    for (int e = threadIdx.x; e < p * p; e += NT) {
+        const int r = e / p, c = e % p;
+        if (r > c) continue;
+        double acc = 0.0;
+        for (int b = 0; b < nb; b++) {
+            const double pr = fnb * est[r] - (fnb - 1.0) * S[(size_t)b * p + r] - mean[r];
+            const double pc = fnb * est[c] - (fnb - 1.0) * S[(size_t)b * p + c] - mean[c];
+            acc = fma(pr, pc, acc);
+        }
+        const double v = scale > 0.0 ? acc / scale : acc;
+        o_cov[(size_t)r * p + c] = v;
+        o_cov[(size_t)c * p + r] = v;
+    }
+    __syncthreads();
+    // total h2 and its SE (total_from_jknife, src/regressions.rs:1565-1610)
+    double tv = 0.0;
+    for (int e = threadIdx.x; e < k * k; e += NT) {
+        const int r = e / k, c = e % k;
+        tv += m_vec[r] * m_vec[c] * (o_cov[(size_t)r * p + c] / (s.nbar * s.nbar));
+    }
+    tv = block_sum(tv, red);
+    if (threadIdx.x == 0) {
+        double tot = 0.0;
+        for (int c = 0; c < k; c++) {
+            const double h = est[c] / s.nbar * m_vec[c];
+            o_h2[c] = h;
+            tot += h;
+        }
+        o_sc[0] = tot;
+        o_sc[1] = sqrt(fmax(tv, 0.0));
+        o_sc[2] = jb.fixed ? jb.fixed_int : est[k];
+        o_sc[3] = jb.fixed ? NAN : sqrt(fmax(o_cov[(size_t)k * p + k], 0.0));
+        o_sc[4] = s.nbar;
+        o_sc[5] = s.mean_chi2;
+        o_sc[6] = s.n_obs;
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_partitioned(const PartJob* jobs, PartState* st, const double* l2, uint64_t ld, int k, bool fixed,
+                               const double* wld, uint64_t n, int nb, double m_tot, const double* m_vec, double* xtot,
+                               bool want_xtot, double* part, double* gram, double* tot, double* sol, double* res,
+                               int njobs, cudaStream_t s) {
+    const int p = part_params(k, fixed), q = p + 1;
+    const int nt = (q + TILE - 1) / TILE;
+    const size_t solve_smem = (size_t)p * (p + 1) * sizeof(double);
+    if (solve_smem > (size_t)PART_SOLVE_SMEM) return cudaErrorInvalidValue;
+    if (want_xtot) {
+        const uint64_t g = (n + NT - 1) / NT;
+        k_p_xtot<<<(unsigned)(g < 148 * 8 ? g : 148 * 8), NT, 0, s>>>(l2, ld, k, n, xtot);
+    }
+    k_p_sums<<<dim3(nb, njobs), NT, 0, s>>>(jobs, xtot, nb, part);
+    k_p_aggregate<<<(njobs + 127) / 128, 128, 0, s>>>(jobs, part, nb, m_tot, st, njobs);
+    k_p_gram<<<dim3(nb, nt * (nt + 1) / 2, njobs), NT, 0, s>>>(jobs, st, l2, ld, k, xtot, wld, m_tot, nb, q, gram);
+    k_p_total<<<dim3((q * q + NT - 1) / NT, njobs), NT, 0, s>>>(gram, nb, q * q, tot);
+    cudaError_t e = cudaFuncSetAttribute(k_p_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve_smem);
+    if (e != cudaSuccess) return e;
+    k_p_solve<<<dim3(nb + 1, njobs), NT, solve_smem, s>>>(gram, tot, nb, q, sol);
+    k_p_finish<<<njobs, NT, (size_t)p * sizeof(double), s>>>(jobs, st, sol, m_vec, nb, k, p, res);
+    return cudaGetLastError();
+}
+
+}  // namespace ldsc

@@ -87,4 +87,40 @@ cudaError_t launch_rg_finish(const RgPairIdx* pairs, const RegOut* outs, const d
 // k-th smallest y of each job (exact), out[job].
 cudaError_t launch_select(const RegJob* jobs, uint64_t n, uint64_t rank, double* out, int njobs, cudaStream_t s);
 
+// ---- partitioned h2 (fit_h2_partitioned, src/regressions.rs:1121-1226) ----
+
+struct PartJob {
+    const double* chi2;    // n (device)
+    const double* nv;      // per-SNP sample sizes (device) or null
+    double ns;             // scalar sample size when nv is null
+    const int32_t* seps;   // nb + 1 jackknife block starts in SNP index space
+    double mask_max;       // SNPs with chi2 < mask_max are kept
+    double n_obs;          // number of kept SNPs
+    int32_t fixed;         // intercept constrained to fixed_int
+    double fixed_int;
+};
+
+struct PartState {
+    double nbar, mean_chi2, hsq, agg_int, n_obs;
+};
+
+// Parameters: K LD-score coefficients, plus the intercept when it is free.
+__host__ __device__ inline int part_params(int k, bool fixed) { return k + (fixed ? 0 : 1); }
+// Doubles per job in the result array: est p, cov p x p, delete values
+// nb x p, h2 per annotation k, then h2_total, h2_total_se, intercept,
+// intercept_se, nbar, mean_chi2, n_obs.
+__host__ __device__ inline size_t part_result_len(int nb, int k, int p) { return (size_t)p * (1 + p + nb) + k + 7; }
+// Shared memory of one delete-value solve (p x (p + 1) doubles) is capped here.
+constexpr int PART_SOLVE_SMEM = 210 * 1024;
+
+// x_tot (when want_xtot), aggregate, per-block Grams of the weighted design,
+// block totals, nb + 1 LU solves and the jackknife for every job.  Scratch:
+// xtot n, part njobs * nb * 3, gram njobs * nb * (p+1)^2, tot njobs *
+// (p+1)^2, sol njobs * (nb+1) * p; res njobs * part_result_len; st njobs.
+// m_vec: k per-annotation M on the device.
+cudaError_t launch_partitioned(const PartJob* jobs, PartState* st, const double* l2, uint64_t ld, int k, bool fixed,
+                               const double* wld, uint64_t n, int nb, double m_tot, const double* m_vec, double* xtot,
+                               bool want_xtot, double* part, double* gram, double* tot, double* sol, double* res,
+                               int njobs, cudaStream_t s);
+
 }  // namespace ldsc

@@ -12,6 +12,10 @@ Follows, step for step:
   ratio_jackknife                        src/regressions.rs:1067-1120
   gencov_weights / run_gencov_ldsc       src/regressions.rs:1612-1645, 1828-2052
   rg, z, p                               src/regressions.rs:2389-2465
+  run_h2's K > 1 filters                 src/regressions.rs:553-593
+  fit_h2_partitioned                     src/regressions.rs:1121-1226
+  total_from_jknife                      src/regressions.rs:1565-1610
+  write_overlap_results (the figures)    src/regressions.rs:1262-1440
 faer's QR and LU are replaced by numpy's (same factorisations, different
 rounding order).
 """
@@ -220,3 +224,115 @@ def run_rg(z1, z2, ref_l2, w_l2, n1, n2, m, n_blocks=200):
     return dict(rg=rg, rg_se=rg_se, z=z, p=p, gencov=g["tot"], gencov_se=g["tot_se"], gencov_intercept=g["intercept"],
                 gencov_intercept_se=g["intercept_se"], h2_1=h1["h2"], h2_1_se=h1["h2_se"], h2_2=h2["h2"],
                 h2_2_se=h2["h2_se"], mean_z1z2=g["mean_z1z2"])
+
+
+def fit_h2_partitioned(chi2, ref_l2_k, w_l2, n_vec, m_vec, n_blocks=200, intercept_h2=None, no_intercept=False,
+                       chisq_max=None):
+    """run_h2's K > 1 branch: drop NaN chi2 / N, drop chi2 >= chisq_max
+    (default max(0.001 max N, 80)), then fit_h2_partitioned.  ref_l2_k: n x K."""
+    chi2 = np.asarray(chi2, float)
+    x_raw = np.asarray(ref_l2_k, float).reshape(len(chi2), -1)
+    w_l2 = np.asarray(w_l2, float)
+    n_vec = np.broadcast_to(np.asarray(n_vec, float), chi2.shape).copy()
+    valid = ~np.isnan(chi2) & ~np.isnan(n_vec)
+    chi2, x_raw, w_l2, n_vec = chi2[valid], x_raw[valid], w_l2[valid], n_vec[valid]
+    if chisq_max is None:
+        chisq_max = max(0.001 * max(float(n_vec.max(initial=0.0)), 0.0), 80.0)
+    keep = chi2 < chisq_max
+    chi2, x_raw, w_l2, n_vec = chi2[keep], x_raw[keep], w_l2[keep], n_vec[keep]
+    n_obs, k = x_raw.shape
+    n_mean = n_vec.mean()
+    m_vec = np.asarray(m_vec, float)
+    m_total = float(np.sum(m_vec))
+    nb = min(n_obs, n_blocks)
+    x_tot = np.zeros(n_obs)
+    for j in range(k):
+        x_tot = x_tot + x_raw[:, j]
+    fixed = intercept_h2 if intercept_h2 is not None else (1.0 if no_intercept else None)
+    y_reg = chi2 - fixed if fixed is not None else chi2.copy()
+    scale = n_vec / n_mean
+    x_reg = x_raw * scale[:, None]
+    if fixed is None:
+        x_reg = np.concatenate([x_reg, np.ones((n_obs, 1))], axis=1)
+    agg_int = fixed if fixed is not None else 1.0
+    hsq = aggregate(chi2, x_tot, n_vec, m_total, agg_int)
+    initial_w = ldsc_weights(x_tot, w_l2, n_vec, m_total, hsq, agg_int)
+    xw, yw = weight_xy(x_reg, y_reg, np.sqrt(initial_w))
+    jk = jackknife_fast(xw, yw, nb)
+    coef = jk["est"][:k] / n_mean
+    h2_annot = coef * m_vec
+    h2_total = float(np.sum(h2_annot))
+    intercept = fixed if fixed is not None else float(jk["est"][k])
+    intercept_se = float("nan") if fixed is not None else float(math.sqrt(_rmax0(jk["cov"][k, k])))
+    coef_cov = jk["cov"][:k, :k] / (n_mean * n_mean)
+    tot_cov = 0.0
+    for i in range(k):
+        for j in range(k):
+            tot_cov += m_vec[i] * m_vec[j] * coef_cov[i, j]
+    return dict(est=jk["est"], cov=jk["cov"], delete_values=jk["delete_values"], m_vec=m_vec, n_mean=n_mean,
+                h2_annot=h2_annot, h2_total=h2_total, h2_total_se=math.sqrt(_rmax0(tot_cov)), intercept=intercept,
+                intercept_se=intercept_se, n_obs=n_obs, n_blocks=nb, mean_chi2=float(chi2.mean()))
+
+
+def _ratio_jackknife_mat(est, numer, denom):
+    nb, k = numer.shape
+    pseudo = np.zeros((nb, k))
+    for b in range(nb):
+        for j in range(k):
+            pseudo[b, j] = float("nan") if denom[b, j] == 0.0 else \
+                nb * est[j] - (nb - 1.0) * (numer[b, j] / denom[b, j])
+    mean = pseudo.sum(axis=0) / nb
+    c = pseudo - mean
+    cov = c.T @ c
+    scale = (nb - 1.0) * nb
+    if scale > 0.0:
+        cov = cov / scale
+    return cov
+
+
+def overlap_figures(fit, overlap, m_tot):
+    """The per-category figures of write_overlap_results (before formatting):
+    prop_m, prop_h2, prop_h2_se, enrichment, enrichment_se, t statistic of the
+    coefficient difference (diff_na where its SE is 0), coef, coef_se."""
+    k = len(fit["m_vec"])
+    m_vec = fit["m_vec"]
+    n_mean = fit["n_mean"]
+    coef = fit["est"][:k] / n_mean
+    coef_cov = fit["cov"][:k, :k] / (n_mean * n_mean)
+    coef_se = np.sqrt(np.array([_rmax0(coef_cov[j, j]) for j in range(k)]))
+    h2_total = fit["h2_total"]
+    prop = np.array([h / h2_total if abs(h2_total) > 1e-12 else float("nan") for h in fit["h2_annot"]])
+    dv = fit["delete_values"]
+    nb = dv.shape[0]
+    numer = np.zeros((nb, k))
+    for b in range(nb):
+        for j in range(k):
+            numer[b, j] = m_vec[j] * dv[b, j] / n_mean
+    denom = np.zeros((nb, k))
+    for b in range(nb):
+        denom[b, :] = numer[b, :].sum()
+    prop_cov = _ratio_jackknife_mat(prop, numer, denom)
+    overlap_prop = np.zeros((k, k))
+    for i in range(k):
+        for j in range(k):
+            overlap_prop[i, j] = overlap[i, j] / m_vec[j]
+    prop_h2_overlap = overlap_prop @ prop
+    var = overlap_prop @ prop_cov @ overlap_prop.T
+    prop_h2_overlap_se = np.sqrt(np.array([_rmax0(var[j, j]) for j in range(k)]))
+    prop_m = np.array([m / m_tot if m_tot > 0 else float("nan") for m in m_vec])
+    enrichment = prop_h2_overlap / prop_m
+    enrichment_se = prop_h2_overlap_se / prop_m
+    diff = np.zeros((k, k))
+    for i in range(k):
+        if abs(m_tot - m_vec[i]) < 1e-12:
+            continue
+        for j in range(k):
+            diff[i, j] = overlap[i, j] / m_vec[i] - (m_vec[j] - overlap[i, j]) / (m_tot - m_vec[i])
+    diff_est = diff @ coef
+    diff_cov = diff @ coef_cov @ diff.T
+    diff_se = np.sqrt(np.array([_rmax0(diff_cov[j, j]) for j in range(k)]))
+    na = np.array([diff_se[i] == 0.0 for i in range(k)])
+    with np.errstate(divide="ignore", invalid="ignore"):
+        t = np.array([abs(diff_est[i] / diff_se[i]) for i in range(k)])
+    return dict(prop_m=prop_m, prop_h2=prop_h2_overlap, prop_h2_se=prop_h2_overlap_se, enrichment=enrichment,
+                enrichment_se=enrichment_se, diff_t=t, diff_na=na, coef=coef, coef_se=coef_se)
