@@ -23,6 +23,7 @@ import numpy as np
 
 from . import io as lio
 from .api import Context, LdscError, WindowMode, run_l2, snp_stats
+from .sliced import call_bytes_per_record, run_l2_sliced
 from .plink import BimTable, count_fam, parse_bim, parse_fam_text, read_bed
 
 
@@ -63,7 +64,49 @@ def build_parser() -> argparse.ArgumentParser:
     ap.add_argument("--gpu-precision", choices=["int8", "fp64"], default="int8",
                     help="arithmetic of the exact form (engine flag; int8 is exact)")
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--max-device-gb", type=float,
+                    help="device memory for the panel and workspace (engine flag); a larger panel runs in "
+                         "SNP slices.  Default: the free device memory less 4 GB, used only when needed")
     return ap
+
+
+def _slice_budget(args, snps: BimTable, n_indiv: int, mode: WindowMode, chunk_c: int, annot, iid,
+                  global_pass: bool) -> Optional[int]:
+    """Device bytes for a sliced run, or None when the whole panel fits."""
+    per = call_bytes_per_record(snps, n_indiv, mode, chunk_c, annot=annot, iid_indices=iid,
+                                precision=args.gpu_precision, sketch=args.sketch,
+                                snp_level_masking=args.snp_level_masking, global_pass=global_pass)
+    need = per * len(snps)
+    if args.max_device_gb is not None:
+        budget = int(args.max_device_gb * 1e9)
+        return budget if need > budget else None
+    import torch
+    free = torch.cuda.mem_get_info(args.device)[0] - (4 << 30)
+    return int(free) if need > free else None
+
+
+def _snp_stats_sliced(ctx: Context, snps: BimTable, body: np.ndarray, n_indiv: int, iid, budget: int):
+    """compute_snp_stats on row slices of the panel (per-record, no halos)."""
+    bpr = (n_indiv + 3) // 4
+    rows = max(1, int(budget // max(bpr + 64, 1)))
+    bed_idx = np.asarray(snps.bed_idx, dtype=np.int64)
+    maf = np.zeros(len(snps))
+    ok = np.zeros(len(snps), dtype=bool)
+    rb = np.asarray(body).reshape(-1, bpr)
+    a = 0
+    while a < len(snps):
+        b = int(np.searchsorted(bed_idx, bed_idx[a] + rows, side="left"))
+        b = max(b, a + 1)
+        r0, r1 = int(bed_idx[a]), int(bed_idx[b - 1]) + 1
+        sub = snps.subset(np.arange(a, b))
+        sub = BimTable(sub.chr, sub.snp, sub.cm, sub.bp, np.asarray(sub.bed_idx, dtype=np.int64) - r0)
+        panel = ctx.upload(rb[r0:r1], n_indiv)
+        try:
+            maf[a:b], ok[a:b] = snp_stats(ctx, sub, panel, iid)
+        finally:
+            panel.close()
+        a = b
+    return maf, ok
 
 
 def run(args, ctx: Optional[Context] = None) -> None:
@@ -144,18 +187,25 @@ def run(args, ctx: Optional[Context] = None) -> None:
         iid = lio.load_individual_indices(args.keep, fam_ids)
     n_used = len(iid) if iid is not None else n_indiv
 
-    # ---- the panel, resident for the prefilter and the compute ----
+    # ---- the panel: resident for the prefilter and the compute, or, when it
+    # does not fit the device budget, uploaded slice by slice ----
     own_ctx = ctx is None
     ctx = ctx or Context(args.device)
+    chunk_c = 50 if args.python_compat else args.chunk_size
+    global_pass = args.global_pass or args.python_compat
     t_bed0 = time.perf_counter()
-    body = read_bed(bed_path, n_indiv, len(snps_raw))
-    panel = ctx.upload(body, n_indiv)
+    budget = _slice_budget(args, snps, n_indiv, mode, chunk_c, annot, iid, global_pass)
+    body = read_bed(bed_path, n_indiv, len(snps_raw), mmap=budget is not None or args.mmap)
+    panel = None if budget is not None else ctx.upload(body, n_indiv)
     t_bed = time.perf_counter() - t_bed0
     try:
         # ---- --maf / --pq-exp prefilter (src/l2/mod.rs:265-333) ----
         maf_pre_vals = None
         if args.maf_pre and (args.maf is not None or pq_exp is not None):
-            maf_all, ok = snp_stats(ctx, snps, panel, iid)
+            if panel is None:
+                maf_all, ok = _snp_stats_sliced(ctx, snps, body, n_indiv, iid, budget)
+            else:
+                maf_all, ok = snp_stats(ctx, snps, panel, iid)
             thr = args.maf if args.maf is not None else 0.0
             keep_mask = ok & (maf_all > thr)
             if not keep_mask.any():
@@ -174,8 +224,6 @@ def run(args, ctx: Optional[Context] = None) -> None:
             pq_scaled = True
         pq_for_compute = None if pq_scaled else pq_exp
 
-        chunk_c = 50 if args.python_compat else args.chunk_size
-        global_pass = args.global_pass or args.python_compat
         if args.python_compat:
             if args.chunk_size != 200:
                 print(f"--python-compat overrides --chunk-size {args.chunk_size} with c=50 for Python LDSC parity",
@@ -188,18 +236,29 @@ def run(args, ctx: Optional[Context] = None) -> None:
             print(f"[perf] maf_prefilter={time.perf_counter() - t_run0 - t_bed:.3f}s", file=sys.stderr)
 
         t_c0 = time.perf_counter()
-        l2, maf, perf = run_l2(ctx, snps, panel, mode, chunk_c, annot=annot, iid_indices=iid,
-                               pq_exp=pq_for_compute, yes_really=args.yes_really, use_f32=args.fast_f32,
-                               sketch=args.sketch, sketch_maf_aware=args.sketch_maf_aware,
-                               snp_level_masking=args.snp_level_masking, global_pass=global_pass,
-                               precision=args.gpu_precision)
+        if panel is None:
+            l2, maf, slices, perfs = run_l2_sliced(
+                ctx, snps, body, n_indiv, mode, chunk_c, device_budget_bytes=budget, annot=annot,
+                iid_indices=iid, pq_exp=pq_for_compute, sketch=args.sketch,
+                sketch_maf_aware=args.sketch_maf_aware, snp_level_masking=args.snp_level_masking,
+                global_pass=global_pass, precision=args.gpu_precision, use_f32=args.fast_f32)
+            print(f"  panel larger than the device budget ({budget / 1e9:.1f} GB): computed in "
+                  f"{len(slices)} SNP slices", file=sys.stderr)
+            perf = perfs[-1]
+        else:
+            l2, maf, perf = run_l2(ctx, snps, panel, mode, chunk_c, annot=annot, iid_indices=iid,
+                                   pq_exp=pq_for_compute, yes_really=args.yes_really, use_f32=args.fast_f32,
+                                   sketch=args.sketch, sketch_maf_aware=args.sketch_maf_aware,
+                                   snp_level_masking=args.snp_level_masking, global_pass=global_pass,
+                                   precision=args.gpu_precision)
         if args.verbose_timing:
             print(f"[perf] bed_read={t_bed:.3f}s norm={perf.norm_secs:.3f}s "
                   f"ab_dot={perf.ab_dot_secs:.3f}s device={perf.device_ms / 1e3:.3f}s "
                   f"pairs={perf.n_pairs}", file=sys.stderr)
             print(f"[perf] compute_ldscore_total={time.perf_counter() - t_c0:.3f}s", file=sys.stderr)
     finally:
-        panel.close()
+        if panel is not None:
+            panel.close()
         if own_ctx:
             ctx.close()
 

@@ -1,19 +1,26 @@
-"""Sharding an l2 run over the ranks of a process group (one GPU per rank).
+"""Splitting an l2 run into record ranges: over the ranks of a process group
+(one GPU per rank), or into slices that run one after another on one GPU
+when the panel is larger than device memory.
 
-The path shards without a data-path collective:
+Every pair (k, j), k < j, that a run accumulates satisfies left[j] <= k,
+and left is non-decreasing.  A core of records [lo, hi) therefore gets its
+exact l2 from one call over [call_lo, call_hi):
 
-* default per-chromosome mode: chromosomes are independent
-  (src/l2/mod.rs:477-553), so each rank takes whole chromosomes, balanced by
-  their pair counts;
-* --snp-level-masking: every SNP's window is its own, independent of the
-  chunk grid (src/l2/compute.rs:1855-1867), so a chromosome may also be cut
-  inside; a rank computes its core records plus a halo -- the records its
-  core pairs with on either side -- and keeps the core rows;
-* --global-pass without masking: the chunk grid runs across chromosomes from
-  the first record, so the run is not split (rank 0 computes it).
+* call_lo = left[lo], the core's smallest limit, moved down to the chunk
+  grid (the first record of its chromosome in the default per-chromosome
+  mode, record 0 with --global-pass; src/l2/compute.rs:1164-1184).  A call
+  that starts on the grid at or below every core limit chunks the core and
+  everything after it exactly as the whole run does, and its block_left
+  values are not clipped there.  With --snp-level-masking every window is
+  the SNP's own (src/l2/compute.rs:1855-1867) and no alignment is needed;
+* call_hi = the first record j >= hi with left[j] >= hi: the records after
+  the core that pair with one of its records.
 
-The only exchange is the final gather of the l2 rows (`gather_l2`), the step
-the reference's single process does not need.
+The call's own rows outside the core (the halos) are discarded.  Chromosomes
+are independent (src/l2/mod.rs:477-553), so a core that holds whole
+chromosomes needs no halo.  The only exchange between ranks is the final
+gather of the l2 rows (`gather_l2`), the step the reference's single process
+does not need.
 """
 from __future__ import annotations
 
@@ -36,56 +43,94 @@ class Shard:
     pairs: int       # in-band pairs of the core records (the load)
 
 
-def _balanced_cuts(load: np.ndarray, units: Sequence[int], world: int) -> List[int]:
-    """Cut positions (indices into `units` boundaries) splitting the units into
-    `world` contiguous groups with about equal load."""
-    cum = np.concatenate([[0], np.cumsum(load)])
+def _balanced_cuts(load: np.ndarray, world: int) -> List[int]:
+    """Cut positions 0 = c_0 <= ... <= c_world = len(load) splitting the
+    records into `world` contiguous groups with about equal load."""
+    cum = np.concatenate([[0.0], np.cumsum(load, dtype=np.float64)])
     total = cum[-1]
+    n = len(load)
     cuts = [0]
     for r in range(1, world):
         target = total * r / world
         i = int(np.searchsorted(cum, target))
         # nearest boundary, never before the previous cut
-        if i > 0 and abs(cum[i - 1] - target) <= abs(cum[min(i, len(cum) - 1)] - target):
+        if i > 0 and abs(cum[i - 1] - target) <= abs(cum[min(i, n)] - target):
             i -= 1
-        cuts.append(max(cuts[-1], min(i, len(units) - 1)))
-    cuts.append(len(units) - 1)
+        cuts.append(max(cuts[-1], min(i, n)))
+    cuts.append(n)
     return cuts
+
+
+def chunk_origin(snps: BimTable, global_pass: bool) -> np.ndarray:
+    """First record of each record's chunking group: its chromosome's first
+    record, or 0 with --global-pass."""
+    m = len(snps)
+    if global_pass or m == 0:
+        return np.zeros(m, dtype=np.int64)
+    chr_ = np.asarray(snps.chr)
+    starts = np.flatnonzero(np.concatenate([[True], chr_[1:] != chr_[:-1]]))
+    return starts[np.searchsorted(starts, np.arange(m), side="right") - 1].astype(np.int64)
+
+
+def call_range(left: np.ndarray, origin: np.ndarray, chunk_c: int, snp_level_masking: bool,
+               lo: int, hi: int) -> tuple:
+    """Records [call_lo, call_hi) of the call that gives the core [lo, hi)
+    its exact l2 (see the module note)."""
+    m = len(left)
+    if lo >= hi:
+        return lo, lo
+    a = int(left[lo])
+    if not snp_level_masking:
+        g = int(origin[a])
+        a = g + (a - g) // chunk_c * chunk_c
+    b = max(hi, int(np.searchsorted(left, hi, side="left")))
+    return a, min(b, m)
+
+
+def _shard(rank: int, lo: int, hi: int, left, origin, chunk_c, masking, pairs) -> Shard:
+    a, b = call_range(left, origin, chunk_c, masking, lo, hi)
+    return Shard(rank, lo, hi, a, b, int(pairs[lo:hi].sum()))
 
 
 def plan_shards(snps: BimTable, mode: WindowMode, world: int, chunk_c: int = 200,
                 snp_level_masking: bool = False, global_pass: bool = False) -> List[Shard]:
-    """Split the records over `world` ranks (see the module note)."""
+    """Split the records over `world` ranks with about equal pair counts."""
     m = len(snps)
     left = left_limits(snps, mode, chunk_c, snp_level_masking=snp_level_masking, global_pass=global_pass)
     pairs = np.arange(m, dtype=np.int64) - left          # pairs (k, j), k < j, credited to j
-    if m == 0 or world == 1 or (global_pass and not snp_level_masking):
-        return [Shard(0, 0, m, 0, m, int(pairs.sum()))] + [Shard(r, m, m, m, m, 0) for r in range(1, world)]
-    if not snp_level_masking:
-        # whole chromosomes: boundaries where the chromosome code changes
-        bounds = [0] + [i for i in range(1, m) if snps.chr[i] != snps.chr[i - 1]] + [m]
-        load = np.array([pairs[a:b].sum() for a, b in zip(bounds[:-1], bounds[1:])], dtype=np.float64)
-        cuts = _balanced_cuts(load, bounds, world)
-        out = []
-        for r in range(world):
-            lo, hi = bounds[cuts[r]], bounds[cuts[r + 1]]
-            out.append(Shard(r, lo, hi, lo, hi, int(pairs[lo:hi].sum())))
-        return out
-    # per-SNP windows: cut anywhere, by pair count; halo from the left limits
-    bounds = list(range(m + 1))
-    cuts = _balanced_cuts(pairs.astype(np.float64), bounds, world)
-    out = []
-    for r in range(world):
-        lo, hi = cuts[r], cuts[r + 1]
-        if lo >= hi:
-            out.append(Shard(r, lo, lo, lo, lo, 0))
-            continue
-        call_lo = int(left[lo:hi].min())
-        # right partners k >= hi of the core: left[k] < hi (left is non-decreasing within a chromosome)
-        call_hi = hi
-        while call_hi < m and left[call_hi] < hi and snps.chr[call_hi] == snps.chr[hi - 1]:
-            call_hi += 1
-        out.append(Shard(r, lo, hi, call_lo, call_hi, int(pairs[lo:hi].sum())))
+    origin = chunk_origin(snps, global_pass)
+    cuts = _balanced_cuts(pairs.astype(np.float64), world) if m else [0] * (world + 1)
+    return [_shard(r, cuts[r], cuts[r + 1], left, origin, chunk_c, snp_level_masking, pairs) for r in range(world)]
+
+
+def plan_slices(snps: BimTable, mode: WindowMode, max_call_records: int, chunk_c: int = 200,
+                snp_level_masking: bool = False, global_pass: bool = False) -> List[Shard]:
+    """Consecutive slices for one device, each call at most max_call_records
+    records (core plus halos), cores as large as the budget allows."""
+    m = len(snps)
+    left = left_limits(snps, mode, chunk_c, snp_level_masking=snp_level_masking, global_pass=global_pass)
+    pairs = np.arange(m, dtype=np.int64) - left
+    origin = chunk_origin(snps, global_pass)
+    out: List[Shard] = []
+    lo = 0
+    while lo < m:
+        def fits(hi):
+            a, b = call_range(left, origin, chunk_c, snp_level_masking, lo, hi)
+            return b - a <= max_call_records
+        if not fits(lo + 1):
+            a, b = call_range(left, origin, chunk_c, snp_level_masking, lo, lo + 1)
+            raise ValueError(f"record {lo} needs a call of {b - a} records (window plus halo), more than "
+                             f"the budget of {max_call_records}")
+        # largest hi that fits (the call grows with hi)
+        good, bad = lo + 1, m + 1
+        while bad - good > 1:
+            mid = (good + bad) // 2
+            if fits(mid):
+                good = mid
+            else:
+                bad = mid
+        out.append(_shard(len(out), lo, good, left, origin, chunk_c, snp_level_masking, pairs))
+        lo = good
     return out
 
 

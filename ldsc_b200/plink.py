@@ -116,8 +116,10 @@ def validate_bed(data: bytes | np.ndarray, n_indiv: int, n_snp: int) -> np.ndarr
     return buf[3:]
 
 
-def read_bed(path: str, n_indiv: int, n_snp: int) -> np.ndarray:
-    data = np.fromfile(path, dtype=np.uint8)
+def read_bed(path: str, n_indiv: int, n_snp: int, mmap: bool = False) -> np.ndarray:
+    """The validated BED body; with mmap, a read-only memory map of the file
+    (rows are read when a slice of them is uploaded)."""
+    data = np.memmap(path, dtype=np.uint8, mode="r") if mmap else np.fromfile(path, dtype=np.uint8)
     return validate_bed(data, n_indiv, n_snp)
 
 

@@ -1,8 +1,9 @@
 """Sharded l2 over two ranks (gloo, CPU).  The compute step is the C oracle
-standing in for each rank's GPU call; what is tested is the plan (whole
-chromosomes by default, cores + halos with per-SNP windows) and the gather,
-against one unsharded oracle run.  src/l2/mod.rs:477-553 (chromosomes are
-independent), src/l2/compute.rs:1855-1867 (per-SNP windows)."""
+standing in for each rank's GPU call; what is tested is the plan (cores
+balanced by pair count, halos from the left limits, aligned to the chunk grid
+without per-SNP windows) and the gather, against one unsharded oracle run.
+src/l2/mod.rs:477-553 (chromosomes are independent),
+src/l2/compute.rs:1164-1184 (chunk windows), 1855-1867 (per-SNP windows)."""
 import os
 import socket
 
@@ -66,19 +67,18 @@ def test_two_ranks_equal_one_run(tmp_path, masking):
                                           chunk_c=200, masking=masking))
     np.testing.assert_allclose(got, ref, rtol=1e-10, atol=1e-12)
     assert plan[0, 1] == plan[1, 0] and plan[1, 1] == spec.m     # cores tile the records
-    if masking:
-        assert plan[1, 2] < plan[1, 0]                            # the second rank needs a left halo
-        assert 0 < plan[0, 1] < spec.m and plan[0, 1] not in (900, 1400)   # cut inside a chromosome
-    else:
-        assert plan[0, 1] in (900, 1400)                          # whole chromosomes
-        assert (plan[:, 0] == plan[:, 2]).all() and (plan[:, 1] == plan[:, 3]).all()
+    assert 0 < plan[0, 1] < spec.m and plan[0, 1] not in (900, 1400)   # cut inside a chromosome
+    assert plan[1, 2] < plan[1, 0]                                # the second rank needs a left halo
+    if not masking:
+        assert (plan[1, 2] - 900) % 200 == 0                      # on chromosome 2's chunk grid
 
 
-def test_global_pass_is_not_split():
+def test_global_pass_splits_on_the_global_grid():
     from ldsc_b200.api import WindowMode
     from ldsc_b200.parallel import plan_shards
     from ldsc_b200.plink import BimTable
     spec, body, chr_, cm, bp = _panel()
     snps = BimTable(chr_, [f"rs{i}" for i in range(spec.m)], cm, bp, np.arange(spec.m, dtype=np.int64))
     plan = plan_shards(snps, WindowMode.Cm(1.0), 2, global_pass=True)
-    assert (plan[0].core_lo, plan[0].core_hi) == (0, spec.m) and plan[1].core_hi == plan[1].core_lo
+    assert plan[0].core_hi == plan[1].core_lo and 0 < plan[1].core_lo < spec.m
+    assert plan[1].call_lo % 200 == 0 and plan[1].call_lo < plan[1].core_lo
