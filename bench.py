@@ -272,6 +272,7 @@ def run_partitioned_workload(args, ctx, stream):
                 "contraction_ms": 1e3 * pr.contract_secs,
                 "device_ms": pr.device_ms,
                 "matches_host_call": float(np.max(np.abs(d_l2.T.cpu().numpy() - res["int8"][1][0])))}
+    h2p = _partitioned_h2(ctx, stream, d_l2, annot, args)
     l2i = res["int8"][1][0]
     l2f = res["fp64"][1][0]
     # oracle on the three smallest chromosomes (independent in per-chromosome mode)
@@ -291,9 +292,57 @@ def run_partitioned_workload(args, ctx, stream):
            "int8_vs_oracle_chr20_22": float(np.max(np.abs(l2i[start:] - ref) / scale)),
            "fp64_vs_oracle_chr20_22": float(np.max(np.abs(l2f[start:] - ref) / scale)),
            "int8_vs_fp64_all": float(np.max(np.abs(l2i - l2f) / np.maximum(np.abs(l2f).max(axis=0, keepdims=True), 1.0))),
-           "error_metric": "max |l2_jC - ref_jC| / max(max_j |ref_jC|, 1) per annotation column"}
+           "error_metric": "max |l2_jC - ref_jC| / max(max_j |ref_jC|, 1) per annotation column",
+           "h2_partitioned": h2p}
     print(json.dumps(out), flush=True)
     panel.close()
+
+
+def _partitioned_h2(ctx, stream, d_l2, annot, args, n_traits=8, n_blocks=200):
+    """Partitioned h2 (fit_h2_partitioned) of n_traits synthetic traits on the
+    device-resident K-column LD scores just computed: chi2 = (sqrt(N s) b +
+    e)^2 with s = max(h2 (l2_all + sum_c tau_c l2_c) / M, 0) over the binary
+    annotations (generating total h2 = h2 sum_k tau_k M_k / M), w_l2 = the
+    all-ones column's l2, M_k = annotation column sums.  Times the whole call (device pointers in, estimates out) and checks
+    the first trait against the oracle."""
+    import torch
+    from ldsc_b200.partitioned import default_chisq_max, h2_partitioned_device
+    from oracle import regress_oracle as R
+    K, m = int(d_l2.shape[0]), int(d_l2.shape[1])
+    l2h = d_l2.T.cpu().numpy()
+    rng = np.random.default_rng(17)
+    h2 = rng.uniform(0.1, 0.5, n_traits)
+    nn = np.exp(rng.uniform(np.log(5e4), np.log(3e5), n_traits))
+    tau = np.zeros((n_traits, K))
+    tau[:, 0] = 1.0
+    tau[:, 1:81] = rng.uniform(0.0, 0.5, (n_traits, 80))
+    s = np.maximum((h2[:, None] / m) * (tau @ l2h.T), 0.0)
+    z = np.sqrt(nn[:, None] * s) * rng.standard_normal((n_traits, m)) + rng.standard_normal((n_traits, m))
+    chi2 = z * z
+    m_vec = annot.sum(axis=0)
+    cmax = np.array([default_chisq_max(chi2[t], nn[t]) for t in range(n_traits)])
+    d_chi2 = torch.from_numpy(chi2).cuda()
+    d_n = torch.from_numpy(nn).cuda()
+    w = d_l2[0].contiguous()
+    call = lambda: h2_partitioned_device(ctx, d_chi2, d_n, d_l2, w, m_vec, cmax, n_blocks)  # noqa: E731
+    t, outs = _timed_passes(ctx, stream, call, max(args.warmup, 1), max(args.steps, 3))
+    fits = outs[-1]
+    want = R.fit_h2_partitioned(chi2[0], l2h, l2h[:, 0], nn[0], m_vec, n_blocks)
+    got = fits[0]
+    n_obs = sum(f.n_obs for f in fits)
+    q = K + 2                       # augmented columns: K LD scores, intercept, chi2
+    gram_flops = n_obs * q * (q + 1)  # upper triangle, one multiply-add per entry and kept SNP
+    ms = 1e3 * t / max(args.steps, 3)
+    return {"traits": n_traits, "annotations": K, "n_snp": m, "n_blocks": n_blocks, "ms_per_call": ms,
+            "traits_per_s": n_traits / (ms / 1e3), "gram_flops_per_call": gram_flops,
+            "gram_tflops_lower_bound": gram_flops / (ms / 1e3) / 1e12,
+            "h2_total": [f.h2_total for f in fits],
+            "h2_generating": [float(h2[t] / m * np.dot(tau[t], m_vec)) for t in range(n_traits)],
+            "vs_oracle_trait0": {"h2_total_rel": abs(got.h2_total - want["h2_total"]) / abs(want["h2_total"]),
+                                 "est_max_rel": float(np.max(np.abs(got.est - want["est"])) /
+                                                      np.max(np.abs(want["est"])))},
+            "note": "whole ldsc_h2_partitioned call on device pointers (8 traits x 500,000 SNPs x 97 "
+                    "annotations); the Gram rate is a lower bound (call time includes the solves)"}
 
 
 def run_serving_workload(args, ctx, duration_s: float, rate: float, seed: int = 7):

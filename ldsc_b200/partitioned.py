@@ -18,6 +18,7 @@ from typing import List, Optional, Sequence
 import numpy as np
 
 from . import _lib as L
+from .api import LdscError
 from .io import rust_f64
 
 
@@ -56,22 +57,30 @@ def default_chisq_max(chi2: np.ndarray, n: np.ndarray) -> float:
     return max(0.001 * max_n, 80.0)
 
 
-def _call(ctx, chi2, n, ref_l2, w_l2, m_vec, n_blocks, fixed, chisq_max) -> List[PartitionedFit]:
-    T, m = chi2.shape
-    K = ref_l2.shape[1]
+def _call(ctx, chi2, n, ref_l2, w_l2, m_vec, n_blocks, fixed, chisq_max, device=None) -> List[PartitionedFit]:
+    """One ldsc_h2_partitioned call.  Host arrays, or with device = (T, m, K,
+    per_snp, ref_ld) the first four arguments are device pointers (ints)."""
+    if device is None:
+        T, m = chi2.shape
+        K = ref_l2.shape[1]
+        per_snp = n.ndim == 2
+        ptrs = (chi2.ctypes.data, n.ctypes.data, ref_l2.ctypes.data, w_l2.ctypes.data)
+        ref_ld = m
+    else:
+        T, m, K, per_snp, ref_ld = device
+        ptrs = (chi2, n, ref_l2, w_l2)
     P = K + (0 if fixed is not None else 1)
-    per_snp = n.ndim == 2
     cmax = np.ascontiguousarray(chisq_max, dtype=np.float64)
     est = np.zeros((T, P))
     cov = np.zeros((T, P, P))
     dv = np.zeros((T, n_blocks, P))
     h2a = np.zeros((T, K))
-    args = L.H2PArgs(n_snp=m, n_traits=T, n_annot=K, n_blocks=n_blocks, chi2=chi2.ctypes.data,
-                     n_per_snp=n.ctypes.data if per_snp else None, n_scalar=None if per_snp else n.ctypes.data,
-                     ref_l2=ref_l2.ctypes.data, ref_ld=m, w_l2=w_l2.ctypes.data, m_vec=m_vec.ctypes.data,
+    args = L.H2PArgs(n_snp=m, n_traits=T, n_annot=K, n_blocks=n_blocks, chi2=ptrs[0],
+                     n_per_snp=ptrs[1] if per_snp else None, n_scalar=None if per_snp else ptrs[1],
+                     ref_l2=ptrs[2], ref_ld=ref_ld, w_l2=ptrs[3], m_vec=m_vec.ctypes.data,
                      fixed_intercept=int(fixed is not None), intercept=float(fixed or 0.0),
-                     chisq_max=cmax.ctypes.data, device_pointers=0, est=est.ctypes.data, cov=cov.ctypes.data,
-                     delete_values=dv.ctypes.data, h2_annot=h2a.ctypes.data)
+                     chisq_max=cmax.ctypes.data, device_pointers=int(device is not None), est=est.ctypes.data,
+                     cov=cov.ctypes.data, delete_values=dv.ctypes.data, h2_annot=h2a.ctypes.data)
     out = (L.H2PResult * T)()
     ctx.check(ctx.lib.ldsc_h2_partitioned(ctx.h, C.byref(args), C.cast(out, C.c_void_p)))
     fits = []
@@ -133,6 +142,28 @@ def h2_partitioned(ctx, chi2, n, ref_l2, w_l2, m_vec, n_blocks: int = 200, inter
                   cmax[t:t + 1])
         fits[t] = f[0]
     return fits[0] if single else fits
+
+
+def h2_partitioned_device(ctx, chi2, n, ref_l2, w_l2, m_vec, chisq_max, n_blocks: int = 200,
+                          intercept_h2: Optional[float] = None, no_intercept: bool = False) -> List[PartitionedFit]:
+    """Partitioned h2 on device-resident CUDA tensors: chi2 (T, n_snp), n
+    (T,) scalar sample sizes or (T, n_snp), ref_l2 (K, n_snp) row-major (=
+    n_snp x K column-major, as the l2 run's device output), w_l2 (n_snp,),
+    all float64.  chisq_max: T cut-offs (host); the caller applies any
+    missing-N filter."""
+    T, m = int(chi2.shape[0]), int(chi2.shape[1])
+    K = int(ref_l2.shape[0])
+    for t, shape in ((chi2, (T, m)), (ref_l2, (K, m)), (w_l2, (m,))):
+        if tuple(t.shape) != shape or not t.is_contiguous() or not t.is_cuda:
+            raise LdscError(L.LDSC_E_INVALID, "h2_partitioned_device wants contiguous float64 CUDA tensors")
+    per_snp = n.dim() == 2
+    if tuple(n.shape) != ((T, m) if per_snp else (T,)) or not n.is_cuda:
+        raise LdscError(L.LDSC_E_INVALID, "n must be a (T,) or (T, n_snp) float64 CUDA tensor")
+    fixed = intercept_h2 if intercept_h2 is not None else (1.0 if no_intercept else None)
+    m_vec = np.ascontiguousarray(np.atleast_1d(m_vec), dtype=np.float64)
+    cmax = np.broadcast_to(np.asarray(chisq_max, dtype=np.float64), (T,))
+    return _call(ctx, chi2.data_ptr(), n.data_ptr(), ref_l2.data_ptr(), w_l2.data_ptr(), m_vec, n_blocks, fixed,
+                 cmax, device=(T, m, K, per_snp, m))
 
 
 def _rust_exp(v: float, prec: int) -> str:

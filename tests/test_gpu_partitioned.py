@@ -161,3 +161,23 @@ def test_partitioned_too_many_annotations_is_an_error(ctx):
     l2, wld = _annot_ld(m, k, 90)
     with pytest.raises(LdscError):
         h2_partitioned(ctx, np.ones(m), 1e4, l2, wld, np.full(k, 10.0), 20)
+
+
+def test_partitioned_device_tensors_equal_host_arrays(ctx):
+    """Device pointers (the l2 run's (K, n_snp) output layout) give the same
+    fit as host arrays: the same kernels on the same values."""
+    import torch
+    from ldsc_b200.partitioned import default_chisq_max, h2_partitioned, h2_partitioned_device
+    m, k = 20_000, 4
+    l2, wld = _annot_ld(m, k, 95)
+    m_vec = np.array([2e4, 1e4, 5e3, 8e3])
+    chi2, n = _traits(l2, m_vec, 3, 96)
+    host = h2_partitioned(ctx, chi2, n, l2, wld, m_vec, 200)
+    cmax = [default_chisq_max(chi2[t], n[t]) for t in range(3)]
+    dev = h2_partitioned_device(ctx, torch.from_numpy(chi2).cuda(), torch.from_numpy(n).cuda(),
+                                torch.from_numpy(np.ascontiguousarray(l2.T)).cuda(), torch.from_numpy(wld).cuda(),
+                                m_vec, cmax, 200)
+    for a, b in zip(host, dev):
+        np.testing.assert_array_equal(a.est, b.est)
+        np.testing.assert_array_equal(a.cov, b.cov)
+        assert a.h2_total == b.h2_total and a.n_obs == b.n_obs
