@@ -129,3 +129,72 @@ def test_synth_panel_statistics():
     # drawing a SNP range on its own gives the same rows
     part = synth.bed_body(spec, 150, 260)
     assert np.array_equal(part, body[150:260])
+
+
+# ---- struct layouts: header vs the ctypes mirror vs the Rust binding ----
+
+_STRUCTS = {"ldsc_progress": "Progress", "ldsc_perf": "Perf", "ldsc_l2_args": "L2Args",
+            "ldsc_synth_spec": "SynthSpec", "ldsc_h2_args": "H2Args", "ldsc_h2_result": "H2Result",
+            "ldsc_h2p_args": "H2PArgs", "ldsc_h2p_result": "H2PResult", "ldsc_rg_args": "RgArgs",
+            "ldsc_rg_result": "RgResult", "ldsc_job": "Job", "ldsc_job_result": "JobResult",
+            "ldsc_server_stats": "ServerStats"}
+_RUST = {"LdscProgress": "ldsc_progress", "LdscPerf": "ldsc_perf", "LdscL2Args": "ldsc_l2_args",
+         "LdscH2Args": "ldsc_h2_args", "LdscH2Result": "ldsc_h2_result", "LdscH2pArgs": "ldsc_h2p_args",
+         "LdscH2pResult": "ldsc_h2p_result", "LdscRgArgs": "ldsc_rg_args", "LdscRgResult": "ldsc_rg_result"}
+
+
+def header_structs():
+    """{typedef name: [field names in order]} from include/ldsc_b200.h."""
+    text = open(os.path.join(ROOT, "include", "ldsc_b200.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    out = {}
+    for body, name in re.findall(r"typedef struct\s*\{(.*?)\}\s*(\w+)\s*;", text, flags=re.S):
+        fields = []
+        for decl in body.split(";"):
+            decl = decl.strip()
+            if not decl:
+                continue
+            for piece in decl.split(","):
+                fields.append(re.findall(r"[A-Za-z_]\w*", piece)[-1])
+        out[name] = fields
+    return out
+
+
+def test_ctypes_mirror_matches_the_header_layout(tmp_path):
+    """offsetof / sizeof of every mirrored struct, from gcc on the header,
+    against the ctypes classes the Python binding passes."""
+    import ctypes
+    import subprocess
+    from ldsc_b200 import _lib
+    hs = header_structs()
+    assert set(_STRUCTS) <= set(hs)
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "ldsc_b200.h"', "int main(void) {"]
+    for cname in _STRUCTS:
+        lines.append(f'printf("{cname} sizeof %zu\\n", sizeof({cname}));')
+        for f in hs[cname]:
+            lines.append(f'printf("{cname} {f} %zu\\n", offsetof({cname}, {f}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), "-o", str(exe), str(src)], check=True)
+    got = {}
+    for line in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.splitlines():
+        s, f, v = line.split()
+        got[(s, f)] = int(v)
+    for cname, pyname in _STRUCTS.items():
+        cls = getattr(_lib, pyname)
+        assert [f for f, _ in cls._fields_] == hs[cname], cname
+        assert ctypes.sizeof(cls) == got[(cname, "sizeof")], cname
+        for f, _ in cls._fields_:
+            assert getattr(cls, f).offset == got[(cname, f)], (cname, f)
+
+
+def test_rust_binding_fields_match_the_header():
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    hs = header_structs()
+    found = dict(re.findall(r"pub struct (Ldsc\w+)\s*\{(.*?)\}", text, flags=re.S))
+    for rname, cname in _RUST.items():
+        assert rname in found, rname
+        fields = re.findall(r"pub (\w+)\s*:", found[rname])
+        assert fields == hs[cname], (rname, fields, hs[cname])
