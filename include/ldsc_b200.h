@@ -359,7 +359,7 @@ int ldsc_h2_partitioned(ldsc_ctx *ctx, const ldsc_h2p_args *args, ldsc_h2p_resul
  * CUDA graphs.  A job's result does not depend on what else runs. */
 typedef struct ldsc_server ldsc_server;
 
-enum { LDSC_JOB_L2 = 0, LDSC_JOB_H2 = 1, LDSC_JOB_RG = 2 };
+enum { LDSC_JOB_L2 = 0, LDSC_JOB_H2 = 1, LDSC_JOB_RG = 2, LDSC_JOB_H2P = 3 };
 
 typedef struct {
     int32_t kind;                 /* LDSC_JOB_* */
@@ -373,6 +373,9 @@ typedef struct {
     ldsc_rg_args rg;              /* RG */
     ldsc_rg_result *rg_out;       /* RG: n_pairs results */
     uint64_t device_bytes;        /* workspace the job needs; 0 = estimated by the server */
+    ldsc_h2p_args h2p;            /* H2P: partitioned h2 (its est / cov / delete_values / h2_annot
+                                     outputs are written when the job completes) */
+    ldsc_h2p_result *h2p_out;     /* H2P: n_traits results */
 } ldsc_job;
 
 typedef struct {

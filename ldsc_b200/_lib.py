@@ -114,13 +114,14 @@ class RgResult(C.Structure):
                                           "h2_1_se", "h2_2", "h2_2_se", "mean_z1z2")]
 
 
-JOB_L2, JOB_H2, JOB_RG = 0, 1, 2
+JOB_L2, JOB_H2, JOB_RG, JOB_H2P = 0, 1, 2, 3
 
 
 class Job(C.Structure):
     _fields_ = [("kind", C.c_int32), ("panel", C.c_void_p), ("l2", L2Args), ("l2_out", C.c_void_p),
                 ("maf_out", C.c_void_p), ("h2", H2Args), ("h2_out", C.c_void_p), ("rg", RgArgs),
-                ("rg_out", C.c_void_p), ("device_bytes", C.c_uint64)]
+                ("rg_out", C.c_void_p), ("device_bytes", C.c_uint64), ("h2p", H2PArgs),
+                ("h2p_out", C.c_void_p)]
 
 
 class JobResult(C.Structure):

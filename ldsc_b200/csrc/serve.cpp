@@ -47,6 +47,16 @@ double ms_between(Clock::time_point a, Clock::time_point b) {
 }
 
 uint64_t regression_bytes(const ldsc_job& j) {
+    if (j.kind == LDSC_JOB_H2P) {
+        // block Grams, totals, solves, results, block starts, the summed LD score
+        const ldsc_h2p_args& a = j.h2p;
+        const uint64_t T = a.n_traits, n = a.n_snp, nb = a.n_blocks, K = a.n_annot;
+        const uint64_t P = K + (a.fixed_intercept ? 0 : 1), Q = P + 1;
+        uint64_t b = 8 * T * (nb * Q * Q + Q * Q + (nb + 1) * P + P * (1 + P + nb) + K + 7 + 3 * nb) +
+                     4 * T * (2 * (nb + 1) + (n + 4095) / 4096) + 8 * n + 4096 + 256 * T;
+        if (!a.device_pointers) b += 8 * T * n * (a.n_per_snp ? 2 : 1) + 8 * n * (K + 1);
+        return b;
+    }
     if (j.kind == LDSC_JOB_H2) {
         const ldsc_h2_args& a = j.h2;
         const uint64_t T = a.n_traits, n = a.n_snp, nb = a.n_blocks < n ? a.n_blocks : n;
@@ -121,6 +131,8 @@ struct ldsc_server {
             rc = ldsc_h2_batch(sl.ctx, &j.h2, j.h2_out);
         else if (j.kind == LDSC_JOB_RG)
             rc = ldsc_rg_batch(sl.ctx, &j.rg, j.rg_out);
+        else if (j.kind == LDSC_JOB_H2P)
+            rc = ldsc_h2_partitioned(sl.ctx, &j.h2p, j.h2p_out);
         res.status = rc;
         res.slot = (uint32_t)i;
         if (rc != LDSC_OK) ldsc_last_error(sl.ctx, res.error, sizeof res.error);
@@ -205,10 +217,13 @@ int ldsc_server_create(int device, uint32_t n_slots, uint64_t device_budget, lds
 
 int ldsc_server_submit(ldsc_server* srv, const ldsc_job* job, uint64_t* ticket) {
     if (!srv || !job || !ticket) return LDSC_E_INVALID;
-    if (job->kind != LDSC_JOB_L2 && job->kind != LDSC_JOB_H2 && job->kind != LDSC_JOB_RG) return LDSC_E_INVALID;
+    if (job->kind != LDSC_JOB_L2 && job->kind != LDSC_JOB_H2 && job->kind != LDSC_JOB_RG &&
+        job->kind != LDSC_JOB_H2P)
+        return LDSC_E_INVALID;
     if (job->kind == LDSC_JOB_L2 && (!job->panel || (job->l2.n_snp && !job->l2_out))) return LDSC_E_INVALID;
     if (job->kind == LDSC_JOB_H2 && !job->h2_out) return LDSC_E_INVALID;
     if (job->kind == LDSC_JOB_RG && !job->rg_out) return LDSC_E_INVALID;
+    if (job->kind == LDSC_JOB_H2P && !job->h2p_out) return LDSC_E_INVALID;
     JobRec* r = new JobRec();
     r->job = *job;
     std::memset(&r->res, 0, sizeof r->res);

@@ -130,6 +130,30 @@ class Server:
         job = L.Job(kind=L.JOB_RG, rg=args, rg_out=C.cast(out, C.c_void_p))
         return self._submit(job, dict(keep=(k1, k2, kn1, kn2, kl, kw), out=out, kind="rg"))
 
+    def submit_h2_partitioned(self, chi2, n, ref_l2, w_l2, m_vec, chisq_max, n_blocks: int = 200,
+                              intercept: Optional[float] = None) -> int:
+        """Partitioned h2 for T traits on CUDA tensors: chi2 (T, n_snp), n
+        (T,) sample sizes, ref_l2 (K, n_snp) (the l2 run's device layout),
+        w_l2 (n_snp,); m_vec K values, chisq_max T cut-offs (host).  wait()
+        returns a list of PartitionedFit."""
+        T, m = int(chi2.shape[0]), int(chi2.shape[1])
+        K = int(ref_l2.shape[0])
+        fixed = intercept is not None
+        P = K + (0 if fixed else 1)
+        mv = np.ascontiguousarray(m_vec, dtype=np.float64)
+        cm = np.ascontiguousarray(np.broadcast_to(np.asarray(chisq_max, float), (T,)))
+        est, cov = np.zeros((T, P)), np.zeros((T, P, P))
+        dv, h2a = np.zeros((T, n_blocks, P)), np.zeros((T, K))
+        args = L.H2PArgs(n_snp=m, n_traits=T, n_annot=K, n_blocks=n_blocks, chi2=chi2.data_ptr(), n_per_snp=None,
+                         n_scalar=n.data_ptr(), ref_l2=ref_l2.data_ptr(), ref_ld=m, w_l2=w_l2.data_ptr(),
+                         m_vec=mv.ctypes.data, fixed_intercept=int(fixed), intercept=float(intercept or 0.0),
+                         chisq_max=cm.ctypes.data, device_pointers=1, est=est.ctypes.data, cov=cov.ctypes.data,
+                         delete_values=dv.ctypes.data, h2_annot=h2a.ctypes.data)
+        out = (L.H2PResult * T)()
+        job = L.Job(kind=L.JOB_H2P, h2p=args, h2p_out=C.cast(out, C.c_void_p))
+        return self._submit(job, dict(keep=(chi2, n, ref_l2, w_l2, mv, cm), out=out, kind="h2p",
+                                      arrays=(est, cov, dv, h2a, mv)))
+
     def wait(self, ticket: int):
         """Block until the job ends.  Returns (result, JobTiming) where
         result is (l2, maf, L2Perf) for l2 jobs and a structured array for
@@ -144,6 +168,18 @@ class Server:
         kind = keep["kind"]
         if kind == "l2":
             return (keep["l2"], keep["maf"], _perf(res.perf)), timing
+        if kind == "h2p":
+            from .partitioned import PartitionedFit
+            est, cov, dv, h2a, mv = keep["arrays"]
+            fits = []
+            for t, r in enumerate(keep["out"]):
+                nb = int(r.n_blocks)
+                fits.append(PartitionedFit(est=est[t], cov=cov[t], delete_values=dv[t, :nb], m_vec=mv.copy(),
+                                           n_mean=r.n_mean, h2_annot=h2a[t], h2_total=r.h2_total,
+                                           h2_total_se=r.h2_total_se, intercept=r.intercept,
+                                           intercept_se=r.intercept_se, mean_chi2=r.mean_chi2,
+                                           n_obs=int(r.n_obs), n_blocks=nb))
+            return fits, timing
         struct = L.H2Result if kind == "h2" else L.RgResult
         names = [f for f, _ in struct._fields_]
         out = np.array([tuple(getattr(r, f) for f in names) for r in keep["out"]],

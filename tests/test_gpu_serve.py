@@ -48,8 +48,14 @@ def test_jobs_alone_equal_jobs_in_the_mix(ctx, resident):
     ld = l2_all[:, 0].copy()
     chi2, n_t, _ = synth.gwas_traits(ld, 1e6, 24, seed=6)
     z1, z2, n1, n2, _ = synth.gwas_pairs(ld, 1e6, 6, seed=7)
+    # K = 10 LD scores for partitioned h2, in the l2 run's (K, n_snp) device layout
+    l2k, _, _ = run_l2(ctx, snps, panel, wm, 200, annot=annot, snp_level_masking=True, precision="int8",
+                       yes_really=True)
+    m_vec = annot.sum(axis=0)
+    from ldsc_b200.partitioned import default_chisq_max, h2_partitioned
+    cmax = np.array([default_chisq_max(chi2[t], n_t[t]) for t in range(len(n_t))])
     dev = {k: torch.from_numpy(np.ascontiguousarray(v, dtype=np.float64)).cuda()
-           for k, v in dict(chi2=chi2, n=n_t, ld=ld, z1=z1, z2=z2, n1=n1, n2=n2).items()}
+           for k, v in dict(chi2=chi2, n=n_t, ld=ld, z1=z1, z2=z2, n1=n1, n2=n2, l2k=l2k.T).items()}
     jobs = [
         ("l2", dict(b=0, e=9000, K=1, sk=None, prec="int8")),
         ("l2", dict(b=5000, e=35000, K=10, sk=None, prec="int8")),
@@ -60,6 +66,8 @@ def test_jobs_alone_equal_jobs_in_the_mix(ctx, resident):
         ("h2", dict(t0=16, t1=24)),
         ("l2", dict(b=12000, e=52000, K=1, sk=None, prec="int8")),
         ("l2", dict(b=100, e=2100, K=10, sk=None, prec="int8")),
+        ("h2p", dict(t0=0, t1=4)),
+        ("h2p", dict(t0=4, t1=12)),
     ]
 
     def alone(kind, p):
@@ -70,6 +78,8 @@ def test_jobs_alone_equal_jobs_in_the_mix(ctx, resident):
                           snp_level_masking=True, yes_really=True)[0]
         if kind == "h2":
             return h2_batch(ctx, chi2[p["t0"]:p["t1"]], n_t[p["t0"]:p["t1"]], ld, ld, 1e6, 200)
+        if kind == "h2p":
+            return h2_partitioned(ctx, chi2[p["t0"]:p["t1"]], n_t[p["t0"]:p["t1"]], l2k, ld, m_vec, 200)
         return rg_batch(ctx, z1[p["p0"]:p["p1"]], z2[p["p0"]:p["p1"]], n1[p["p0"]:p["p1"]],
                         n2[p["p0"]:p["p1"]], ld, ld, 1e6, 200)
 
@@ -91,6 +101,9 @@ def test_jobs_alone_equal_jobs_in_the_mix(ctx, resident):
                 elif kind == "h2":
                     t = srv.submit_h2(dev["chi2"][p["t0"]:p["t1"]], dev["n"][p["t0"]:p["t1"]], dev["ld"],
                                       dev["ld"], 1e6, 200)
+                elif kind == "h2p":
+                    t = srv.submit_h2_partitioned(dev["chi2"][p["t0"]:p["t1"]], dev["n"][p["t0"]:p["t1"]],
+                                                  dev["l2k"], dev["ld"], m_vec, cmax[p["t0"]:p["t1"]], 200)
                 else:
                     t = srv.submit_rg(dev["z1"][p["p0"]:p["p1"]], dev["z2"][p["p0"]:p["p1"]],
                                       dev["n1"][p["p0"]:p["p1"]], dev["n2"][p["p0"]:p["p1"]], dev["ld"],
@@ -103,6 +116,11 @@ def test_jobs_alone_equal_jobs_in_the_mix(ctx, resident):
             want = ref[i % len(jobs)]
             if kind == "l2":
                 assert relerr(got[0], want) < MIX_TOL, (i, jobs[i % len(jobs)])
+            elif kind == "h2p":
+                for a, b in zip(got, want):
+                    np.testing.assert_array_equal(a.est, b.est)
+                    np.testing.assert_array_equal(a.cov, b.cov)
+                    assert a.h2_total == b.h2_total
             else:
                 for f in got.dtype.names:
                     np.testing.assert_array_equal(got[f], want[f])
