@@ -8,9 +8,8 @@
 //
 // The design is augmented with y as its last column, Z = [x_1..x_K, 1, y],
 // so one symmetric Gram per jackknife block, sum_i w_i z_i z_i', holds X'X,
-// X'y and y'y.  Per-SNP weights enter squared-root-free: the reference scales
-// rows by sqrt(w_i) / sum_j sqrt(w_j), whose square's global factor cancels
-// in every solve.  SNPs dropped by the chi2 cut contribute nothing and the
+// X'y and y'y.  Rows are scaled by sqrt(w_i) as in the reference, which also
+// divides by sum_j sqrt(w_j): that global factor cancels in every solve.  SNPs dropped by the chi2 cut contribute nothing and the
 // jackknife blocks are the reference's blocks over the kept SNPs (block starts
 // mapped back to SNP indices).  Block partial sums are combined in block
 // order, so results do not depend on scheduling.
@@ -25,9 +24,7 @@ namespace ldsc {
 namespace {
 
 constexpr int NT = 256;
-constexpr int TILE = 64;       // Gram output tile (64 x 64, 4 x 4 per thread)
-constexpr int ROWS = 32;       // SNPs staged per step
-constexpr int SROW = TILE + 2; // staged row stride in doubles (16-byte aligned rows)
+constexpr int ROWS = 32;       // SNPs staged per step of the Gram
 
 __device__ __forceinline__ double part_n(const PartJob& jb, uint64_t i) { return jb.nv ? jb.nv[i] : jb.ns; }
 __device__ __forceinline__ bool part_kept(const PartJob& jb, uint64_t i) { return jb.chi2[i] < jb.mask_max; }
@@ -103,33 +100,43 @@ __global__ void k_p_aggregate(const PartJob* __restrict__ jobs, const double* __
     o.hsq = m_tot * (o.mean_chi2 - o.agg_int) / (s1 / nobs);
 }
 
-// Gram of the augmented weighted design over one jackknife block, one 64 x 64
-// tile pair (ti <= tj) per CTA.  Columns: K scaled LD scores N_i l2_ij / nbar,
-// the intercept column (free intercept only), y = chi2 - fixed intercept.
-__global__ void __launch_bounds__(NT) k_p_gram(const PartJob* __restrict__ jobs, const PartState* __restrict__ st,
+// Gram of the augmented weighted design over one jackknife block: rows
+// u_i = sqrt(w_i) z_i with z_i = [N_i l2_i1 / nbar, ..., N_i l2_iK / nbar, 1
+// (free intercept only), chi2_i - fixed intercept] (the reference's weighted
+// design, src/h2.rs:60-80, without the 1/sum(sqrt(w)) factor that cancels),
+// G = sum_i u_i u_i'.  The upper triangle is cut into 16 x 16 micro-tiles,
+// 16 per CTA (4 x 4 outputs per thread); a CTA stages 32 rows of all
+// round_up(q, 16) columns at a time.
+constexpr int MT = 16;                                  // micro-tile edge
+__host__ __device__ inline int part_qp(int q) { return (q + MT - 1) / MT * MT; }
+__host__ __device__ inline int part_ustride(int q) { return part_qp(q) + 2; }  // doubles per staged row
+
+__global__ void __launch_bounds__(NT, 3) k_p_gram(const PartJob* __restrict__ jobs, const PartState* __restrict__ st,
                                               const double* __restrict__ l2, uint64_t ld, int k,
                                               const double* __restrict__ xtot, const double* __restrict__ wld,
                                               double m_tot, int nb, int q, double* __restrict__ gram) {
-    __shared__ __align__(16) double As[ROWS * SROW];
-    __shared__ __align__(16) double Bs[ROWS * SROW];
+    extern __shared__ __align__(16) double U[];  // ROWS x ustride
     __shared__ double rw[ROWS], rs[ROWS], ry[ROWS];
     __shared__ int rk[ROWS];
     const int b = blockIdx.x, j = blockIdx.z;
-    // tile pair index -> (ti, tj), ti <= tj, row-major over the upper triangle
-    const int nt = (q + TILE - 1) / TILE;
-    int ti = 0, rem = blockIdx.y;
-    while (rem >= nt - ti) {
-        rem -= nt - ti;
-        ti++;
+    const int qp = part_qp(q), us = part_ustride(q), nm = qp / MT;
+    const int count = nm * (nm + 1) / 2;
+    // this thread's micro-tile (row-major over the upper triangle) and 4 x 4 block in it
+    const int g = blockIdx.y * (NT / MT) + threadIdx.x / MT;
+    const bool active = g < count;
+    int mi = 0, rem = active ? g : 0;
+    while (rem >= nm - mi) {
+        rem -= nm - mi;
+        mi++;
     }
-    const int tj = ti + rem;
+    const int mj = mi + rem;
+    const int r0c = mi * MT + ((threadIdx.x % MT) / 4) * 4, c0c = mj * MT + (threadIdx.x % 4) * 4;
     const PartJob jb = jobs[j];
     const PartState s = st[j];
     const bool free_int = !jb.fixed;
     const double yoff = jb.fixed ? jb.fixed_int : 0.0;
     const double hsq = fmin(fmax(s.hsq, 0.0), 1.0);
     const uint64_t lo = (uint64_t)jb.seps[b], hi = (uint64_t)jb.seps[b + 1];
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
     double acc[4][4];
 #pragma unroll
     for (int u = 0; u < 4; u++)
@@ -139,66 +146,64 @@ __global__ void __launch_bounds__(NT) k_p_gram(const PartJob* __restrict__ jobs,
     for (uint64_t r0 = lo; r0 < hi; r0 += ROWS) {
         if (threadIdx.x < ROWS) {
             const uint64_t i = r0 + threadIdx.x;
-            double w = 0.0, sc = 0.0, y = 0.0;
+            double sw = 0.0, sc = 0.0, y = 0.0;
             const bool kept = i < hi && part_kept(jb, i);
             if (kept) {
                 // ldsc_weights (src/h2.rs:185-206) on x_tot with M = sum(M_k)
                 const double nn = part_n(jb, i);
                 const double c = hsq * nn / m_tot;
                 const double t = s.agg_int + c * fmax(xtot[i], 1.0);
-                w = 1.0 / (2.0 * t * t) / fmax(wld[i], 1.0);
+                sw = sqrt(1.0 / (2.0 * t * t) / fmax(wld[i], 1.0));
                 sc = nn / s.nbar;
                 y = jb.chi2[i] - yoff;
             }
-            rw[threadIdx.x] = w;
+            rw[threadIdx.x] = sw;
             rs[threadIdx.x] = sc;
             ry[threadIdx.x] = y;
             rk[threadIdx.x] = kept;
         }
         __syncthreads();
         // stage: lane = row (32 consecutive SNPs of one column per warp)
-        for (int e = threadIdx.x; e < 2 * ROWS * TILE; e += NT) {
-            const int side = e / (ROWS * TILE);
-            const int c = (e % (ROWS * TILE)) / ROWS, r = e % ROWS;
-            const int g = (side ? tj : ti) * TILE + c;
+        for (int e = threadIdx.x; e < ROWS * qp; e += NT) {
+            const int c = e / ROWS, r = e % ROWS;
             const uint64_t i = r0 + r;
             double z = 0.0;
             if (rk[r]) {
-                if (g < k)
-                    z = l2[(size_t)g * ld + i] * rs[r];
-                else if (g == k && free_int)
+                if (c < k)
+                    z = l2[(size_t)c * ld + i] * rs[r];
+                else if (c == k && free_int)
                     z = 1.0;
-                else if (g == q - 1)
+                else if (c == q - 1)
                     z = ry[r];
             }
-            if (side)
-                Bs[r * SROW + c] = z;
-            else
-                As[r * SROW + c] = z * rw[r];
+            U[r * us + c] = z * rw[r];
         }
         __syncthreads();
-        const int nr = (int)(hi - r0 < (uint64_t)ROWS ? hi - r0 : (uint64_t)ROWS);
-        for (int r = 0; r < nr; r++) {
-            const double2 a01 = *reinterpret_cast<const double2*>(&As[r * SROW + ty * 4]);
-            const double2 a23 = *reinterpret_cast<const double2*>(&As[r * SROW + ty * 4 + 2]);
-            const double2 b01 = *reinterpret_cast<const double2*>(&Bs[r * SROW + tx * 4]);
-            const double2 b23 = *reinterpret_cast<const double2*>(&Bs[r * SROW + tx * 4 + 2]);
-            const double av[4] = {a01.x, a01.y, a23.x, a23.y};
-            const double bv[4] = {b01.x, b01.y, b23.x, b23.y};
+        if (active) {
+            const int nr = (int)(hi - r0 < (uint64_t)ROWS ? hi - r0 : (uint64_t)ROWS);
+            for (int r = 0; r < nr; r++) {
+                const double2 a01 = *reinterpret_cast<const double2*>(&U[r * us + r0c]);
+                const double2 a23 = *reinterpret_cast<const double2*>(&U[r * us + r0c + 2]);
+                const double2 b01 = *reinterpret_cast<const double2*>(&U[r * us + c0c]);
+                const double2 b23 = *reinterpret_cast<const double2*>(&U[r * us + c0c + 2]);
+                const double av[4] = {a01.x, a01.y, a23.x, a23.y};
+                const double bv[4] = {b01.x, b01.y, b23.x, b23.y};
 #pragma unroll
-            for (int u = 0; u < 4; u++)
+                for (int u = 0; u < 4; u++)
 #pragma unroll
-                for (int v = 0; v < 4; v++) acc[u][v] = fma(av[u], bv[v], acc[u][v]);
+                    for (int v = 0; v < 4; v++) acc[u][v] = fma(av[u], bv[v], acc[u][v]);
+            }
         }
         __syncthreads();
     }
+    if (!active) return;
     // write row <= col and its mirror, so the stored matrix is exactly symmetric
     double* G = gram + ((size_t)j * nb + b) * (size_t)q * q;
 #pragma unroll
     for (int u = 0; u < 4; u++)
 #pragma unroll
         for (int v = 0; v < 4; v++) {
-            const int rr = ti * TILE + ty * 4 + u, cc = tj * TILE + tx * 4 + v;
+            const int rr = r0c + u, cc = c0c + v;
             if (rr < q && cc < q && rr <= cc) {
                 G[(size_t)rr * q + cc] = acc[u][v];
                 G[(size_t)cc * q + rr] = acc[u][v];
@@ -382,7 +387,8 @@ cudaError_t launch_partitioned(const PartJob* jobs, PartState* st, const double*
                                bool want_xtot, double* part, double* gram, double* tot, double* sol, double* res,
                                int njobs, cudaStream_t s) {
     const int p = part_params(k, fixed), q = p + 1;
-    const int nt = (q + TILE - 1) / TILE;
+    const int nm = part_qp(q) / MT, gram_ctas = (nm * (nm + 1) / 2 + NT / MT - 1) / (NT / MT);
+    const size_t gram_smem = (size_t)ROWS * part_ustride(q) * sizeof(double);
     const size_t solve_smem = (size_t)p * (p + 1) * sizeof(double);
     if (solve_smem > (size_t)PART_SOLVE_SMEM) return cudaErrorInvalidValue;
     if (want_xtot) {
@@ -391,7 +397,11 @@ cudaError_t launch_partitioned(const PartJob* jobs, PartState* st, const double*
     }
     k_p_sums<<<dim3(nb, njobs), NT, 0, s>>>(jobs, xtot, nb, part);
     k_p_aggregate<<<(njobs + 127) / 128, 128, 0, s>>>(jobs, part, nb, m_tot, st, njobs);
-    k_p_gram<<<dim3(nb, nt * (nt + 1) / 2, njobs), NT, 0, s>>>(jobs, st, l2, ld, k, xtot, wld, m_tot, nb, q, gram);
+    if (gram_smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k_p_gram, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gram_smem);
+        if (e != cudaSuccess) return e;
+    }
+    k_p_gram<<<dim3(nb, gram_ctas, njobs), NT, gram_smem, s>>>(jobs, st, l2, ld, k, xtot, wld, m_tot, nb, q, gram);
     k_p_total<<<dim3((q * q + NT - 1) / NT, njobs), NT, 0, s>>>(gram, nb, q * q, tot);
     cudaError_t e = cudaFuncSetAttribute(k_p_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve_smem);
     if (e != cudaSuccess) return e;
