@@ -100,24 +100,39 @@ __global__ void k_p_aggregate(const PartJob* __restrict__ jobs, const double* __
     o.hsq = m_tot * (o.mean_chi2 - o.agg_int) / (s1 / nobs);
 }
 
-// Gram of the augmented weighted design over one jackknife block: rows
-// u_i = sqrt(w_i) z_i with z_i = [N_i l2_i1 / nbar, ..., N_i l2_iK / nbar, 1
-// (free intercept only), chi2_i - fixed intercept] (the reference's weighted
-// design, src/h2.rs:60-80, without the 1/sum(sqrt(w)) factor that cancels),
-// G = sum_i u_i u_i'.  The upper triangle is cut into 16 x 16 micro-tiles,
-// 16 per CTA (4 x 4 outputs per thread); a CTA stages 32 rows of all
-// round_up(q, 16) columns at a time.
+// Gram of the augmented weighted design over one jackknife block:
+// G = sum_i w_i z_i z_i' with z_i = [N_i l2_i1 / nbar, ..., N_i l2_iK / nbar,
+// 1 (free intercept only), chi2_i - fixed intercept] and w_i the reference's
+// weight (its weighted design scales rows by sqrt(w_i) / sum_j sqrt(w_j),
+// src/h2.rs:60-80; the global factor cancels in every solve).  The upper
+// triangle is cut into 16 x 16 micro-tiles, 16 per CTA (4 x 4 outputs per
+// thread).  Rows are staged 32 at a time, double-buffered: the raw LD scores
+// of the next 32 rows arrive by cp.async while the current ones are
+// multiplied.  A row is staged as v_i = z_i / s_i with s_i = N_i / nbar (the
+// LD-score columns are then the raw values, the intercept 1 / s_i, the chi2
+// column y_i / s_i) and enters as (w_i s_i^2) v_i v_i'; a row with N_i = 0
+// is staged as z_i with factor w_i.
 constexpr int MT = 16;                                  // micro-tile edge
 __host__ __device__ inline int part_qp(int q) { return (q + MT - 1) / MT * MT; }
 __host__ __device__ inline int part_ustride(int q) { return part_qp(q) + 2; }  // doubles per staged row
+__host__ __device__ inline size_t part_gram_smem(int q) { return 2 * (size_t)ROWS * part_ustride(q) * sizeof(double); }
+
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(smem)),
+                 "l"(gmem)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 __global__ void __launch_bounds__(NT, 3) k_p_gram(const PartJob* __restrict__ jobs, const PartState* __restrict__ st,
-                                              const double* __restrict__ l2, uint64_t ld, int k,
-                                              const double* __restrict__ xtot, const double* __restrict__ wld,
-                                              double m_tot, int nb, int q, double* __restrict__ gram) {
-    extern __shared__ __align__(16) double U[];  // ROWS x ustride
-    __shared__ double rw[ROWS], rs[ROWS], ry[ROWS];
-    __shared__ int rk[ROWS];
+                                                 const double* __restrict__ l2, uint64_t ld, int k,
+                                                 const double* __restrict__ xtot, const double* __restrict__ wld,
+                                                 double m_tot, int nb, int q, double* __restrict__ gram) {
+    extern __shared__ __align__(16) double U[];  // 2 x ROWS x ustride
+    __shared__ double rf[2][ROWS];               // row factors w_i s_i^2 (0: row not kept)
+    __shared__ double rsc[2][ROWS];              // s_i, or 0 when the row is staged as z_i
     const int b = blockIdx.x, j = blockIdx.z;
     const int qp = part_qp(q), us = part_ustride(q), nm = qp / MT;
     const int count = nm * (nm + 1) / 2;
@@ -137,56 +152,91 @@ __global__ void __launch_bounds__(NT, 3) k_p_gram(const PartJob* __restrict__ jo
     const double yoff = jb.fixed ? jb.fixed_int : 0.0;
     const double hsq = fmin(fmax(s.hsq, 0.0), 1.0);
     const uint64_t lo = (uint64_t)jb.seps[b], hi = (uint64_t)jb.seps[b + 1];
+    const int nchunks = (int)((hi - lo + ROWS - 1) / ROWS);
+    // padding columns [q, qp) stay zero in both buffers
+    for (int e = threadIdx.x; e < 2 * ROWS * (qp - q); e += NT) {
+        const int bb = e / (ROWS * (qp - q)), r = (e / (qp - q)) % ROWS, c = q + e % (qp - q);
+        U[(size_t)bb * ROWS * us + r * us + c] = 0.0;
+    }
+    // stage rows [lo + c ROWS, ...) into buffer c & 1: factors and the special
+    // columns by one thread per row, then the LD scores (barrier between)
+    auto stage_meta = [&](int c) {
+        if (threadIdx.x < ROWS) {
+            const int bb = c & 1;
+            const uint64_t i = lo + (uint64_t)c * ROWS + threadIdx.x;
+            double* row = U + (size_t)bb * ROWS * us + threadIdx.x * us;
+            double f = 0.0, sc = 0.0, vi = 0.0, vy = 0.0;
+            if (i < hi && part_kept(jb, i)) {
+                // ldsc_weights (src/h2.rs:185-206) on x_tot with M = sum(M_k)
+                const double nn = part_n(jb, i);
+                const double cc = hsq * nn / m_tot;
+                const double t = s.agg_int + cc * fmax(xtot[i], 1.0);
+                const double w = 1.0 / (2.0 * t * t) / fmax(wld[i], 1.0);
+                sc = nn / s.nbar;
+                const double y = jb.chi2[i] - yoff;
+                if (sc != 0.0) {
+                    f = w * sc * sc;
+                    vi = 1.0 / sc;
+                    vy = y / sc;
+                } else {
+                    f = w;
+                    vi = 1.0;
+                    vy = y;
+                }
+            }
+            if (free_int) row[k] = vi;
+            row[q - 1] = vy;
+            rf[bb][threadIdx.x] = f;
+            rsc[bb][threadIdx.x] = sc;
+        }
+    };
+    auto stage_ld = [&](int c) {
+        const int bb = c & 1;
+        const uint64_t r0 = lo + (uint64_t)c * ROWS;
+        double* buf = U + (size_t)bb * ROWS * us;
+        for (int e = threadIdx.x; e < ROWS * k; e += NT) {
+            const int col = e / ROWS, r = e % ROWS;
+            const uint64_t i = r0 + r;
+            if (rf[bb][r] != 0.0 && rsc[bb][r] != 0.0)
+                cp_async8(buf + r * us + col, l2 + (size_t)col * ld + i);
+            else
+                buf[r * us + col] = 0.0;   // row not kept (or N = 0: its LD-score columns are 0)
+        }
+        cp_async_commit();
+    };
     double acc[4][4];
 #pragma unroll
     for (int u = 0; u < 4; u++)
 #pragma unroll
         for (int v = 0; v < 4; v++) acc[u][v] = 0.0;
-
-    for (uint64_t r0 = lo; r0 < hi; r0 += ROWS) {
-        if (threadIdx.x < ROWS) {
-            const uint64_t i = r0 + threadIdx.x;
-            double sw = 0.0, sc = 0.0, y = 0.0;
-            const bool kept = i < hi && part_kept(jb, i);
-            if (kept) {
-                // ldsc_weights (src/h2.rs:185-206) on x_tot with M = sum(M_k)
-                const double nn = part_n(jb, i);
-                const double c = hsq * nn / m_tot;
-                const double t = s.agg_int + c * fmax(xtot[i], 1.0);
-                sw = sqrt(1.0 / (2.0 * t * t) / fmax(wld[i], 1.0));
-                sc = nn / s.nbar;
-                y = jb.chi2[i] - yoff;
-            }
-            rw[threadIdx.x] = sw;
-            rs[threadIdx.x] = sc;
-            ry[threadIdx.x] = y;
-            rk[threadIdx.x] = kept;
-        }
+    if (nchunks > 0) {
+        stage_meta(0);
         __syncthreads();
-        // stage: lane = row (32 consecutive SNPs of one column per warp)
-        for (int e = threadIdx.x; e < ROWS * qp; e += NT) {
-            const int c = e / ROWS, r = e % ROWS;
-            const uint64_t i = r0 + r;
-            double z = 0.0;
-            if (rk[r]) {
-                if (c < k)
-                    z = l2[(size_t)c * ld + i] * rs[r];
-                else if (c == k && free_int)
-                    z = 1.0;
-                else if (c == q - 1)
-                    z = ry[r];
-            }
-            U[r * us + c] = z * rw[r];
+        stage_ld(0);
+    }
+    for (int c = 0; c < nchunks; c++) {
+        const bool next = c + 1 < nchunks;
+        if (next) stage_meta(c + 1);   // buffer (c + 1) & 1 was released by the previous iteration's barrier
+        __syncthreads();
+        if (next) {
+            stage_ld(c + 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
         }
         __syncthreads();
         if (active) {
+            const int bb = c & 1;
+            const double* buf = U + (size_t)bb * ROWS * us;
+            const uint64_t r0 = lo + (uint64_t)c * ROWS;
             const int nr = (int)(hi - r0 < (uint64_t)ROWS ? hi - r0 : (uint64_t)ROWS);
             for (int r = 0; r < nr; r++) {
-                const double2 a01 = *reinterpret_cast<const double2*>(&U[r * us + r0c]);
-                const double2 a23 = *reinterpret_cast<const double2*>(&U[r * us + r0c + 2]);
-                const double2 b01 = *reinterpret_cast<const double2*>(&U[r * us + c0c]);
-                const double2 b23 = *reinterpret_cast<const double2*>(&U[r * us + c0c + 2]);
-                const double av[4] = {a01.x, a01.y, a23.x, a23.y};
+                const double f = rf[bb][r];
+                const double2 a01 = *reinterpret_cast<const double2*>(&buf[r * us + r0c]);
+                const double2 a23 = *reinterpret_cast<const double2*>(&buf[r * us + r0c + 2]);
+                const double2 b01 = *reinterpret_cast<const double2*>(&buf[r * us + c0c]);
+                const double2 b23 = *reinterpret_cast<const double2*>(&buf[r * us + c0c + 2]);
+                const double av[4] = {a01.x * f, a01.y * f, a23.x * f, a23.y * f};
                 const double bv[4] = {b01.x, b01.y, b23.x, b23.y};
 #pragma unroll
                 for (int u = 0; u < 4; u++)
@@ -388,7 +438,7 @@ cudaError_t launch_partitioned(const PartJob* jobs, PartState* st, const double*
                                int njobs, cudaStream_t s) {
     const int p = part_params(k, fixed), q = p + 1;
     const int nm = part_qp(q) / MT, gram_ctas = (nm * (nm + 1) / 2 + NT / MT - 1) / (NT / MT);
-    const size_t gram_smem = (size_t)ROWS * part_ustride(q) * sizeof(double);
+    const size_t gram_smem = part_gram_smem(q);
     const size_t solve_smem = (size_t)p * (p + 1) * sizeof(double);
     if (solve_smem > (size_t)PART_SOLVE_SMEM) return cudaErrorInvalidValue;
     if (want_xtot) {
