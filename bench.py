@@ -298,6 +298,34 @@ def run_partitioned_workload(args, ctx, stream):
     panel.close()
 
 
+def run_partitioned_h2_workload(args, ctx, stream):
+    """Partitioned h2 alone: seeded synthetic K-column LD scores resident in
+    HBM (l2_k = base * Dirichlet fractions, base = 1 + Gamma(2, 15)), traits
+    chi2 = chi2_1 * (1 + base / 60), N = 1e5, 200 blocks; times the whole
+    ldsc_h2_partitioned call on device pointers.  Sizes: --h2p-snps,
+    --h2p-annot, --h2p-traits."""
+    import torch
+    from ldsc_b200.partitioned import default_chisq_max, h2_partitioned_device
+    m, K, T = args.h2p_snps, args.h2p_annot, args.h2p_traits
+    rng = np.random.default_rng(1)
+    base = 1.0 + rng.gamma(2.0, 15.0, m)
+    l2 = np.ascontiguousarray((base[:, None] * rng.dirichlet(np.ones(K), size=m)).T)   # (K, m)
+    chi2 = rng.chisquare(1, (T, m)) * (1.0 + base / 60.0)
+    nn = np.full(T, 1e5)
+    d = dict(chi2=torch.from_numpy(chi2).cuda(), n=torch.from_numpy(nn).cuda(), l2=torch.from_numpy(l2).cuda(),
+             w=torch.from_numpy(base).cuda())
+    cmax = [default_chisq_max(chi2[t], nn[t]) for t in range(T)]
+    m_vec = np.full(K, 1e4)
+    call = lambda: h2_partitioned_device(ctx, d["chi2"], d["n"], d["l2"], d["w"], m_vec, cmax, 200)  # noqa: E731
+    t, outs = _timed_passes(ctx, stream, call, max(args.warmup, 1), max(args.steps, 1))
+    ms = 1e3 * t / max(args.steps, 1)
+    q = K + 2
+    print(json.dumps({"workload": "partitioned-h2", "config": {"n_snp": m, "annotations": K, "traits": T,
+                                                              "n_blocks": 200},
+                      "ms_per_call": ms, "traits_per_s": T / (ms / 1e3),
+                      "gram_flops_per_call": sum(f.n_obs for f in outs[-1]) * q * (q + 1)}), flush=True)
+
+
 def _partitioned_h2(ctx, stream, d_l2, annot, args, n_traits=8, n_blocks=200):
     """Partitioned h2 (fit_h2_partitioned) of n_traits synthetic traits on the
     device-resident K-column LD scores just computed: chi2 = (sqrt(N s) b +
@@ -533,7 +561,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", default="biobank",
-                    choices=["biobank", "profile", "sketch", "partitioned", "serving"])
+                    choices=["biobank", "profile", "sketch", "partitioned", "partitioned-h2", "serving"])
+    ap.add_argument("--h2p-snps", type=int, default=500_000, help="partitioned-h2: regression SNPs")
+    ap.add_argument("--h2p-annot", type=int, default=97, help="partitioned-h2: LD-score columns K")
+    ap.add_argument("--h2p-traits", type=int, default=8, help="partitioned-h2: traits per call")
     ap.add_argument("--serve-rate", type=float, default=40.0, help="serving: Poisson arrivals per second")
     ap.add_argument("--serve-seconds", type=float, default=30.0, help="serving: length of the arrival window")
     ap.add_argument("--serve-slots", type=int, default=6, help="serving: concurrent job slots")
@@ -579,6 +610,9 @@ def main():
         return
     if args.workload == "partitioned":
         run_partitioned_workload(args, ctx, stream)
+        return
+    if args.workload == "partitioned-h2":
+        run_partitioned_h2_workload(args, ctx, stream)
         return
     if args.workload == "serving":
         print(json.dumps(run_serving_workload(args, ctx, args.serve_seconds, args.serve_rate)), flush=True)

@@ -343,10 +343,10 @@ __global__ void __launch_bounds__(NT) k_p_solve(const double* __restrict__ gram,
         const double d = M[c * w + c];
         for (int r = c + 1 + threadIdx.x; r < p; r += NT) M[r * w + c] = M[r * w + c] / d;
         __syncthreads();
-        const int rows = p - c - 1, cols = w - c - 1;
-        for (int e = threadIdx.x; e < rows * cols; e += NT) {
-            const int r = c + 1 + e / cols, x = c + 1 + e % cols;
-            M[r * w + x] = fma(-M[r * w + c], M[c * w + x], M[r * w + x]);
+        // trailing update: warps over rows, lanes over columns
+        for (int r = c + 1 + warp; r < p; r += NT / 32) {
+            const double mr = M[r * w + c];
+            for (int x = c + 1 + lane; x < w; x += 32) M[r * w + x] = fma(-mr, M[c * w + x], M[r * w + x]);
         }
         __syncthreads();
     }
