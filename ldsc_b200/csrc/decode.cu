@@ -83,8 +83,10 @@ __device__ __forceinline__ void expand16(uint32_t w, uint8_t* grow, uint8_t* mro
         mk.y = spread4(pres >> 8);
         mk.z = spread4(pres >> 16);
         mk.w = spread4(pres >> 24);
-        *reinterpret_cast<uint4*>(grow + i0) = g;   // a warp stores 512 contiguous bytes
-        *reinterpret_cast<uint4*>(mrow + i0) = mk;
+        // a warp stores 512 contiguous bytes; streaming stores: the operand
+        // rows are re-read by the Gram from HBM, not from L2
+        __stcs(reinterpret_cast<uint4*>(grow + i0), g);
+        __stcs(reinterpret_cast<uint4*>(mrow + i0), mk);
     }
 }
 
