@@ -355,8 +355,10 @@ int ldsc_h2_partitioned(ldsc_ctx *ctx, const ldsc_h2p_args *args, ldsc_h2p_resul
  * device_budget (0 = free memory at creation minus 4 GiB).  A later job may
  * pass an older one that does not fit yet; idle slots give their workspace
  * back when the oldest job needs it.  Admitted jobs run concurrently and
- * their kernels overlap on the device; regression pipelines replay as cached
- * CUDA graphs.  A job's result does not depend on what else runs. */
+ * their kernels overlap on the device; the h2 and rg pipelines replay as
+ * cached CUDA graphs (partitioned h2 reads its kept-SNP counts on the host
+ * part-way and runs as plain launches).  A job's result does not depend on
+ * what else runs. */
 typedef struct ldsc_server ldsc_server;
 
 enum { LDSC_JOB_L2 = 0, LDSC_JOB_H2 = 1, LDSC_JOB_RG = 2, LDSC_JOB_H2P = 3 };
