@@ -181,3 +181,16 @@ def test_partitioned_device_tensors_equal_host_arrays(ctx):
         np.testing.assert_array_equal(a.est, b.est)
         np.testing.assert_array_equal(a.cov, b.cov)
         assert a.h2_total == b.h2_total and a.n_obs == b.n_obs
+
+
+def test_partitioned_errors(ctx):
+    """Every SNP above the chi2 cut, and an M vector of the wrong length, are
+    errors (run_h2 stops on both: src/regressions.rs:530-533, 1131-1136)."""
+    from ldsc_b200.api import LdscError
+    from ldsc_b200.partitioned import h2_partitioned
+    m, k = 3_000, 2
+    l2, wld = _annot_ld(m, k, 97)
+    with pytest.raises(LdscError):
+        h2_partitioned(ctx, np.full(m, 500.0), 1e4, l2, wld, [1e3, 1e3], 20)
+    with pytest.raises(ValueError):
+        h2_partitioned(ctx, np.ones(m), 1e4, l2, wld, [1e3, 1e3, 1e3], 20)
