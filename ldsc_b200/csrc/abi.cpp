@@ -1580,6 +1580,9 @@ extern "C" int ldsc_h2_partitioned(ldsc_ctx* ctx, const ldsc_h2p_args* a, ldsc_h
     }
     size_t max_gj = 0;
     for (auto& gr : groups) max_gj = std::max(max_gj, gr.size());
+    // traits per launch, so the block Grams stay within a fixed budget
+    const size_t chunk = (size_t)part_trait_chunk((int)std::max<size_t>(max_gj, 1), nb, Q);
+    max_gj = std::min(max_gj, chunk);
     CK(ctx->p_jobs.ensure(sizeof(PartJob) * T));
     CK(ctx->p_st.ensure(sizeof(PartState) * T));
     CK(ctx->p_xtot.ensure(8 * n));
@@ -1591,16 +1594,20 @@ extern "C" int ldsc_h2_partitioned(ldsc_ctx* ctx, const ldsc_h2p_args* a, ldsc_h
     CK(cudaMemcpyAsync(ctx->p_jobs.p, pj.data(), sizeof(PartJob) * T, cudaMemcpyHostToDevice, s));
     std::vector<double> hres(res_len);
     size_t ro = 0;
+    bool first = true;
     for (size_t gi = 0; gi < groups.size(); gi++) {
-        const int nj = (int)groups[gi].size();
-        if (nj == 0) continue;
         const int gb = gnb[gi];
-        CK(launch_partitioned(ctx->p_jobs.as<PartJob>() + gofs[gi], ctx->p_st.as<PartState>() + gofs[gi], d_l2, d_ld,
-                              K, fixed, d_w, n, gb, m_tot, ctx->p_m.as<double>(), ctx->p_xtot.as<double>(), ro == 0,
-                              ctx->p_part.as<double>(), ctx->p_gram.as<double>(), ctx->p_tot.as<double>(),
-                              ctx->p_sol.as<double>(), ctx->p_res.as<double>() + ro, nj, s));
-        ctx->kernels += ro == 0 ? 7 : 6;
-        ro += (size_t)nj * part_result_len(gb, K, P);
+        for (size_t c0 = 0; c0 < groups[gi].size(); c0 += chunk) {
+            const int nj = (int)std::min(chunk, groups[gi].size() - c0);
+            const size_t jo = (size_t)gofs[gi] + c0;
+            CK(launch_partitioned(ctx->p_jobs.as<PartJob>() + jo, ctx->p_st.as<PartState>() + jo, d_l2, d_ld, K,
+                                  fixed, d_w, n, gb, m_tot, ctx->p_m.as<double>(), ctx->p_xtot.as<double>(), first,
+                                  ctx->p_part.as<double>(), ctx->p_gram.as<double>(), ctx->p_tot.as<double>(),
+                                  ctx->p_sol.as<double>(), ctx->p_res.as<double>() + ro, nj, s));
+            ctx->kernels += first ? 7 : 6;
+            first = false;
+            ro += (size_t)nj * part_result_len(gb, K, P);
+        }
     }
     CK(cudaMemcpyAsync(hres.data(), ctx->p_res.p, 8 * res_len, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));

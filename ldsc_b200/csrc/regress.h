@@ -112,6 +112,14 @@ __host__ __device__ inline int part_params(int k, bool fixed) { return k + (fixe
 __host__ __device__ inline size_t part_result_len(int nb, int k, int p) { return (size_t)p * (1 + p + nb) + k + 7; }
 // Shared memory of one delete-value solve (p x (p + 1) doubles) is capped here.
 constexpr int PART_SOLVE_SMEM = 210 * 1024;
+// Traits per launch: the block Grams of a launch (traits x nb x q^2 doubles)
+// stay within 1 GiB.
+inline int part_trait_chunk(int traits, int nb, int q) {
+    const double per = 8.0 * nb * (double)q * q;
+    int c = (int)((double)(1u << 30) / per);
+    if (c < 1) c = 1;
+    return c < traits ? c : traits;
+}
 
 // x_tot (when want_xtot), aggregate, per-block Grams of the weighted design,
 // block totals, nb + 1 LU solves and the jackknife for every job.  Scratch:

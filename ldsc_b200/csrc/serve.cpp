@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/ldsc_b200.h"
+#include "regress.h"
 
 namespace {
 
@@ -52,7 +53,8 @@ uint64_t regression_bytes(const ldsc_job& j) {
         const ldsc_h2p_args& a = j.h2p;
         const uint64_t T = a.n_traits, n = a.n_snp, nb = a.n_blocks, K = a.n_annot;
         const uint64_t P = K + (a.fixed_intercept ? 0 : 1), Q = P + 1;
-        uint64_t b = 8 * T * (nb * Q * Q + Q * Q + (nb + 1) * P + P * (1 + P + nb) + K + 7 + 3 * nb) +
+        const uint64_t C = (uint64_t)ldsc::part_trait_chunk((int)(T ? T : 1), (int)nb, (int)Q);  // traits per launch
+        uint64_t b = 8 * C * (nb * Q * Q + Q * Q + (nb + 1) * P + 3 * nb) + 8 * T * (P * (1 + P + nb) + K + 7) +
                      4 * T * (2 * (nb + 1) + (n + 4095) / 4096) + 8 * n + 4096 + 256 * T;
         if (!a.device_pointers) b += 8 * T * n * (a.n_per_snp ? 2 : 1) + 8 * n * (K + 1);
         return b;

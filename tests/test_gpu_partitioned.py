@@ -194,3 +194,19 @@ def test_partitioned_errors(ctx):
         h2_partitioned(ctx, np.full(m, 500.0), 1e4, l2, wld, [1e3, 1e3], 20)
     with pytest.raises(ValueError):
         h2_partitioned(ctx, np.ones(m), 1e4, l2, wld, [1e3, 1e3, 1e3], 20)
+
+
+def test_partitioned_trait_chunks_equal_single_calls(ctx):
+    """A batch whose block Grams exceed one launch's budget (K = 159: 25
+    traits per launch) runs in trait chunks; each trait's fit equals its fit
+    alone, bit for bit."""
+    from ldsc_b200.partitioned import h2_partitioned
+    m, k, T = 6_000, 159, 30
+    l2, wld = _annot_ld(m, k, 98)
+    m_vec = np.full(k, 100.0)
+    chi2, n = _traits(l2, m_vec, T, 99)
+    batch = h2_partitioned(ctx, chi2, n, l2, wld, m_vec, 200)
+    for t in (0, 24, 25, 29):
+        one = h2_partitioned(ctx, chi2[t], n[t], l2, wld, m_vec, 200)
+        np.testing.assert_array_equal(batch[t].est, one.est)
+        np.testing.assert_array_equal(batch[t].delete_values, one.delete_values)
