@@ -6,7 +6,8 @@
 //     then the quadratic bias inversion (+ MAF-aware shift) in f64
 //     (src/l2/compute.rs:947-998).
 // Tiles are 128 x 128 records, 256 threads, 8 x 8 outputs per thread, K-slices
-// of 8 double-buffered through shared memory.  The epilogue masks pairs
+// of 16 double-buffered through shared memory (rows padded by one element so
+// the transposed staging stores do not share banks).  The epilogue masks pairs
 // outside the band and accumulates l2 in f64.
 #include <cuda_runtime.h>
 
@@ -17,7 +18,8 @@ namespace ldsc {
 
 namespace {
 
-constexpr int TA = 128, TB = 128, BK = 8, NT = 256;
+constexpr int TA = 128, TB = 128, BK = 16, NT = 256;
+constexpr int STA = TA + 1, STB = TB + 1;  // staged row strides
 constexpr int RLD = TB + 1;  // padded row stride of the staged R tile
 
 template <int MODE>
@@ -57,10 +59,10 @@ __global__ void __launch_bounds__(NT, 1)
     k_gram_simt(const T* __restrict__ x, uint64_t ld, uint64_t kdim, const Tile* __restrict__ tiles,
                 int64_t n_tiles, EpilogueArgs ep) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* As = reinterpret_cast<T*>(smem_raw);  // [2][BK][TA]
-    T* Bs = As + 2 * BK * TA;                // [2][BK][TB]
+    T* As = reinterpret_cast<T*>(smem_raw);  // [2][BK][STA]
+    T* Bs = As + 2 * BK * STA;               // [2][BK][STB]
     const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-    const int lrow = tid >> 1, lcol = (tid & 1) * 4;
+    const int lrow = tid >> 1, lcol = (tid & 1) * (BK / 2);
     const int64_t m = ep.m;
 
     for (int64_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
@@ -74,18 +76,23 @@ __global__ void __launch_bounds__(NT, 1)
 #pragma unroll
             for (int l = 0; l < 8; l++) acc[i][l] = T(0);
 
-        T ra[4], rb[4];
+        T ra[BK / 2], rb[BK / 2];
         auto gload = [&](uint64_t kk) {
-            if (arow) Vec4<T>::load(arow + kk + lcol, ra);
-            else ra[0] = ra[1] = ra[2] = ra[3] = T(0);
-            if (brow) Vec4<T>::load(brow + kk + lcol, rb);
-            else rb[0] = rb[1] = rb[2] = rb[3] = T(0);
+#pragma unroll
+            for (int h = 0; h < BK / 8; h++) {
+                T* pa = ra + 4 * h;
+                T* pb = rb + 4 * h;
+                if (arow) Vec4<T>::load(arow + kk + lcol + 4 * h, *reinterpret_cast<T(*)[4]>(pa));
+                else pa[0] = pa[1] = pa[2] = pa[3] = T(0);
+                if (brow) Vec4<T>::load(brow + kk + lcol + 4 * h, *reinterpret_cast<T(*)[4]>(pb));
+                else pb[0] = pb[1] = pb[2] = pb[3] = T(0);
+            }
         };
         auto sstore = [&](int buf) {
 #pragma unroll
-            for (int q = 0; q < 4; q++) {
-                As[(buf * BK + lcol + q) * TA + lrow] = ra[q];
-                Bs[(buf * BK + lcol + q) * TB + lrow] = rb[q];
+            for (int q = 0; q < BK / 2; q++) {
+                As[(buf * BK + lcol + q) * STA + lrow] = ra[q];
+                Bs[(buf * BK + lcol + q) * STB + lrow] = rb[q];
             }
         };
         gload(0);
@@ -99,9 +106,9 @@ __global__ void __launch_bounds__(NT, 1)
             for (int s = 0; s < BK; s++) {
                 T a[8], b[8];
 #pragma unroll
-                for (int i = 0; i < 8; i++) a[i] = As[(buf * BK + s) * TA + ty + 16 * i];
+                for (int i = 0; i < 8; i++) a[i] = As[(buf * BK + s) * STA + ty + 16 * i];
 #pragma unroll
-                for (int l = 0; l < 8; l++) b[l] = Bs[(buf * BK + s) * TB + tx + 16 * l];
+                for (int l = 0; l < 8; l++) b[l] = Bs[(buf * BK + s) * STB + tx + 16 * l];
 #pragma unroll
                 for (int i = 0; i < 8; i++)
 #pragma unroll
@@ -184,7 +191,7 @@ template <typename T, int MODE>
 cudaError_t launch(const T* x, uint64_t ld, uint64_t kdim, const Tile* tiles, int64_t n_tiles,
                    const EpilogueArgs& ep, int sms, cudaStream_t stream) {
     if (n_tiles <= 0) return cudaSuccess;
-    size_t op_bytes = sizeof(T) * 2 * BK * (TA + TB);
+    size_t op_bytes = sizeof(T) * 2 * BK * (STA + STB);
     size_t cpart_bytes = sizeof(double) * 16 * TB;
     size_t r_bytes = ep.K > 1 ? sizeof(float) * TA * RLD : 0;
     size_t smem = op_bytes;
