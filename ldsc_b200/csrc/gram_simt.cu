@@ -5,9 +5,11 @@
 //   * FP32 CountSketch form: sketched, renormalised f32 rows, val = s_k . s_j,
 //     then the quadratic bias inversion (+ MAF-aware shift) in f64
 //     (src/l2/compute.rs:947-998).
-// Tiles are 128 x 128 records, 256 threads, 8 x 8 outputs per thread, K-slices
-// of 16 double-buffered through shared memory (rows padded by one element so
-// the transposed staging stores do not share banks).  The epilogue masks pairs
+// Tiles are 128 x 128 records, 256 threads, 8 x 8 outputs per thread.
+// K-slices of 16 are copied into shared memory by cp.async, three in flight,
+// row-major with an odd row stride (17 elements) so the 16 lanes that read
+// one operand column hit distinct banks; rows past the record count are
+// zero-filled by the copy.  The epilogue masks pairs
 // outside the band and accumulates l2 in f64.
 #include <cuda_runtime.h>
 
@@ -19,7 +21,22 @@ namespace ldsc {
 namespace {
 
 constexpr int TA = 128, TB = 128, BK = 16, NT = 256;
-constexpr int STA = TA + 1, STB = TB + 1;  // staged row strides
+constexpr int SK = BK + 1;   // staged row stride (elements)
+constexpr int NSTAGE = 3;    // K-slices in flight
+
+// Element-sized asynchronous copy global -> shared; with valid == false the
+// destination is zero-filled and nothing is read.
+template <typename T>
+__device__ __forceinline__ void cp_elem(T* dst, const T* src, bool valid) {
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+    if (sizeof(T) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(valid ? 8 : 0) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(d), "l"(src), "r"(valid ? 4 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 constexpr int RLD = TB + 1;  // padded row stride of the staged R tile
 
 template <int MODE>
@@ -36,88 +53,66 @@ __device__ __forceinline__ double correct(double v, int64_t k, int64_t j, const 
     }
 }
 
-template <typename T>
-struct Vec4;
-template <>
-struct Vec4<double> {
-    static __device__ __forceinline__ void load(const double* p, double (&r)[4]) {
-        const double2 a = *reinterpret_cast<const double2*>(p);
-        const double2 b = *reinterpret_cast<const double2*>(p + 2);
-        r[0] = a.x; r[1] = a.y; r[2] = b.x; r[3] = b.y;
-    }
-};
-template <>
-struct Vec4<float> {
-    static __device__ __forceinline__ void load(const float* p, float (&r)[4]) {
-        const float4 a = *reinterpret_cast<const float4*>(p);
-        r[0] = a.x; r[1] = a.y; r[2] = a.z; r[3] = a.w;
-    }
-};
-
 template <typename T, int MODE>
 __global__ void __launch_bounds__(NT, 1)
     k_gram_simt(const T* __restrict__ x, uint64_t ld, uint64_t kdim, const Tile* __restrict__ tiles,
                 int64_t n_tiles, EpilogueArgs ep) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* As = reinterpret_cast<T*>(smem_raw);  // [2][BK][STA]
-    T* Bs = As + 2 * BK * STA;               // [2][BK][STB]
+    T* As = reinterpret_cast<T*>(smem_raw);  // [NSTAGE][TA][SK]
+    T* Bs = As + NSTAGE * TA * SK;           // [NSTAGE][TB][SK]
     const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-    const int lrow = tid >> 1, lcol = (tid & 1) * (BK / 2);
     const int64_t m = ep.m;
+    const uint64_t nk = kdim / BK;
 
     for (int64_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
         const Tile tl = tiles[t];
         const int64_t k0 = (int64_t)tl.a_blk * TA, j0 = (int64_t)tl.b_blk * TB;
-        const T* arow = (k0 + lrow < m) ? x + (uint64_t)(k0 + lrow) * ld : nullptr;
-        const T* brow = (j0 + lrow < m) ? x + (uint64_t)(j0 + lrow) * ld : nullptr;
         T acc[8][8];
 #pragma unroll
         for (int i = 0; i < 8; i++)
 #pragma unroll
             for (int l = 0; l < 8; l++) acc[i][l] = T(0);
 
-        T ra[BK / 2], rb[BK / 2];
-        auto gload = [&](uint64_t kk) {
+        // K-slice `it` into stage it % NSTAGE: TA x BK and TB x BK elements,
+        // 8 + 8 per thread, consecutive threads along a row's K elements
+        auto issue = [&](uint64_t it) {
+            if (it < nk) {
+                const int st = (int)(it % NSTAGE);
+                const uint64_t kk = it * BK;
 #pragma unroll
-            for (int h = 0; h < BK / 8; h++) {
-                T* pa = ra + 4 * h;
-                T* pb = rb + 4 * h;
-                if (arow) Vec4<T>::load(arow + kk + lcol + 4 * h, *reinterpret_cast<T(*)[4]>(pa));
-                else pa[0] = pa[1] = pa[2] = pa[3] = T(0);
-                if (brow) Vec4<T>::load(brow + kk + lcol + 4 * h, *reinterpret_cast<T(*)[4]>(pb));
-                else pb[0] = pb[1] = pb[2] = pb[3] = T(0);
+                for (int q = 0; q < TA * BK / NT; q++) {
+                    const int e = tid + NT * q, r = e / BK, c = e % BK;
+                    const bool va = k0 + r < m, vb = j0 + r < m;
+                    cp_elem(As + (st * TA + r) * SK + c, va ? x + (uint64_t)(k0 + r) * ld + kk + c : x, va);
+                    cp_elem(Bs + (st * TB + r) * SK + c, vb ? x + (uint64_t)(j0 + r) * ld + kk + c : x, vb);
+                }
             }
+            cp_commit();
         };
-        auto sstore = [&](int buf) {
 #pragma unroll
-            for (int q = 0; q < BK / 2; q++) {
-                As[(buf * BK + lcol + q) * STA + lrow] = ra[q];
-                Bs[(buf * BK + lcol + q) * STB + lrow] = rb[q];
-            }
-        };
-        gload(0);
-        sstore(0);
-        __syncthreads();
-        int buf = 0;
-        for (uint64_t kk = 0; kk < kdim; kk += BK) {
-            const bool more = kk + BK < kdim;
-            if (more) gload(kk + BK);
+        for (int s0 = 0; s0 < NSTAGE - 1; s0++) issue(s0);
+        for (uint64_t it = 0; it < nk; it++) {
+            cp_wait<NSTAGE - 2>();
+            __syncthreads();              // slice `it` landed; slice it - 1 is no longer read
+            issue(it + NSTAGE - 1);       // into the stage slice it - 1 used
+            const int st = (int)(it % NSTAGE);
+            const T* as = As + st * TA * SK;
+            const T* bs = Bs + st * TB * SK;
 #pragma unroll
             for (int s = 0; s < BK; s++) {
                 T a[8], b[8];
 #pragma unroll
-                for (int i = 0; i < 8; i++) a[i] = As[(buf * BK + s) * STA + ty + 16 * i];
+                for (int i = 0; i < 8; i++) a[i] = as[(ty + 16 * i) * SK + s];
 #pragma unroll
-                for (int l = 0; l < 8; l++) b[l] = Bs[(buf * BK + s) * STB + tx + 16 * l];
+                for (int l = 0; l < 8; l++) b[l] = bs[(tx + 16 * l) * SK + s];
 #pragma unroll
                 for (int i = 0; i < 8; i++)
 #pragma unroll
                     for (int l = 0; l < 8; l++) acc[i][l] = fma(a[i], b[l], acc[i][l]);
             }
-            if (more) sstore(buf ^ 1);
-            __syncthreads();
-            buf ^= 1;
         }
+        cp_wait<0>();
+        __syncthreads();  // the epilogue reuses the staging memory
 
         // ---- epilogue: r^2 correction, band mask, l2 accumulation ----
         if (ep.K == 1) {
@@ -191,7 +186,7 @@ template <typename T, int MODE>
 cudaError_t launch(const T* x, uint64_t ld, uint64_t kdim, const Tile* tiles, int64_t n_tiles,
                    const EpilogueArgs& ep, int sms, cudaStream_t stream) {
     if (n_tiles <= 0) return cudaSuccess;
-    size_t op_bytes = sizeof(T) * 2 * BK * (STA + STB);
+    size_t op_bytes = sizeof(T) * NSTAGE * (TA + TB) * SK;
     size_t cpart_bytes = sizeof(double) * 16 * TB;
     size_t r_bytes = ep.K > 1 ? sizeof(float) * TA * RLD : 0;
     size_t smem = op_bytes;
