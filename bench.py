@@ -719,8 +719,10 @@ def main():
     roofline = {"bound": "tensor", "achieved": achieved, "peak": int8_peak, "unit": "TFLOP/s",
                 "frac": achieved / int8_peak, "traffic": committed_traffic("k_gram_tc"),
                 "kernel": "k_gram_tc<4,0> (tcgen05.mma kind::i8)",
-                "note": f"int8 ops counted like flops (2 per MAC, 4 products per pair); peak = 2 x {src} "
-                        "bf16 dense burst (MEASURED_PEAKS.json), nominal int8 dense 4500"}
+                "note": "int8 ops counted like flops (2 per MAC, 4 products per pair); peak = 2 x "
+                        + ("measured bf16 dense burst (MEASURED_PEAKS.json)" if src == "measured" else
+                           "fallback bf16 dense burst 1590 TFLOP/s (MEASURED_PEAKS.json absent)")
+                        + ", nominal int8 dense 4500"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
