@@ -115,9 +115,18 @@ cudaError_t launch_sketch_permute(const PanelView& p, const int32_t* perm, uint6
 // k/2, sign + for even k).
 // out: m rows of `ld` floats, or with split = 1 the tensor-core operand form:
 // rows 2r = tf32(v) and 2r+1 = tf32(v - tf32(v)), `ld` floats each.
+// segt (may be null): the layout's thread-major boundary table
+// (launch_sketch_segt); with it, large d (sketch_large_d) runs the
+// shared-memory-row form.
 cudaError_t launch_sketch_seg(const uint32_t* pp, uint64_t pp_pitch_words, const uint64_t* rec_rows, int64_t m,
-                              uint64_t n_used, const int32_t* seg_off, uint32_t d, RecStats st,
+                              uint64_t n_used, const int32_t* seg_off, const int32_t* segt, uint32_t d, RecStats st,
                               int want_moments, int split, float* out, uint64_t ld, cudaStream_t stream);
+// Whether d and n_used take the large-d form (d >= 2048 and its shared memory fits).
+bool sketch_large_d(uint64_t n_used, uint32_t d);
+// Entries of the thread-major boundary table, and its construction from the
+// 2d + 1 run starts (once per layout).
+uint64_t sketch_segt_count(uint32_t d);
+cudaError_t launch_sketch_segt(const int32_t* seg_off, uint32_t d, int32_t* segt, cudaStream_t stream);
 // Whether the sketch kernel's shared memory holds n_used individuals and d buckets.
 bool sketch_supported(uint64_t n_used, uint32_t d);
 

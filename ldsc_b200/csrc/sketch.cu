@@ -302,6 +302,220 @@ __global__ void __launch_bounds__(SNT, 8) k_sketch_seg(const uint32_t* __restric
     }
 }
 
+// ---- large d: quads in shared memory, thread-major boundary positions ----
+//
+// With many buckets the boundary phase dominates and its quad re-reads go to
+// L2.  This form keeps the row's quads in shared memory and, per quad, the
+// prefix before it and the offsets of its words 1..3 inside it (8 bits each),
+// made block-absolute by a fix-up pass; thread t's boundary positions come
+// from a thread-major table (entry i * S6T + t = i-th boundary of thread t,
+// built once per layout), so their loads are coalesced, and each boundary
+// prefix costs two shared-memory loads and two popcounts.  256 threads per
+// CTA: its shared memory (32 B per 64 individuals + 4 B per bucket) allows
+// few CTAs per SM, so each CTA brings more warps.  Same arithmetic as the
+// kernel above; results are bit-identical.
+constexpr int S6T = 256;
+constexpr int S6W = S6T / 32;
+
+__host__ __device__ inline uint32_t seg6_b(uint32_t d, uint32_t t) { return (uint32_t)((uint64_t)d * t / S6T); }
+__host__ __device__ inline uint32_t seg6_count(uint32_t d, uint32_t t) {
+    const uint32_t b0 = seg6_b(d, t), b1 = seg6_b(d, t + 1);
+    return b0 < b1 ? 2 * (b1 - b0) + 1 : 0;
+}
+__host__ __device__ inline uint32_t seg6_rows(uint32_t d) { return 2 * ((d + S6T - 1) / S6T) + 1; }
+__host__ __device__ inline size_t sketch6_smem(uint64_t n_used, uint32_t d) {
+    return 32 * sketch_quads(n_used) + 4 * (size_t)d + 16;
+}
+
+__global__ void k_sketch_segt(const int32_t* __restrict__ seg_off, uint32_t d, uint32_t rows,
+                              int32_t* __restrict__ segt) {
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < rows * S6T; e += gridDim.x * blockDim.x) {
+        const uint32_t i = e / S6T, t = e % S6T;
+        segt[e] = i < seg6_count(d, t) ? seg_off[2 * seg6_b(d, t) + i] : 0x7FFFFFFF;
+    }
+}
+
+__global__ void __launch_bounds__(S6T, 2) k_sketch_seg6(const uint32_t* __restrict__ pp, uint64_t pp_pitch_words,
+                                                      const uint64_t* __restrict__ rec_rows, int64_t m,
+                                                      uint64_t n_used, const int32_t* __restrict__ segt, uint32_t d,
+                                                      RecStats st, int want_moments, int split,
+                                                      float* __restrict__ out, uint64_t ld) {
+    extern __shared__ __align__(16) uint4 sh6[];
+    const uint32_t quads = (uint32_t)sketch_quads(n_used);
+    uint4* PQ = sh6;          // prefix (popc, missing) before the quad, packed word offsets
+    uint4* Rs = sh6 + quads;  // the quads
+    float* ob = reinterpret_cast<float*>(sh6 + 2 * (size_t)quads);
+    __shared__ int32_t wa[S6W], wm[S6W], wt[S6W];
+    __shared__ double dred[S6W];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t wq0 = (uint32_t)((uint64_t)quads * warp / S6W), wq1 = (uint32_t)((uint64_t)quads * (warp + 1) / S6W);
+    const uint32_t b0 = seg6_b(d, threadIdx.x), nbd = seg6_count(d, threadIdx.x);
+    const int32_t row_len = (int32_t)(64 * quads);
+    for (int64_t r = blockIdx.x; r < m; r += gridDim.x) {
+        const uint64_t brow = rec_rows ? rec_rows[r] : (uint64_t)r;
+        const uint4* row = reinterpret_cast<const uint4*>(pp + brow * pp_pitch_words);
+        // ---- phase 1 ----
+        int32_t carryA = 0, carryM = 0;
+        uint32_t T2 = 0;
+        uint4 n0 = make_uint4(0, 0, 0, 0), n1 = n0;
+        if (wq0 + 2 * lane < wq1) n0 = __ldg(row + wq0 + 2 * lane);
+        if (wq0 + 2 * lane + 1 < wq1) n1 = __ldg(row + wq0 + 2 * lane + 1);
+        for (uint32_t c0 = wq0; c0 < wq1; c0 += CHUNK_Q) {
+            const uint32_t qa = c0 + 2 * lane;
+            const bool l0 = qa < wq1, l1 = qa + 1 < wq1;
+            const uint4 v0 = n0, v1 = n1;
+            if (qa + CHUNK_Q < wq1) n0 = __ldg(row + qa + CHUNK_Q);
+            if (qa + CHUNK_Q + 1 < wq1) n1 = __ldg(row + qa + CHUNK_Q + 1);
+            const uint32_t x[8] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y, v1.z, v1.w};
+            int32_t ca[8], cm[8];
+#pragma unroll
+            for (int t = 0; t < 8; t++) {
+                ca[t] = __popc(x[t]);
+                cm[t] = __popc(miss_bits(x[t]));
+            }
+            const uint32_t t0 = __popc(two_bits(x[0]) | (two_bits(x[1]) << 1)) +
+                                __popc(two_bits(x[2]) | (two_bits(x[3]) << 1));
+            const uint32_t t1 = __popc(two_bits(x[4]) | (two_bits(x[5]) << 1)) +
+                                __popc(two_bits(x[6]) | (two_bits(x[7]) << 1));
+            const int32_t a0 = ca[0] + ca[1] + ca[2] + ca[3], a1 = ca[4] + ca[5] + ca[6] + ca[7];
+            const int32_t m0 = cm[0] + cm[1] + cm[2] + cm[3], m1 = cm[4] + cm[5] + cm[6] + cm[7];
+            const int32_t la = (l0 ? a0 : 0) + (l1 ? a1 : 0), lm = (l0 ? m0 : 0) + (l1 ? m1 : 0);
+            T2 += (l0 ? t0 : 0u) + (l1 ? t1 : 0u);
+            const int32_t ia = warp_incl_scan(la, lane), im = warp_incl_scan(lm, lane);
+            const int32_t ea = carryA + ia - la, em = carryM + im - lm;
+            // offsets of words 1..3 inside each quad, byte t for word t (byte 0 = 0)
+            const uint32_t pa0 = ((uint32_t)ca[0] << 8) | ((uint32_t)(ca[0] + ca[1]) << 16) |
+                                 ((uint32_t)(ca[0] + ca[1] + ca[2]) << 24);
+            const uint32_t pm0 = ((uint32_t)cm[0] << 8) | ((uint32_t)(cm[0] + cm[1]) << 16) |
+                                 ((uint32_t)(cm[0] + cm[1] + cm[2]) << 24);
+            const uint32_t pa1 = ((uint32_t)ca[4] << 8) | ((uint32_t)(ca[4] + ca[5]) << 16) |
+                                 ((uint32_t)(ca[4] + ca[5] + ca[6]) << 24);
+            const uint32_t pm1 = ((uint32_t)cm[4] << 8) | ((uint32_t)(cm[4] + cm[5]) << 16) |
+                                 ((uint32_t)(cm[4] + cm[5] + cm[6]) << 24);
+            if (l0) {
+                PQ[qa] = make_uint4((uint32_t)ea, (uint32_t)em, pa0, pm0);
+                Rs[qa] = v0;
+            }
+            if (l1) {
+                PQ[qa + 1] = make_uint4((uint32_t)(ea + a0), (uint32_t)(em + m0), pa1, pm1);
+                Rs[qa + 1] = v1;
+            }
+            carryA += __shfl_sync(0xFFFFFFFFu, ia, 31);
+            carryM += __shfl_sync(0xFFFFFFFFu, im, 31);
+        }
+        const int32_t t2w = warp_sum((int32_t)T2);
+        if (lane == 0) {
+            wa[warp] = carryA;
+            wm[warp] = carryM;
+            wt[warp] = t2w;
+        }
+        __syncthreads();
+        int32_t A = 0, MS = 0, TT = 0, offA = 0, offM = 0;
+#pragma unroll
+        for (int w = 0; w < S6W; w++) {
+            if (w < warp) {
+                offA += wa[w];
+                offM += wm[w];
+            }
+            A += wa[w];
+            MS += wm[w];
+            TT += wt[w];
+        }
+        const int32_t G = 2 * row_len - A - MS, N = row_len - MS;
+        if (threadIdx.x == 0) {
+            st.n[r] = N;
+            st.s[r] = G;
+            st.q[r] = G + 2 * TT;
+            if (want_moments && st.q3) {
+                st.q3[r] = G + 6 * TT;
+                st.q4[r] = G + 14 * TT;
+            }
+        }
+        const double dmean = N > 0 ? (double)G / (double)N : 0.0;
+        const double css = (double)(G + 2 * TT) - (double)N * dmean * dmean;
+        const double sd = sqrt(css / (double)n_used);
+        const double mean = (double)(float)dmean;
+        const double inv = sd > 0.0 ? (double)(float)(1.0 / sd) : 0.0;
+        // block-absolute quad prefixes
+        if (offA | offM)
+            for (uint32_t q = wq0 + lane; q < wq1; q += 32) {
+                uint2* e = reinterpret_cast<uint2*>(PQ + q);
+                const uint2 v = *e;
+                *e = make_uint2(v.x + (uint32_t)offA, v.y + (uint32_t)offM);
+            }
+        __syncthreads();
+        // ---- phase 2 ----
+        double part = 0.0;
+        if (nbd) {
+            const uint32_t* rw = reinterpret_cast<const uint32_t*>(Rs);
+            int32_t pn[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) pn[u] = (uint32_t)u < nbd ? __ldg(segt + u * S6T + threadIdx.x) : row_len;
+            int32_t g1 = 0, n1w = 0, g2 = 0, n2w = 0;
+            for (uint32_t i = 0; i < nbd; i += 4) {
+                int32_t pc[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    pc[u] = pn[u];
+                    pn[u] = i + 4 + u < nbd ? __ldg(segt + (i + 4 + u) * S6T + threadIdx.x) : row_len;
+                }
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    if (i + u >= nbd) break;
+                    const int32_t p = pc[u];
+                    int32_t pg = G, pnr = N;  // at the row end: the totals
+                    if (p < row_len) {
+                        const uint32_t q = (uint32_t)p >> 6, tw = ((uint32_t)p >> 4) & 3u, j = (uint32_t)p & 15u;
+                        const uint4 e = PQ[q];
+                        const uint32_t y = rw[4 * q + tw];
+                        const uint32_t msk = j ? (0xFFFFFFFFu >> (32 - 2 * j)) : 0u;
+                        const int32_t pa = (int32_t)e.x + (int32_t)((e.z >> (8 * tw)) & 0xFFu) + __popc(y & msk);
+                        const int32_t pm = (int32_t)e.y + (int32_t)((e.w >> (8 * tw)) & 0xFFu) +
+                                           __popc(miss_bits(y) & msk);
+                        pg = 2 * p - pa - pm;
+                        pnr = p - pm;
+                    }
+                    const uint32_t idx = i + u;
+                    if (idx >= 2 && !(idx & 1)) {  // bucket b0 + idx/2 - 1 is complete
+                        const int32_t s1 = (g1 - g2) - (pg - g1), s0 = (n1w - n2w) - (pnr - n1w);
+                        const float o = (float)(inv * ((double)s1 - mean * (double)s0));
+                        ob[b0 + idx / 2 - 1] = o;
+                        part += (double)o * (double)o;
+                    }
+                    g2 = g1;
+                    n2w = n1w;
+                    g1 = pg;
+                    n1w = pnr;
+                }
+            }
+        }
+        part = warp_sum(part);
+        if (lane == 0) dred[warp] = part;
+        __syncthreads();
+        double nrm = 0.0;
+#pragma unroll
+        for (int w = 0; w < S6W; w++) nrm += dred[w];
+        const float scale = nrm > 0.0 ? (float)sqrt((double)n_used / nrm) : 1.0f;
+        float* orow = out + (uint64_t)r * (split ? 2 : 1) * ld;
+        if (split) {
+            float* lrow = orow + ld;
+            for (uint64_t b = threadIdx.x; b < ld; b += S6T) {
+                float hi = 0.f, lo = 0.f;
+                if (b < d) {
+                    const float v = nrm > 0.0 ? ob[b] * scale : ob[b];
+                    hi = to_tf32(v);
+                    lo = to_tf32(v - hi);
+                }
+                orow[b] = hi;
+                lrow[b] = lo;
+            }
+        } else {
+            for (uint64_t b = threadIdx.x; b < ld; b += S6T) orow[b] = b < d ? (nrm > 0.0 ? ob[b] * scale : ob[b]) : 0.f;
+        }
+        __syncthreads();  // PQ, Rs, ob, wa and dred are rewritten by the next record
+    }
+}
+
 }  // namespace
 
 cudaError_t launch_sketch_permute(const PanelView& p, const int32_t* perm, uint64_t n_used, uint32_t* out,
@@ -319,21 +533,39 @@ cudaError_t launch_sketch_permute(const PanelView& p, const int32_t* perm, uint6
 }
 
 cudaError_t launch_sketch_seg(const uint32_t* pp, uint64_t pp_pitch_words, const uint64_t* rec_rows, int64_t m,
-                              uint64_t n_used, const int32_t* seg_off, uint32_t d, RecStats st, int want_moments,
-                              int split, float* out, uint64_t ld, cudaStream_t stream) {
+                              uint64_t n_used, const int32_t* seg_off, const int32_t* segt, uint32_t d, RecStats st,
+                              int want_moments, int split, float* out, uint64_t ld, cudaStream_t stream) {
     if (m <= 0) return cudaSuccess;
+    const int64_t grid = m < 148 * 16 ? m : 148 * 16;
+    if (segt && sketch_large_d(n_used, d)) {
+        const size_t smem6 = sketch6_smem(n_used, d);
+        cudaError_t e = cudaFuncSetAttribute(k_sketch_seg6, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem6);
+        if (e != cudaSuccess) return e;
+        k_sketch_seg6<<<(unsigned)grid, S6T, smem6, stream>>>(pp, pp_pitch_words, rec_rows, m, n_used, segt, d, st,
+                                                               want_moments, split, out, ld);
+        return cudaGetLastError();
+    }
     const size_t smem = sketch_smem(n_used, d);
     if (smem > 200 * 1024) return cudaErrorInvalidValue;  // rejected by the caller first (ldsc_sketch_supported)
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(k_sketch_seg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
-    int64_t grid = m < 148 * 16 ? m : 148 * 16;
     k_sketch_seg<<<(unsigned)grid, SNT, smem, stream>>>(pp, pp_pitch_words, rec_rows, m, n_used, seg_off, d, st,
                                                        want_moments, split, out, ld);
     return cudaGetLastError();
 }
 
 bool sketch_supported(uint64_t n_used, uint32_t d) { return sketch_smem(n_used, d) <= 200 * 1024; }
+
+bool sketch_large_d(uint64_t n_used, uint32_t d) { return d >= 2048 && sketch6_smem(n_used, d) <= 200 * 1024; }
+
+uint64_t sketch_segt_count(uint32_t d) { return (uint64_t)seg6_rows(d) * S6T; }
+
+cudaError_t launch_sketch_segt(const int32_t* seg_off, uint32_t d, int32_t* segt, cudaStream_t stream) {
+    const uint32_t rows = seg6_rows(d);
+    k_sketch_segt<<<64, 256, 0, stream>>>(seg_off, d, rows, segt);
+    return cudaGetLastError();
+}
 
 }  // namespace ldsc
