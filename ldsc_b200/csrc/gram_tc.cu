@@ -31,7 +31,9 @@
 //              UMMA issuer (tcgen05.mma kind::i8, M=128 N=256 K=32, four per stage)
 //   warps 2-5  epilogue: tcgen05.ld of the accumulator, exact r^2, band mask,
 //              l2 accumulation; accumulator double-buffering overlaps the
-//              epilogue of tile t with the MMAs of tile t+1.
+//              epilogue of tile t with the MMAs of tile t+1.  The sketch
+//              forms (short K, a heavier per-pair correction) use warps 2-9:
+//              two warps per TMEM lane quarter, each on half the columns.
 // Every mbarrier wait is bounded; on timeout the kernel records an error word,
 // drains its own in-flight copies / MMAs (bounded), frees TMEM and returns.
 #include <cuda.h>
@@ -49,7 +51,8 @@ constexpr int TA = 64;             // left records per tile (A rows = 128)
 constexpr int TB = 128;            // right records per tile (B rows = 256)
 constexpr int A_BYTES = 128 * 128; // one stage of A
 constexpr int B_BYTES = 256 * 128; // one stage of B
-constexpr int NTHREADS = 192;
+// threads per CTA: TMA and MMA warps + 4 (INT8) or 8 (sketch) epilogue warps
+__host__ __device__ constexpr int gram_threads(int mode) { return mode == 0 ? 192 : 320; }
 constexpr int RLD = TB + 1;
 constexpr uint64_t WAIT_LIMIT_NS = 2000000000ull;  // 2 s per wait
 
@@ -73,7 +76,7 @@ __device__ __forceinline__ double sketch_r2u(float val, int64_t k, int64_t j, co
 }
 
 template <int STAGES, int MODE>
-__global__ void __launch_bounds__(NTHREADS, 1)
+__global__ void __launch_bounds__(gram_threads(MODE), 1)
     k_gram_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
               int num_kb, const Tile* __restrict__ tiles, int64_t n_tiles, EpilogueArgs ep,
               int32_t* __restrict__ dbg) {
@@ -102,7 +105,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         }
         for (int b = 0; b < 2; b++) {
             mbar_init(&tfull[b], 1);
-            mbar_init(&tempty[b], 128);
+            mbar_init(&tempty[b], gram_threads(MODE) - 64);
         }
         mbar_init(drain, 1);
         fence_mbar_init();
@@ -209,10 +212,15 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             }
         }
     } else {
-        // ------------------------------------------------ epilogue (128 threads)
-        const int et = threadIdx.x - 64;         // 0..127
-        const int ew = et >> 5;                  // epilogue warp 0..3
+        // ------------------------------------------------ epilogue
+        constexpr int EPI_T = gram_threads(MODE) - 64;  // epilogue threads
+        constexpr int CPW = 4 / (EPI_T / 128);          // 64-column chunks per warp
+        const int et = threadIdx.x - 64;         // 0..EPI_T-1
+        const int ew = et >> 5;                  // epilogue warp
         const int quarter = warp & 3;            // TMEM lanes this warp may access
+        const int c_lo = (ew >> 2) * CPW;        // this warp's first column chunk
+        // column partials: one slot per warp with four epilogue warps, per lane quarter with eight
+        const int cslot = EPI_T == 128 ? ew : quarter;
         const int row = quarter * 32 + lane;     // accumulator row = A row
         const bool grow = (row & 1) == 0;        // genotype row (else mask row)
         const int64_t m = ep.m;
@@ -233,21 +241,21 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             // continues, so no thread can be left waiting at a named barrier.
             volatile uint32_t* go = tmem_slot + 1;
             if (et == 0) *go = mbar_wait(&tfull[acc], aphase, WAIT_LIMIT_NS) ? 1u : 0u;
-            named_bar_sync(2, 128);
+            named_bar_sync(2, EPI_T);
             if (*go == 0u) {
                 if (et == 0) atomicOr(ep.err, 4u);
                 break;
             }
             tc_fence_after();
             double rsum = 0.0;
-            for (int c = 0; c < 4; c++) {
+            for (int c = c_lo; c < c_lo + CPW; c++) {
                 uint32_t v[64];
                 tmem_ld_32x32b_x64(tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)acc * 256u +
                                        (uint32_t)c * 64u,
                                    v);
                 tmem_ld_wait();
-                if (c == 3) {
-                    // accumulator fully read: hand it back to the MMA warp
+                if (c == c_lo + CPW - 1) {
+                    // this thread's part of the accumulator read: hand it back to the MMA warp
                     tc_fence_before();
                     mbar_arrive(&tempty[acc]);
                 }
@@ -302,7 +310,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                         cv += __shfl_xor_sync(0xFFFFFFFFu, cv, 4);
                         cv += __shfl_xor_sync(0xFFFFFFFFu, cv, 8);
                         cv += __shfl_xor_sync(0xFFFFFFFFu, cv, 16);
-                        if (lane < 2) cpart[ew * TB + c * 32 + p + lane] = cv;
+                        if (lane < 2) cpart[cslot * TB + c * 32 + p + lane] = cv;
                     } else {
                         Rs[(row >> 1) * RLD + c * 32 + p + (grow ? 0 : 1)] = (float)r2u;
                     }
@@ -311,22 +319,24 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             if (ep.K == 1) {
                 rsum += __shfl_xor_sync(0xFFFFFFFFu, rsum, 1);
                 if (grow && kval && rsum != 0.0) atomicAdd(ep.l2 + k, rsum);
-                named_bar_sync(1, 128);
-                const int64_t j = j0 + et;
-                const double cs = cpart[et] + cpart[TB + et] + cpart[2 * TB + et] + cpart[3 * TB + et];
-                if (j < m && cs != 0.0) atomicAdd(ep.l2 + j, cs);
-                named_bar_sync(1, 128);
+                named_bar_sync(1, EPI_T);
+                if (et < TB) {
+                    const int64_t j = j0 + et;
+                    const double cs = cpart[et] + cpart[TB + et] + cpart[2 * TB + et] + cpart[3 * TB + et];
+                    if (j < m && cs != 0.0) atomicAdd(ep.l2 + j, cs);
+                }
+                named_bar_sync(1, EPI_T);
             } else {
                 // K > 1: the masked r2u tile goes to global memory for the
                 // banded annotation contraction (contract.cu)
-                named_bar_sync(1, 128);
+                named_bar_sync(1, EPI_T);
                 float4* dst = reinterpret_cast<float4*>(ep.rtiles + (size_t)t * TA * TB);
-                for (int q = et; q < TA * TB / 4; q += 128) {
+                for (int q = et; q < TA * TB / 4; q += EPI_T) {
                     const int e = q * 4, rr = e / TB, cc = e % TB;
                     dst[q] = make_float4(Rs[rr * RLD + cc], Rs[rr * RLD + cc + 1], Rs[rr * RLD + cc + 2],
                                          Rs[rr * RLD + cc + 3]);
                 }
-                named_bar_sync(1, 128);
+                named_bar_sync(1, EPI_T);
             }
             if (++acc == 2) {
                 acc = 0;
@@ -396,14 +406,14 @@ static cudaError_t launch_tc(const void* ops, CUtensorMapDataType dt, uint64_t e
         cudaError_t e = cudaFuncSetAttribute(k_gram_tc<4, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
         if (e != cudaSuccess) return e;
-        k_gram_tc<4, MODE><<<(unsigned)grid, NTHREADS, smem, stream>>>(tmA, tmB, num_kb, tiles,
+        k_gram_tc<4, MODE><<<(unsigned)grid, gram_threads(MODE), smem, stream>>>(tmA, tmB, num_kb, tiles,
                                                                        dbg ? 1 : n_tiles, ep, dbg);
     } else {
         const size_t smem = 1024 + 3 * (size_t)(A_BYTES + B_BYTES) + ctrl + cbytes + sizeof(float) * TA * RLD;
         cudaError_t e = cudaFuncSetAttribute(k_gram_tc<3, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
         if (e != cudaSuccess) return e;
-        k_gram_tc<3, MODE><<<(unsigned)grid, NTHREADS, smem, stream>>>(tmA, tmB, num_kb, tiles,
+        k_gram_tc<3, MODE><<<(unsigned)grid, gram_threads(MODE), smem, stream>>>(tmA, tmB, num_kb, tiles,
                                                                        dbg ? 1 : n_tiles, ep, dbg);
     }
     return cudaGetLastError();
