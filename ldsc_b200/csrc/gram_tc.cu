@@ -31,9 +31,11 @@
 //              UMMA issuer (tcgen05.mma kind::i8, M=128 N=256 K=32, four per stage)
 //   warps 2-5  epilogue: tcgen05.ld of the accumulator, exact r^2, band mask,
 //              l2 accumulation; accumulator double-buffering overlaps the
-//              epilogue of tile t with the MMAs of tile t+1.  The sketch
-//              forms (short K, a heavier per-pair correction) use warps 2-9:
-//              two warps per TMEM lane quarter, each on half the columns.
+//              epilogue of tile t with the MMAs of tile t+1.  Where the
+//              epilogue outweighs the MMAs -- the sketch forms (short K, a
+//              heavier per-pair correction) and INT8 rows of fewer than
+//              32,768 individuals -- warps 2-9 do it: two warps per TMEM lane
+//              quarter, each on half the columns.
 // Every mbarrier wait is bounded; on timeout the kernel records an error word,
 // drains its own in-flight copies / MMAs (bounded), frees TMEM and returns.
 #include <cuda.h>
@@ -51,8 +53,8 @@ constexpr int TA = 64;             // left records per tile (A rows = 128)
 constexpr int TB = 128;            // right records per tile (B rows = 256)
 constexpr int A_BYTES = 128 * 128; // one stage of A
 constexpr int B_BYTES = 256 * 128; // one stage of B
-// threads per CTA: TMA and MMA warps + 4 (INT8) or 8 (sketch) epilogue warps
-__host__ __device__ constexpr int gram_threads(int mode) { return mode == 0 ? 192 : 320; }
+// threads per CTA: TMA and MMA warps + ew epilogue warps (4 or 8)
+__host__ __device__ constexpr int gram_threads(int ew) { return 64 + 32 * ew; }
 constexpr int RLD = TB + 1;
 constexpr uint64_t WAIT_LIMIT_NS = 2000000000ull;  // 2 s per wait
 
@@ -75,8 +77,8 @@ __device__ __forceinline__ double sketch_r2u(float val, int64_t k, int64_t j, co
     return r2 * ep.r2u_a + ep.r2u_b;
 }
 
-template <int STAGES, int MODE>
-__global__ void __launch_bounds__(gram_threads(MODE), 1)
+template <int STAGES, int MODE, int EW>
+__global__ void __launch_bounds__(gram_threads(EW), 1)
     k_gram_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
               int num_kb, const Tile* __restrict__ tiles, int64_t n_tiles, EpilogueArgs ep,
               int32_t* __restrict__ dbg) {
@@ -105,7 +107,7 @@ __global__ void __launch_bounds__(gram_threads(MODE), 1)
         }
         for (int b = 0; b < 2; b++) {
             mbar_init(&tfull[b], 1);
-            mbar_init(&tempty[b], gram_threads(MODE) - 64);
+            mbar_init(&tempty[b], 32 * EW);
         }
         mbar_init(drain, 1);
         fence_mbar_init();
@@ -213,7 +215,7 @@ __global__ void __launch_bounds__(gram_threads(MODE), 1)
         }
     } else {
         // ------------------------------------------------ epilogue
-        constexpr int EPI_T = gram_threads(MODE) - 64;  // epilogue threads
+        constexpr int EPI_T = 32 * EW;                  // epilogue threads
         constexpr int CPW = 4 / (EPI_T / 128);          // 64-column chunks per warp
         const int et = threadIdx.x - 64;         // 0..EPI_T-1
         const int ew = et >> 5;                  // epilogue warp
@@ -384,6 +386,18 @@ static bool make_map(CUtensorMap* map, const void* base, CUtensorMapDataType dt,
     return r == CUDA_SUCCESS;
 }
 
+template <int STAGES, int MODE, int EW>
+static cudaError_t run_tc(const CUtensorMap& tmA, const CUtensorMap& tmB, int num_kb, const Tile* tiles,
+                          int64_t n_tiles, const EpilogueArgs& ep, int32_t* dbg, size_t smem, int64_t grid,
+                          cudaStream_t stream) {
+    cudaError_t e = cudaFuncSetAttribute(k_gram_tc<STAGES, MODE, EW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    k_gram_tc<STAGES, MODE, EW><<<(unsigned)grid, gram_threads(EW), smem, stream>>>(tmA, tmB, num_kb, tiles,
+                                                                                   dbg ? 1 : n_tiles, ep, dbg);
+    return cudaGetLastError();
+}
+
 template <int MODE>
 static cudaError_t launch_tc(const void* ops, CUtensorMapDataType dt, uint64_t elem_bytes, uint64_t ld_elems,
                              int64_t m, const Tile* tiles, int64_t n_tiles, const EpilogueArgs& ep, int32_t* dbg,
@@ -401,22 +415,18 @@ static cudaError_t launch_tc(const void* ops, CUtensorMapDataType dt, uint64_t e
     const size_t cbytes = sizeof(double) * 4 * TB;
     int64_t grid = n_tiles < sms ? n_tiles : sms;
     if (dbg) grid = 1;
+    // eight epilogue warps where the epilogue outweighs the MMAs
+    const bool wide = MODE != 0 || ld_elems * elem_bytes < 32768;
     if (ep.K == 1) {
         const size_t smem = 1024 + 4 * (size_t)(A_BYTES + B_BYTES) + ctrl + cbytes;
-        cudaError_t e = cudaFuncSetAttribute(k_gram_tc<4, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem);
-        if (e != cudaSuccess) return e;
-        k_gram_tc<4, MODE><<<(unsigned)grid, gram_threads(MODE), smem, stream>>>(tmA, tmB, num_kb, tiles,
-                                                                       dbg ? 1 : n_tiles, ep, dbg);
-    } else {
-        const size_t smem = 1024 + 3 * (size_t)(A_BYTES + B_BYTES) + ctrl + cbytes + sizeof(float) * TA * RLD;
-        cudaError_t e = cudaFuncSetAttribute(k_gram_tc<3, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem);
-        if (e != cudaSuccess) return e;
-        k_gram_tc<3, MODE><<<(unsigned)grid, gram_threads(MODE), smem, stream>>>(tmA, tmB, num_kb, tiles,
-                                                                       dbg ? 1 : n_tiles, ep, dbg);
+        if (MODE != 0 || wide)
+            return run_tc<4, MODE, 8>(tmA, tmB, num_kb, tiles, n_tiles, ep, dbg, smem, grid, stream);
+        return run_tc<4, MODE, MODE == 0 ? 4 : 8>(tmA, tmB, num_kb, tiles, n_tiles, ep, dbg, smem, grid, stream);
     }
-    return cudaGetLastError();
+    const size_t smem = 1024 + 3 * (size_t)(A_BYTES + B_BYTES) + ctrl + cbytes + sizeof(float) * TA * RLD;
+    if (MODE != 0 || wide)
+        return run_tc<3, MODE, 8>(tmA, tmB, num_kb, tiles, n_tiles, ep, dbg, smem, grid, stream);
+    return run_tc<3, MODE, MODE == 0 ? 4 : 8>(tmA, tmB, num_kb, tiles, n_tiles, ep, dbg, smem, grid, stream);
 }
 
 cudaError_t launch_gram_i8(const uint8_t* ops, uint64_t ld, int64_t m, const Tile* tiles, int64_t n_tiles,
