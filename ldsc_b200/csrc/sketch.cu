@@ -10,11 +10,11 @@
 //     S1_b  = sum_{i in b, present} sign_i g_i,   S0_b = sum_{i in b, present} sign_i,
 // two integer sums.  The bucket/sign map is the same for every SNP, so the
 // individuals are put once into bucket-major order (bucket, then sign):
-// k_sketch_permute rewrites every panel row in that order (2-bit codes, 16 per
-// word), after which each (bucket, sign) group is a contiguous run of
-// positions.  k_sketch_seg then streams a permuted row once and forms the
-// bucket sums from popcount prefix sums at the run boundaries (16 genotypes
-// per 32-bit word); the same popcounts give the per-SNP moments.
+// k_sketch_permute rewrites every panel row in that order (bit-plane quads of
+// 64 positions, sketch_quad.cuh), after which each (bucket, sign) group is a
+// contiguous run of positions.  k_sketch_seg then streams a permuted row once
+// and forms the bucket sums from popcount prefix sums at the run boundaries;
+// the same popcounts give the per-SNP moments.
 //
 // mean / inv_std are the reference's f32-rounded values; each bucket value is
 // formed exactly and rounded to f32 once (the reference accumulates f32 in
@@ -24,13 +24,13 @@
 #include <cuda_runtime.h>
 
 #include "engine.h"
+#include "sketch_quad.cuh"
 #include "sm100.cuh"
 
 namespace ldsc {
 
 namespace {
 
-constexpr uint32_t kEven = 0x55555555u;
 constexpr int NT = 256;
 
 template <typename T>
@@ -40,16 +40,17 @@ __device__ __forceinline__ T warp_sum(T v) {
     return v;
 }
 
-// Rewrite panel rows in bucket-major individual order.  perm[p] = FAM index
-// of the individual at permuted position p (p < n_used); positions past n_used
-// read as missing.  One CTA per row, the row staged in shared memory when it
-// fits (smem_row != 0).
+// Rewrite panel rows in bucket-major individual order, as bit-plane quads
+// (sketch_quad.cuh).  perm[p] = FAM index of the individual at permuted
+// position p (p < n_used); positions past n_used read as missing.  One CTA per
+// row, the row staged in shared memory when it fits (smem_row != 0); each
+// thread forms one 32-position half: its low-plane and high-plane words.
 __global__ void __launch_bounds__(NT) k_sketch_permute(PanelView p, const int32_t* __restrict__ perm,
                                                        uint64_t n_used, uint32_t* __restrict__ out,
                                                        uint64_t out_pitch_words, int smem_row) {
     extern __shared__ uint32_t srow32[];
     const uint8_t* srow = reinterpret_cast<const uint8_t*>(srow32);
-    const uint64_t words = (n_used + 15) / 16;
+    const uint64_t halves = out_pitch_words / 2;
     for (uint64_t r = blockIdx.x; r < p.n_snp; r += gridDim.x) {
         const uint8_t* row = p.rows + r * p.pitch;
         if (smem_row) {
@@ -59,51 +60,45 @@ __global__ void __launch_bounds__(NT) k_sketch_permute(PanelView p, const int32_
             __syncthreads();
         }
         const uint8_t* from = smem_row ? srow : row;
-        uint32_t* orow = out + r * out_pitch_words;
-        for (uint64_t w = threadIdx.x; w < out_pitch_words; w += NT) {
-            uint32_t word = 0x55555555u;
-            if (w < words) {
-                word = 0;
+        uint2* orow = reinterpret_cast<uint2*>(out + r * out_pitch_words);
+        for (uint64_t h = threadIdx.x; h < halves; h += NT) {
+            uint32_t lo = 0, hi = 0;
 #pragma unroll 4
-                for (int t = 0; t < 16; t++) {
-                    const uint64_t pos = w * 16 + t;
-                    uint32_t code = 1u;
-                    if (pos < n_used) {
-                        const int32_t iid = __ldg(perm + pos);
-                        code = (from[iid >> 2] >> ((iid & 3) * 2)) & 3u;
-                    }
-                    word |= code << (2 * t);
+            for (int t = 0; t < 32; t++) {
+                const uint64_t pos = h * 32 + t;
+                uint32_t code = 1u;  // missing
+                if (pos < n_used) {
+                    const int32_t iid = __ldg(perm + pos);
+                    code = (from[iid >> 2] >> ((iid & 3) * 2)) & 3u;
                 }
+                lo |= (code & 1u) << t;
+                hi |= (code >> 1) << t;
             }
-            orow[w] = word;
+            orow[h] = make_uint2(lo, hi);
         }
         __syncthreads();
     }
 }
 
-// Bucket sums from prefix sums.  Position p of the permuted row has
-//     g = 2 - (lo + hi) - miss,   present = 1 - miss
-// (codes 00 -> 2, 10 -> 1, 11 -> 0, 01 = missing -> 0), so over any span of
-// positions  sum g = 2 len - popc(bits) - popc(miss)  and  present = len -
-// popc(miss).  With the prefix (sum g, present) at every run boundary k,
-// bucket b is
+// Bucket sums from prefix sums.  Over any span of positions (quad counts in
+// sketch_quad.cuh)  sum g = 2 len - bits - missing  and  present = len -
+// missing.  With the prefix (sum g, present) at every run boundary k, bucket
+// b is
 //     S1_b = (PF[2b+1] - PF[2b]) - (PF[2b+2] - PF[2b+1])   (g sums; S0_b with present)
 // and row moments come from the totals:
 //     n = present, s = sum g, q = s + 2 #2, q3 = s + 6 #2, q4 = s + 14 #2
-// (#2 = number of genotype-2 codes).
+// (#2 = number of genotype-2 codes = len - high bits - missing).
 //
 // Two phases per record.  (1) Streaming: each warp owns a contiguous block of
 // the row's 16-byte quads and walks it 64 quads at a time, two adjacent quads
-// per lane (coalesced loads, branch-free popcounts); a warp scan gives the
-// prefix (popc, missing) at the start of every quad, kept in shared memory.
-// (2) Boundaries: after a block scan over the warps, thread t takes the
-// buckets [d t / NT, d (t+1) / NT) and walks their boundaries in order; each
-// prefix is the quad prefix plus popcounts inside one quad (re-read from
-// L1/L2, once per quad per thread), and each bucket's value is formed on the
-// spot.  No atomics, and nothing needs clearing between records.
-__device__ __forceinline__ uint32_t miss_bits(uint32_t x) { return x & ~(x >> 1) & kEven; }
-__device__ __forceinline__ uint32_t two_bits(uint32_t x) { return ~(x | (x >> 1)) & kEven; }
-
+// per lane (coalesced loads, branch-free popcounts); one warp scan of the
+// packed (bits, missing) counts gives the prefix at the start of every quad,
+// kept in shared memory.  (2) Boundaries: after a block scan over the warps,
+// thread t takes the buckets [d t / NT, d (t+1) / NT) and walks their
+// boundaries in order; each prefix is the quad prefix plus popcounts inside
+// one quad (re-read from L1/L2, once per quad per thread), and each bucket's
+// value is formed on the spot.  No atomics, and nothing needs clearing
+// between records.
 template <typename T>
 __device__ __forceinline__ T warp_incl_scan(T v, int lane) {
 #pragma unroll
@@ -150,8 +145,7 @@ __global__ void __launch_bounds__(SNT, 8) k_sketch_seg(const uint32_t* __restric
         const uint64_t brow = rec_rows ? rec_rows[r] : (uint64_t)r;
         const uint4* row = reinterpret_cast<const uint4*>(pp + brow * pp_pitch_words);
         // ---- phase 1: stream the warp's quads ----
-        int32_t carryA = 0, carryM = 0;
-        uint32_t T2 = 0;
+        int32_t carryA = 0, carryM = 0, HT = 0;
         uint4 n0 = make_uint4(0, 0, 0, 0), n1 = n0;
         if (wq0 + 2 * lane < wq1) n0 = __ldg(row + wq0 + 2 * lane);
         if (wq0 + 2 * lane + 1 < wq1) n1 = __ldg(row + wq0 + 2 * lane + 1);
@@ -161,41 +155,40 @@ __global__ void __launch_bounds__(SNT, 8) k_sketch_seg(const uint32_t* __restric
             const uint4 v0 = n0, v1 = n1;
             if (qa + CHUNK_Q < wq1) n0 = __ldg(row + qa + CHUNK_Q);
             if (qa + CHUNK_Q + 1 < wq1) n1 = __ldg(row + qa + CHUNK_Q + 1);
-            const int32_t a0 = __popc(v0.x) + __popc(v0.y) + __popc(v0.z) + __popc(v0.w);
-            const int32_t a1 = __popc(v1.x) + __popc(v1.y) + __popc(v1.z) + __popc(v1.w);
-            const int32_t m0 = __popc(miss_bits(v0.x) | (miss_bits(v0.y) << 1)) +
-                               __popc(miss_bits(v0.z) | (miss_bits(v0.w) << 1));
-            const int32_t m1 = __popc(miss_bits(v1.x) | (miss_bits(v1.y) << 1)) +
-                               __popc(miss_bits(v1.z) | (miss_bits(v1.w) << 1));
-            const uint32_t t0 = __popc(two_bits(v0.x) | (two_bits(v0.y) << 1)) +
-                                __popc(two_bits(v0.z) | (two_bits(v0.w) << 1));
-            const uint32_t t1 = __popc(two_bits(v1.x) | (two_bits(v1.y) << 1)) +
-                                __popc(two_bits(v1.z) | (two_bits(v1.w) << 1));
+            int32_t a0, m0, h0, a1, m1, h1;
+            quad_counts(v0, a0, m0, h0);
+            quad_counts(v1, a1, m1, h1);
             const int32_t la = (l0 ? a0 : 0) + (l1 ? a1 : 0), lm = (l0 ? m0 : 0) + (l1 ? m1 : 0);
-            T2 += (l0 ? t0 : 0u) + (l1 ? t1 : 0u);
-            const int32_t ia = warp_incl_scan(la, lane), im = warp_incl_scan(lm, lane);
+            HT += (l0 ? h0 : 0) + (l1 ? h1 : 0);
+            // (bits, missing) packed in 16-bit halves: a chunk holds at most
+            // 64 quads x 128 bits = 8,192, so the halves cannot carry
+            const int32_t lp = la | (lm << 16);
+            const int32_t ip = warp_incl_scan(lp, lane);
+            const int32_t ia = ip & 0xFFFF, im = ip >> 16;
             const int32_t ea = carryA + ia - la, em = carryM + im - lm;
             if (l0) Pq[qa] = make_int2(ea, em);
             if (l1) Pq[qa + 1] = make_int2(ea + a0, em + m0);
-            carryA += __shfl_sync(0xFFFFFFFFu, ia, 31);
-            carryM += __shfl_sync(0xFFFFFFFFu, im, 31);
+            const int32_t tp = __shfl_sync(0xFFFFFFFFu, ip, 31);
+            carryA += tp & 0xFFFF;
+            carryM += tp >> 16;
         }
-        const int32_t t2w = warp_sum((int32_t)T2);
+        const int32_t htw = warp_sum(HT);
         if (lane == 0) {
             wa[warp] = carryA;
             wm[warp] = carryM;
-            wt[warp] = t2w;
+            wt[warp] = htw;
         }
         __syncthreads();
         // ---- block scan over the warps: offsets and row totals ----
-        int32_t A = 0, MS = 0, TT = 0;
+        int32_t A = 0, MS = 0, H = 0;
 #pragma unroll
         for (int w = 0; w < SNW; w++) {
             A += wa[w];
             MS += wm[w];
-            TT += wt[w];
+            H += wt[w];
         }
-        const int32_t G = 2 * row_len - A - MS, N = row_len - MS;  // padding positions are missing: no effect
+        // padding positions are missing: no effect on G and N, and TT = #2
+        const int32_t G = 2 * row_len - A - MS, N = row_len - MS, TT = row_len - H - MS;
         if (threadIdx.x == 0) {
             st.n[r] = N;
             st.s[r] = G;
@@ -247,16 +240,10 @@ __global__ void __launch_bounds__(SNT, 8) k_sketch_seg(const uint32_t* __restric
                                 pa += wa[o];
                                 pm += wm[o];
                             }
-                        const uint4 v = qv[u];
-                        const int t = (p >> 4) & 3, j = p & 15;
-                        const uint32_t msk = j ? (0xFFFFFFFFu >> (32 - 2 * j)) : 0u;
-                        const uint32_t mk0 = t > 0 ? 0xFFFFFFFFu : (t == 0 ? msk : 0u);
-                        const uint32_t mk1 = t > 1 ? 0xFFFFFFFFu : (t == 1 ? msk : 0u);
-                        const uint32_t mk2 = t > 2 ? 0xFFFFFFFFu : (t == 2 ? msk : 0u);
-                        const uint32_t mk3 = t == 3 ? msk : 0u;
-                        pa += __popc(v.x & mk0) + __popc(v.y & mk1) + __popc(v.z & mk2) + __popc(v.w & mk3);
-                        pm += __popc(miss_bits(v.x) & mk0) + __popc(miss_bits(v.y) & mk1) +
-                              __popc(miss_bits(v.z) & mk2) + __popc(miss_bits(v.w) & mk3);
+                        int32_t ha, hm;
+                        quad_head(qv[u], (uint32_t)p & 63u, ha, hm);
+                        pa += ha;
+                        pm += hm;
                         pg = 2 * p - pa - pm;
                         pnr = p - pm;
                     }
@@ -306,11 +293,12 @@ __global__ void __launch_bounds__(SNT, 8) k_sketch_seg(const uint32_t* __restric
 //
 // With many buckets the boundary phase dominates and its quad re-reads go to
 // L2.  This form keeps the row's quads in shared memory and, per quad, the
-// prefix before it and the offsets of its words 1..3 inside it (8 bits each),
-// made block-absolute by a fix-up pass; thread t's boundary positions come
-// from a thread-major table (entry i * S6T + t = i-th boundary of thread t,
-// built once per layout), so their loads are coalesced, and each boundary
-// prefix costs two shared-memory loads and two popcounts.  256 threads per
+// prefix before it (made block-absolute by a fix-up pass) and the counts of
+// its first half; thread t's boundary positions come from a thread-major
+// table (entry i * S6T + t = i-th boundary of thread t, built once per
+// layout), so their loads are coalesced, and each boundary prefix costs two
+// shared-memory loads (the quad's prefix entry and its half's two plane
+// words) and three popcounts.  256 threads per
 // CTA: its shared memory (32 B per 64 individuals + 4 B per bucket) allows
 // few CTAs per SM, so each CTA brings more warps.  Same arithmetic as the
 // kernel above; results are bit-identical.
@@ -342,7 +330,7 @@ __global__ void __launch_bounds__(S6T, 2) k_sketch_seg6(const uint32_t* __restri
                                                       float* __restrict__ out, uint64_t ld) {
     extern __shared__ __align__(16) uint4 sh6[];
     const uint32_t quads = (uint32_t)sketch_quads(n_used);
-    uint4* PQ = sh6;          // prefix (popc, missing) before the quad, packed word offsets
+    uint4* PQ = sh6;          // (bits, missing) before the quad, then in its first half
     uint4* Rs = sh6 + quads;  // the quads
     float* ob = reinterpret_cast<float*>(sh6 + 2 * (size_t)quads);
     __shared__ int32_t wa[S6W], wm[S6W], wt[S6W];
@@ -355,8 +343,7 @@ __global__ void __launch_bounds__(S6T, 2) k_sketch_seg6(const uint32_t* __restri
         const uint64_t brow = rec_rows ? rec_rows[r] : (uint64_t)r;
         const uint4* row = reinterpret_cast<const uint4*>(pp + brow * pp_pitch_words);
         // ---- phase 1 ----
-        int32_t carryA = 0, carryM = 0;
-        uint32_t T2 = 0;
+        int32_t carryA = 0, carryM = 0, HT = 0;
         uint4 n0 = make_uint4(0, 0, 0, 0), n1 = n0;
         if (wq0 + 2 * lane < wq1) n0 = __ldg(row + wq0 + 2 * lane);
         if (wq0 + 2 * lane + 1 < wq1) n1 = __ldg(row + wq0 + 2 * lane + 1);
@@ -366,51 +353,35 @@ __global__ void __launch_bounds__(S6T, 2) k_sketch_seg6(const uint32_t* __restri
             const uint4 v0 = n0, v1 = n1;
             if (qa + CHUNK_Q < wq1) n0 = __ldg(row + qa + CHUNK_Q);
             if (qa + CHUNK_Q + 1 < wq1) n1 = __ldg(row + qa + CHUNK_Q + 1);
-            const uint32_t x[8] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y, v1.z, v1.w};
-            int32_t ca[8], cm[8];
-#pragma unroll
-            for (int t = 0; t < 8; t++) {
-                ca[t] = __popc(x[t]);
-                cm[t] = __popc(miss_bits(x[t]));
-            }
-            const uint32_t t0 = __popc(two_bits(x[0]) | (two_bits(x[1]) << 1)) +
-                                __popc(two_bits(x[2]) | (two_bits(x[3]) << 1));
-            const uint32_t t1 = __popc(two_bits(x[4]) | (two_bits(x[5]) << 1)) +
-                                __popc(two_bits(x[6]) | (two_bits(x[7]) << 1));
-            const int32_t a0 = ca[0] + ca[1] + ca[2] + ca[3], a1 = ca[4] + ca[5] + ca[6] + ca[7];
-            const int32_t m0 = cm[0] + cm[1] + cm[2] + cm[3], m1 = cm[4] + cm[5] + cm[6] + cm[7];
+            int32_t a0, m0, h0, fa0, fm0, a1, m1, h1, fa1, fm1;
+            quad_counts(v0, a0, m0, h0, fa0, fm0);
+            quad_counts(v1, a1, m1, h1, fa1, fm1);
             const int32_t la = (l0 ? a0 : 0) + (l1 ? a1 : 0), lm = (l0 ? m0 : 0) + (l1 ? m1 : 0);
-            T2 += (l0 ? t0 : 0u) + (l1 ? t1 : 0u);
-            const int32_t ia = warp_incl_scan(la, lane), im = warp_incl_scan(lm, lane);
+            HT += (l0 ? h0 : 0) + (l1 ? h1 : 0);
+            const int32_t lp = la | (lm << 16);  // at most 8,192 bits per chunk: no carry
+            const int32_t ip = warp_incl_scan(lp, lane);
+            const int32_t ia = ip & 0xFFFF, im = ip >> 16;
             const int32_t ea = carryA + ia - la, em = carryM + im - lm;
-            // offsets of words 1..3 inside each quad, byte t for word t (byte 0 = 0)
-            const uint32_t pa0 = ((uint32_t)ca[0] << 8) | ((uint32_t)(ca[0] + ca[1]) << 16) |
-                                 ((uint32_t)(ca[0] + ca[1] + ca[2]) << 24);
-            const uint32_t pm0 = ((uint32_t)cm[0] << 8) | ((uint32_t)(cm[0] + cm[1]) << 16) |
-                                 ((uint32_t)(cm[0] + cm[1] + cm[2]) << 24);
-            const uint32_t pa1 = ((uint32_t)ca[4] << 8) | ((uint32_t)(ca[4] + ca[5]) << 16) |
-                                 ((uint32_t)(ca[4] + ca[5] + ca[6]) << 24);
-            const uint32_t pm1 = ((uint32_t)cm[4] << 8) | ((uint32_t)(cm[4] + cm[5]) << 16) |
-                                 ((uint32_t)(cm[4] + cm[5] + cm[6]) << 24);
             if (l0) {
-                PQ[qa] = make_uint4((uint32_t)ea, (uint32_t)em, pa0, pm0);
+                PQ[qa] = make_uint4((uint32_t)ea, (uint32_t)em, (uint32_t)fa0, (uint32_t)fm0);
                 Rs[qa] = v0;
             }
             if (l1) {
-                PQ[qa + 1] = make_uint4((uint32_t)(ea + a0), (uint32_t)(em + m0), pa1, pm1);
+                PQ[qa + 1] = make_uint4((uint32_t)(ea + a0), (uint32_t)(em + m0), (uint32_t)fa1, (uint32_t)fm1);
                 Rs[qa + 1] = v1;
             }
-            carryA += __shfl_sync(0xFFFFFFFFu, ia, 31);
-            carryM += __shfl_sync(0xFFFFFFFFu, im, 31);
+            const int32_t tp = __shfl_sync(0xFFFFFFFFu, ip, 31);
+            carryA += tp & 0xFFFF;
+            carryM += tp >> 16;
         }
-        const int32_t t2w = warp_sum((int32_t)T2);
+        const int32_t htw = warp_sum(HT);
         if (lane == 0) {
             wa[warp] = carryA;
             wm[warp] = carryM;
-            wt[warp] = t2w;
+            wt[warp] = htw;
         }
         __syncthreads();
-        int32_t A = 0, MS = 0, TT = 0, offA = 0, offM = 0;
+        int32_t A = 0, MS = 0, H = 0, offA = 0, offM = 0;
 #pragma unroll
         for (int w = 0; w < S6W; w++) {
             if (w < warp) {
@@ -419,9 +390,9 @@ __global__ void __launch_bounds__(S6T, 2) k_sketch_seg6(const uint32_t* __restri
             }
             A += wa[w];
             MS += wm[w];
-            TT += wt[w];
+            H += wt[w];
         }
-        const int32_t G = 2 * row_len - A - MS, N = row_len - MS;
+        const int32_t G = 2 * row_len - A - MS, N = row_len - MS, TT = row_len - H - MS;
         if (threadIdx.x == 0) {
             st.n[r] = N;
             st.s[r] = G;
@@ -447,7 +418,7 @@ __global__ void __launch_bounds__(S6T, 2) k_sketch_seg6(const uint32_t* __restri
         // ---- phase 2 ----
         double part = 0.0;
         if (nbd) {
-            const uint32_t* rw = reinterpret_cast<const uint32_t*>(Rs);
+            const uint2* rh = reinterpret_cast<const uint2*>(Rs);  // (low, high) plane words of each half
             int32_t pn[4];
 #pragma unroll
             for (int u = 0; u < 4; u++) pn[u] = (uint32_t)u < nbd ? __ldg(segt + u * S6T + threadIdx.x) : row_len;
@@ -465,13 +436,13 @@ __global__ void __launch_bounds__(S6T, 2) k_sketch_seg6(const uint32_t* __restri
                     const int32_t p = pc[u];
                     int32_t pg = G, pnr = N;  // at the row end: the totals
                     if (p < row_len) {
-                        const uint32_t q = (uint32_t)p >> 6, tw = ((uint32_t)p >> 4) & 3u, j = (uint32_t)p & 15u;
+                        const uint32_t q = (uint32_t)p >> 6, hf = ((uint32_t)p >> 5) & 1u;
                         const uint4 e = PQ[q];
-                        const uint32_t y = rw[4 * q + tw];
-                        const uint32_t msk = j ? (0xFFFFFFFFu >> (32 - 2 * j)) : 0u;
-                        const int32_t pa = (int32_t)e.x + (int32_t)((e.z >> (8 * tw)) & 0xFFu) + __popc(y & msk);
-                        const int32_t pm = (int32_t)e.y + (int32_t)((e.w >> (8 * tw)) & 0xFFu) +
-                                           __popc(miss_bits(y) & msk);
+                        const uint2 lh = rh[2 * q + hf];
+                        int32_t ha, hm;
+                        half_head(lh.x, lh.y, (uint32_t)p & 31u, ha, hm);
+                        const int32_t pa = (int32_t)e.x + (hf ? (int32_t)e.z : 0) + ha;
+                        const int32_t pm = (int32_t)e.y + (hf ? (int32_t)e.w : 0) + hm;
                         pg = 2 * p - pa - pm;
                         pnr = p - pm;
                     }
