@@ -488,12 +488,9 @@ int sketch_prepare(ldsc_ctx* ctx, const ldsc_panel* panel, uint64_t n_used, uint
     CK(cudaMemcpyAsync(c.seg.p, o.seg_off.data(), 4 * o.seg_off.size(), cudaMemcpyHostToDevice, s));
     PanelView pv{panel->rows, panel->n_snp, panel->n_indiv, panel->bpr, panel->pitch};
     CK(launch_sketch_permute(pv, c.perm.as<int32_t>(), n_used, c.pp.as<uint32_t>(), pitch_words, s));
-    if (sketch_large_d(n_used, d)) {
-        CK(c.segt.ensure(4 * (size_t)sketch_segt_count(d)));
-        CK(launch_sketch_segt(c.seg.as<int32_t>(), d, c.segt.as<int32_t>(), s));
-        ctx->kernels++;
-    }
-    ctx->kernels++;
+    CK(c.segt.ensure(4 * (size_t)sketch_segt_count(n_used, d)));
+    CK(launch_sketch_segt(c.seg.as<int32_t>(), n_used, d, c.segt.as<int32_t>(), s));
+    ctx->kernels += 2;
     // host vectors go out of scope, and other streams may read the layout next
     CK(cudaStreamSynchronize(s));
     c.n = n_used;
@@ -920,9 +917,8 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
     } else if (d) {
         // fused: moments + CountSketch rows in one pass over the permuted panel
         CK(launch_sketch_seg(skc->pp.as<uint32_t>() + (rr ? 0 : a->row_begin * skc->pitch_words), skc->pitch_words,
-                             rr, m, n_used, skc->seg.as<int32_t>(),
-                             sketch_large_d(n_used, d) ? skc->segt.as<int32_t>() : nullptr, d, st,
-                             maf_aware ? 1 : 0, 1, ctx->xsk.as<float>(), ld_sk, s));
+                             rr, m, n_used, skc->segt.as<int32_t>(), d, st, maf_aware ? 1 : 0, 1,
+                             ctx->xsk.as<float>(), ld_sk, s));
         e_sk = ev.mark();
     } else {
         CK(launch_decode_i8(pv, rr, m, sel, nullptr, 0, st, 0, s));
@@ -1168,8 +1164,7 @@ int ldsc_sketch_project(ldsc_ctx* ctx, const ldsc_panel* panel, uint64_t b, uint
     st.s = ctx->st_s.as<int32_t>();
     st.q = ctx->st_q.as<int32_t>();
     CK(launch_sketch_seg(ctx->sk.pp.as<uint32_t>(), ctx->sk.pitch_words, ctx->recrows.as<uint64_t>(), m, n_used,
-                         ctx->sk.seg.as<int32_t>(), sketch_large_d(n_used, d) ? ctx->sk.segt.as<int32_t>() : nullptr,
-                         d, st, 0, 0, ctx->xsk.as<float>(), d, s));
+                         ctx->sk.segt.as<int32_t>(), d, st, 0, 0, ctx->xsk.as<float>(), d, s));
     ctx->kernels += 1;
     CK(cudaMemcpyAsync(out, ctx->xsk.p, 4 * (size_t)m * d, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));

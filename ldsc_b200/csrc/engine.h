@@ -105,28 +105,28 @@ cudaError_t launch_gram_i8(const uint8_t* ops, uint64_t ld, int64_t m, const Til
 // CountSketch, step 1 (once per panel, sketch dimension and individual set):
 // rewrite every panel row in bucket-major individual order, perm[p] = FAM
 // index of the individual at permuted position p.  out: n_snp rows of
-// out_pitch_words 32-bit words (16 codes each).
+// out_pitch_words 32-bit words, bit-plane quads of 64 positions.
 cudaError_t launch_sketch_permute(const PanelView& p, const int32_t* perm, uint64_t n_used, uint32_t* out,
                                   uint64_t out_pitch_words, cudaStream_t stream);
 
 // CountSketch, step 2 (per call): per record, run sums over the permuted row,
 // per-SNP moments into st.n/s/q (and q3/q4 when want_moments), standardised
-// and renormalised bucket values.  seg_off: 2d+1 run starts (run k = bucket
-// k/2, sign + for even k).
+// and renormalised bucket values.  segt: the layout's thread-major boundary
+// table (launch_sketch_segt) for this n_used and d; large d (sketch_large_d)
+// runs the shared-memory-row form.
 // out: m rows of `ld` floats, or with split = 1 the tensor-core operand form:
 // rows 2r = tf32(v) and 2r+1 = tf32(v - tf32(v)), `ld` floats each.
-// segt (may be null): the layout's thread-major boundary table
-// (launch_sketch_segt); with it, large d (sketch_large_d) runs the
-// shared-memory-row form.
 cudaError_t launch_sketch_seg(const uint32_t* pp, uint64_t pp_pitch_words, const uint64_t* rec_rows, int64_t m,
-                              uint64_t n_used, const int32_t* seg_off, const int32_t* segt, uint32_t d, RecStats st,
-                              int want_moments, int split, float* out, uint64_t ld, cudaStream_t stream);
-// Whether d and n_used take the large-d form (d >= 2048 and its shared memory fits).
+                              uint64_t n_used, const int32_t* segt, uint32_t d, RecStats st, int want_moments,
+                              int split, float* out, uint64_t ld, cudaStream_t stream);
+// Whether d and n_used take the large-d form (d >= 2560 and its shared memory fits).
 bool sketch_large_d(uint64_t n_used, uint32_t d);
-// Entries of the thread-major boundary table, and its construction from the
-// 2d + 1 run starts (once per layout).
-uint64_t sketch_segt_count(uint32_t d);
-cudaError_t launch_sketch_segt(const int32_t* seg_off, uint32_t d, int32_t* segt, cudaStream_t stream);
+// Entries of the thread-major boundary table, and its construction (once per
+// layout) from seg_off, the 2d + 1 run starts (run k = bucket k/2, sign + for
+// even k).
+uint64_t sketch_segt_count(uint64_t n_used, uint32_t d);
+cudaError_t launch_sketch_segt(const int32_t* seg_off, uint64_t n_used, uint32_t d, int32_t* segt,
+                               cudaStream_t stream);
 // Whether the sketch kernel's shared memory holds n_used individuals and d buckets.
 bool sketch_supported(uint64_t n_used, uint32_t d);
 

@@ -95,10 +95,13 @@ __global__ void __launch_bounds__(NT) k_sketch_permute(PanelView p, const int32_
 // packed (bits, missing) counts gives the prefix at the start of every quad,
 // kept in shared memory.  (2) Boundaries: after a block scan over the warps,
 // thread t takes the buckets [d t / NT, d (t+1) / NT) and walks their
-// boundaries in order; each prefix is the quad prefix plus popcounts inside
-// one quad (re-read from L1/L2, once per quad per thread), and each bucket's
-// value is formed on the spot.  No atomics, and nothing needs clearing
-// between records.
+// boundaries in order; each prefix is the quad prefix, plus the offset of the
+// warp that streamed the quad, plus popcounts inside the quad (re-read from
+// L1/L2).  Thread t's boundary positions come from a thread-major table built
+// once per layout (entry i * NT + t = its i-th boundary, with the owning warp
+// in the top bits), so their loads are coalesced.  Each bucket's value is
+// formed on the spot.  No atomics, and nothing needs clearing between
+// records.
 template <typename T>
 __device__ __forceinline__ T warp_incl_scan(T v, int lane) {
 #pragma unroll
@@ -115,6 +118,22 @@ constexpr int CHUNK_Q = 64;    // quads per warp step (2 per lane)
 
 __host__ __device__ inline uint64_t sketch_quads(uint64_t n_used) { return ((n_used + 15) / 16 + 3) / 4; }
 
+// Thread t of a T-thread CTA takes buckets [seg_b(d, t), seg_b(d, t + 1)):
+// 2 (b1 - b0) + 1 boundaries; seg_rows bounds that count over t.
+template <int T>
+__host__ __device__ inline uint32_t seg_b(uint32_t d, uint32_t t) { return (uint32_t)((uint64_t)d * t / T); }
+template <int T>
+__host__ __device__ inline uint32_t seg_count(uint32_t d, uint32_t t) {
+    const uint32_t b0 = seg_b<T>(d, t), b1 = seg_b<T>(d, t + 1);
+    return b0 < b1 ? 2 * (b1 - b0) + 1 : 0;
+}
+template <int T>
+__host__ __device__ inline uint32_t seg_rows(uint32_t d) { return 2 * ((d + T - 1) / T) + 1; }
+
+// Boundary table entry of the streaming-form kernel: position | owning warp << 28.
+constexpr int SEG_POS_BITS = 28;
+constexpr int32_t SEG_POS_MASK = (1 << SEG_POS_BITS) - 1;
+
 // Dynamic shared memory of the sketch kernel: per-quad prefixes and the d
 // bucket values.
 __host__ __device__ inline size_t sketch_smem(uint64_t n_used, uint32_t d) {
@@ -125,7 +144,7 @@ __host__ __device__ inline size_t sketch_smem(uint64_t n_used, uint32_t d) {
 // (zero padded past d), or with split the hi/lo tensor-core rows 2r / 2r+1.
 __global__ void __launch_bounds__(SNT, 8) k_sketch_seg(const uint32_t* __restrict__ pp, uint64_t pp_pitch_words,
                                                     const uint64_t* __restrict__ rec_rows, int64_t m, uint64_t n_used,
-                                                    const int32_t* __restrict__ seg_off, uint32_t d, RecStats st,
+                                                    const int32_t* __restrict__ segt, uint32_t d, RecStats st,
                                                     int want_moments, int split, float* __restrict__ out,
                                                     uint64_t ld) {
     extern __shared__ __align__(16) int32_t sh[];
@@ -133,14 +152,12 @@ __global__ void __launch_bounds__(SNT, 8) k_sketch_seg(const uint32_t* __restric
     int2* Pq = reinterpret_cast<int2*>(sh);                  // (popc, missing) before each quad, warp-relative
     float* ob = reinterpret_cast<float*>(sh + 2 * quads);    // bucket values
     __shared__ int32_t wa[SNW], wm[SNW], wt[SNW];
+    __shared__ int2 woff[SNW];  // (bits, missing) before each warp's block
     __shared__ double dred[SNW];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t wq0 = (uint32_t)((uint64_t)quads * warp / SNW), wq1 = (uint32_t)((uint64_t)quads * (warp + 1) / SNW);
-    const uint32_t b0 = (uint32_t)((uint64_t)d * threadIdx.x / SNT), b1 = (uint32_t)((uint64_t)d * (threadIdx.x + 1) / SNT);
+    const uint32_t b0 = seg_b<SNT>(d, threadIdx.x), nbd = seg_count<SNT>(d, threadIdx.x);
     const int32_t row_len = (int32_t)(64 * quads);
-    __shared__ uint32_t wstart[SNW];  // first quad of each warp's block
-    if (threadIdx.x < SNW) wstart[threadIdx.x] = (uint32_t)((uint64_t)quads * threadIdx.x / SNW);
-    __syncthreads();
     for (int64_t r = blockIdx.x; r < m; r += gridDim.x) {
         const uint64_t brow = rec_rows ? rec_rows[r] : (uint64_t)r;
         const uint4* row = reinterpret_cast<const uint4*>(pp + brow * pp_pitch_words);
@@ -204,50 +221,54 @@ __global__ void __launch_bounds__(SNT, 8) k_sketch_seg(const uint32_t* __restric
         const double sd = sqrt(css / (double)n_used);
         const double mean = (double)(float)dmean;
         const double inv = sd > 0.0 ? (double)(float)(1.0 / sd) : 0.0;
+        if (threadIdx.x < SNW) {
+            int32_t oa = 0, om = 0;
+#pragma unroll
+            for (int w = 0; w < SNW - 1; w++)
+                if (w < (int)threadIdx.x) {
+                    oa += wa[w];
+                    om += wm[w];
+                }
+            woff[threadIdx.x] = make_int2(oa, om);
+        }
+        __syncthreads();
         // ---- phase 2: this thread's buckets ----
-        // Boundaries 2 b0 .. 2 b1 in groups of four: the group's positions are
-        // loaded one group ahead and its four quads are loaded together.
+        // Boundaries in groups of four: the group's table entries are loaded
+        // one group ahead and its four quads are loaded together.
         double part = 0.0;
-        if (b0 < b1) {
-            const uint32_t kb = 2 * b0, ke = 2 * b1 + 1;
+        if (nbd) {
             int32_t pn[4];
 #pragma unroll
-            for (int u = 0; u < 4; u++) pn[u] = kb + u < ke ? __ldg(seg_off + kb + u) : row_len;
+            for (int u = 0; u < 4; u++) pn[u] = (uint32_t)u < nbd ? __ldg(segt + u * SNT + threadIdx.x) : row_len;
             int32_t g1 = 0, n1w = 0, g2 = 0, n2w = 0;  // prefixes at the previous two boundaries
-            for (uint32_t k = kb; k < ke; k += 4) {
+            for (uint32_t i = 0; i < nbd; i += 4) {
                 int32_t pc[4];
                 uint4 qv[4];
 #pragma unroll
                 for (int u = 0; u < 4; u++) {
                     pc[u] = pn[u];
-                    pn[u] = k + 4 + u < ke ? __ldg(seg_off + k + 4 + u) : row_len;
+                    pn[u] = i + 4 + u < nbd ? __ldg(segt + (i + 4 + u) * SNT + threadIdx.x) : row_len;
                 }
 #pragma unroll
-                for (int u = 0; u < 4; u++) qv[u] = pc[u] < row_len ? __ldg(row + (pc[u] >> 6)) : make_uint4(0, 0, 0, 0);
+                for (int u = 0; u < 4; u++) {
+                    const int32_t p = pc[u] & SEG_POS_MASK;
+                    qv[u] = p < row_len ? __ldg(row + (p >> 6)) : make_uint4(0, 0, 0, 0);
+                }
 #pragma unroll
                 for (int u = 0; u < 4; u++) {
-                    if (k + u >= ke) break;
-                    const int32_t p = pc[u];
+                    if (i + u >= nbd) break;
+                    const int32_t p = pc[u] & SEG_POS_MASK;
                     int32_t pg = G, pnr = N;  // at or past the row end: the totals
                     if (p < row_len) {
-                        const uint32_t q = (uint32_t)p >> 6;
-                        // plus the offset of the warp that owns quad q
-                        const int2 pq = Pq[q];
-                        int32_t pa = pq.x, pm = pq.y;
-#pragma unroll
-                        for (int o = 0; o < SNW - 1; o++)
-                            if (q >= wstart[o + 1]) {
-                                pa += wa[o];
-                                pm += wm[o];
-                            }
+                        // quad prefix + offset of the warp that streamed the quad + inside the quad
+                        const int2 pq = Pq[p >> 6], of = woff[(uint32_t)pc[u] >> SEG_POS_BITS];
                         int32_t ha, hm;
                         quad_head(qv[u], (uint32_t)p & 63u, ha, hm);
-                        pa += ha;
-                        pm += hm;
+                        const int32_t pa = pq.x + of.x + ha, pm = pq.y + of.y + hm;
                         pg = 2 * p - pa - pm;
                         pnr = p - pm;
                     }
-                    const uint32_t idx = k + u - kb;
+                    const uint32_t idx = i + u;
                     if (idx >= 2 && !(idx & 1)) {  // bucket b0 + idx/2 - 1 is complete
                         const int32_t s1 = (g1 - g2) - (pg - g1), s0 = (n1w - n2w) - (pnr - n1w);
                         const float o = (float)(inv * ((double)s1 - mean * (double)s0));
@@ -305,25 +326,35 @@ __global__ void __launch_bounds__(SNT, 8) k_sketch_seg(const uint32_t* __restric
 constexpr int S6T = 256;
 constexpr int S6W = S6T / 32;
 
-__host__ __device__ inline uint32_t seg6_b(uint32_t d, uint32_t t) { return (uint32_t)((uint64_t)d * t / S6T); }
-__host__ __device__ inline uint32_t seg6_count(uint32_t d, uint32_t t) {
-    const uint32_t b0 = seg6_b(d, t), b1 = seg6_b(d, t + 1);
-    return b0 < b1 ? 2 * (b1 - b0) + 1 : 0;
-}
-__host__ __device__ inline uint32_t seg6_rows(uint32_t d) { return 2 * ((d + S6T - 1) / S6T) + 1; }
 __host__ __device__ inline size_t sketch6_smem(uint64_t n_used, uint32_t d) {
     return 32 * sketch_quads(n_used) + 4 * (size_t)d + 16;
 }
 
-__global__ void k_sketch_segt(const int32_t* __restrict__ seg_off, uint32_t d, uint32_t rows,
+// Thread-major boundary table for a T-thread kernel: entry i * T + t = the
+// i-th boundary position of thread t (0x7FFFFFFF past its count); with
+// owners, the streaming-form entry (position | owning warp << 28, the warp
+// of SNW whose block holds the position's quad).
+template <int T, bool OWNERS>
+__global__ void k_sketch_segt(const int32_t* __restrict__ seg_off, uint32_t d, uint32_t rows, uint32_t quads,
                               int32_t* __restrict__ segt) {
-    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < rows * S6T; e += gridDim.x * blockDim.x) {
-        const uint32_t i = e / S6T, t = e % S6T;
-        segt[e] = i < seg6_count(d, t) ? seg_off[2 * seg6_b(d, t) + i] : 0x7FFFFFFF;
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < rows * T; e += gridDim.x * blockDim.x) {
+        const uint32_t i = e / T, t = e % T;
+        int32_t v = 0x7FFFFFFF;
+        if (i < seg_count<T>(d, t)) {
+            v = seg_off[2 * seg_b<T>(d, t) + i];
+            if (OWNERS) {
+                const uint64_t q = (uint64_t)v >> 6;
+                int32_t w = 0;
+                for (int o = 1; o < SNW; o++)
+                    if (q >= (uint64_t)quads * o / SNW) w = o;
+                v |= w << SEG_POS_BITS;
+            }
+        }
+        segt[e] = v;
     }
 }
 
-__global__ void __launch_bounds__(S6T, 2) k_sketch_seg6(const uint32_t* __restrict__ pp, uint64_t pp_pitch_words,
+__global__ void __launch_bounds__(S6T, 3) k_sketch_seg6(const uint32_t* __restrict__ pp, uint64_t pp_pitch_words,
                                                       const uint64_t* __restrict__ rec_rows, int64_t m,
                                                       uint64_t n_used, const int32_t* __restrict__ segt, uint32_t d,
                                                       RecStats st, int want_moments, int split,
@@ -337,7 +368,7 @@ __global__ void __launch_bounds__(S6T, 2) k_sketch_seg6(const uint32_t* __restri
     __shared__ double dred[S6W];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t wq0 = (uint32_t)((uint64_t)quads * warp / S6W), wq1 = (uint32_t)((uint64_t)quads * (warp + 1) / S6W);
-    const uint32_t b0 = seg6_b(d, threadIdx.x), nbd = seg6_count(d, threadIdx.x);
+    const uint32_t b0 = seg_b<S6T>(d, threadIdx.x), nbd = seg_count<S6T>(d, threadIdx.x);
     const int32_t row_len = (int32_t)(64 * quads);
     for (int64_t r = blockIdx.x; r < m; r += gridDim.x) {
         const uint64_t brow = rec_rows ? rec_rows[r] : (uint64_t)r;
@@ -504,13 +535,18 @@ cudaError_t launch_sketch_permute(const PanelView& p, const int32_t* perm, uint6
 }
 
 cudaError_t launch_sketch_seg(const uint32_t* pp, uint64_t pp_pitch_words, const uint64_t* rec_rows, int64_t m,
-                              uint64_t n_used, const int32_t* seg_off, const int32_t* segt, uint32_t d, RecStats st,
-                              int want_moments, int split, float* out, uint64_t ld, cudaStream_t stream) {
+                              uint64_t n_used, const int32_t* segt, uint32_t d, RecStats st, int want_moments,
+                              int split, float* out, uint64_t ld, cudaStream_t stream) {
     if (m <= 0) return cudaSuccess;
     const int64_t grid = m < 148 * 16 ? m : 148 * 16;
-    if (segt && sketch_large_d(n_used, d)) {
+    if (sketch_large_d(n_used, d)) {
         const size_t smem6 = sketch6_smem(n_used, d);
         cudaError_t e = cudaFuncSetAttribute(k_sketch_seg6, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem6);
+        if (e != cudaSuccess) return e;
+        // three 256-thread CTAs per SM: their rows and prefixes need the
+        // largest shared-memory carveout
+        e = cudaFuncSetAttribute(k_sketch_seg6, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared);
         if (e != cudaSuccess) return e;
         k_sketch_seg6<<<(unsigned)grid, S6T, smem6, stream>>>(pp, pp_pitch_words, rec_rows, m, n_used, segt, d, st,
                                                                want_moments, split, out, ld);
@@ -522,20 +558,29 @@ cudaError_t launch_sketch_seg(const uint32_t* pp, uint64_t pp_pitch_words, const
         cudaError_t e = cudaFuncSetAttribute(k_sketch_seg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
-    k_sketch_seg<<<(unsigned)grid, SNT, smem, stream>>>(pp, pp_pitch_words, rec_rows, m, n_used, seg_off, d, st,
+    k_sketch_seg<<<(unsigned)grid, SNT, smem, stream>>>(pp, pp_pitch_words, rec_rows, m, n_used, segt, d, st,
                                                        want_moments, split, out, ld);
     return cudaGetLastError();
 }
 
 bool sketch_supported(uint64_t n_used, uint32_t d) { return sketch_smem(n_used, d) <= 200 * 1024; }
 
-bool sketch_large_d(uint64_t n_used, uint32_t d) { return d >= 2048 && sketch6_smem(n_used, d) <= 200 * 1024; }
+// Measured at N = 100,000: the streaming form is faster up to d ~ 2,600, the
+// shared-memory-row form above (d = 2,500: 0.50 vs 0.52 ms per 20,000 rows;
+// d = 3,000: 0.63 vs 0.57 ms).
+bool sketch_large_d(uint64_t n_used, uint32_t d) { return d >= 2560 && sketch6_smem(n_used, d) <= 200 * 1024; }
 
-uint64_t sketch_segt_count(uint32_t d) { return (uint64_t)seg6_rows(d) * S6T; }
+uint64_t sketch_segt_count(uint64_t n_used, uint32_t d) {
+    return sketch_large_d(n_used, d) ? (uint64_t)seg_rows<S6T>(d) * S6T : (uint64_t)seg_rows<SNT>(d) * SNT;
+}
 
-cudaError_t launch_sketch_segt(const int32_t* seg_off, uint32_t d, int32_t* segt, cudaStream_t stream) {
-    const uint32_t rows = seg6_rows(d);
-    k_sketch_segt<<<64, 256, 0, stream>>>(seg_off, d, rows, segt);
+cudaError_t launch_sketch_segt(const int32_t* seg_off, uint64_t n_used, uint32_t d, int32_t* segt,
+                               cudaStream_t stream) {
+    const uint32_t quads = (uint32_t)sketch_quads(n_used);
+    if (sketch_large_d(n_used, d))
+        k_sketch_segt<S6T, false><<<64, 256, 0, stream>>>(seg_off, d, seg_rows<S6T>(d), quads, segt);
+    else
+        k_sketch_segt<SNT, true><<<64, 256, 0, stream>>>(seg_off, d, seg_rows<SNT>(d), quads, segt);
     return cudaGetLastError();
 }
 

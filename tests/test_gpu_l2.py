@@ -232,11 +232,12 @@ def test_small_config_parity(ctx, cfg_small, masking):
         np.testing.assert_allclose(maf, ref_maf, atol=1e-15)
 
 
-@pytest.mark.parametrize("d", [3, 200, 5000])
+@pytest.mark.parametrize("d", [3, 200, 2559, 2560, 5000])
 def test_sketch_project_large_panel(ctx, d):
     """Bucket sums over a 20,000-individual panel with the seed-42 stream
-    (runs shorter and longer than a thread's word range) vs a direct f64
-    scatter; the tolerance is the reference scatter test's (1e-4)."""
+    (runs shorter and longer than a thread's word range; both kernel forms,
+    either side of the d = 2,560 switch) vs a direct f64 scatter; the
+    tolerance is the reference scatter test's (1e-4)."""
     from ldsc_b200.api import countsketch_hash, sketch_project
     from ldsc_b200.plink import decode_genotypes
     spec = synth.PanelSpec(n_indiv=20011, chrom_sizes=[6], chrom_cm=[1.0], founders=30, miss=0.03, seed=8)
