@@ -134,10 +134,40 @@ __host__ __device__ inline uint32_t seg_rows(uint32_t d) { return 2 * ((d + T - 
 constexpr int SEG_POS_BITS = 28;
 constexpr int32_t SEG_POS_MASK = (1 << SEG_POS_BITS) - 1;
 
-// Dynamic shared memory of the sketch kernel: per-quad prefixes and the d
-// bucket values.
+// Dynamic shared memory of the sketch kernel: per-quad prefixes (an even
+// count, so the bucket values start on 16 bytes) and the d bucket values
+// (+16 bytes read past d by the vector output loop).
 __host__ __device__ inline size_t sketch_smem(uint64_t n_used, uint32_t d) {
-    return 8 * sketch_quads(n_used) + 4 * (size_t)d + 16;
+    return 8 * ((sketch_quads(n_used) + 1) & ~1ull) + 4 * (size_t)d + 16;
+}
+
+// Record r's output from the bucket values ob (16-byte aligned): `ld` floats
+// (zero padded past d), or with split the tensor-core operand rows
+// 2r = tf32(v) and 2r+1 = tf32(v - tf32(v)), stored four at a time (ld is a
+// multiple of 32 there).
+template <int T>
+__device__ __forceinline__ void write_sketch_row(const float* ob, uint32_t d, double nrm, float scale, int split,
+                                                 float* orow, uint64_t ld) {
+    if (split) {
+        float4* h4 = reinterpret_cast<float4*>(orow);
+        float4* l4 = reinterpret_cast<float4*>(orow + ld);
+        const float4* o4 = reinterpret_cast<const float4*>(ob);
+        for (uint32_t v = threadIdx.x; v < (uint32_t)(ld / 4); v += T) {
+            const float4 x = 4 * v < d ? o4[v] : make_float4(0.f, 0.f, 0.f, 0.f);
+            const float e[4] = {x.x, x.y, x.z, x.w};
+            float hi[4], lo[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const float val = nrm > 0.0 ? e[k] * scale : e[k];
+                hi[k] = 4 * v + k < d ? to_tf32(val) : 0.f;
+                lo[k] = 4 * v + k < d ? to_tf32(val - hi[k]) : 0.f;
+            }
+            h4[v] = make_float4(hi[0], hi[1], hi[2], hi[3]);
+            l4[v] = make_float4(lo[0], lo[1], lo[2], lo[3]);
+        }
+    } else {
+        for (uint64_t b = threadIdx.x; b < ld; b += T) orow[b] = b < d ? (nrm > 0.0 ? ob[b] * scale : ob[b]) : 0.f;
+    }
 }
 
 // One CTA per record (grid-stride over records).  Output row r: `ld` floats
@@ -150,7 +180,7 @@ __global__ void __launch_bounds__(SNT, 8) k_sketch_seg(const uint32_t* __restric
     extern __shared__ __align__(16) int32_t sh[];
     const uint32_t quads = (uint32_t)sketch_quads(n_used);  // the permuted pitch is 4 quads' worth of words, padded
     int2* Pq = reinterpret_cast<int2*>(sh);                  // (popc, missing) before each quad, warp-relative
-    float* ob = reinterpret_cast<float*>(sh + 2 * quads);    // bucket values
+    float* ob = reinterpret_cast<float*>(sh + 2 * ((quads + 1) & ~1u));  // bucket values
     __shared__ int32_t wa[SNW], wm[SNW], wt[SNW];
     __shared__ int2 woff[SNW];  // (bits, missing) before each warp's block
     __shared__ double dred[SNW];
@@ -289,23 +319,7 @@ __global__ void __launch_bounds__(SNT, 8) k_sketch_seg(const uint32_t* __restric
 #pragma unroll
         for (int w = 0; w < SNW; w++) nrm += dred[w];
         const float scale = nrm > 0.0 ? (float)sqrt((double)n_used / nrm) : 1.0f;
-        float* orow = out + (uint64_t)r * (split ? 2 : 1) * ld;
-        if (split) {
-            // tensor-core operand rows: 2r = tf32(v), 2r+1 = tf32(v - tf32(v))
-            float* lrow = orow + ld;
-            for (uint64_t b = threadIdx.x; b < ld; b += SNT) {
-                float hi = 0.f, lo = 0.f;
-                if (b < d) {
-                    const float v = nrm > 0.0 ? ob[b] * scale : ob[b];
-                    hi = to_tf32(v);
-                    lo = to_tf32(v - hi);
-                }
-                orow[b] = hi;
-                lrow[b] = lo;
-            }
-        } else {
-            for (uint64_t b = threadIdx.x; b < ld; b += SNT) orow[b] = b < d ? (nrm > 0.0 ? ob[b] * scale : ob[b]) : 0.f;
-        }
+        write_sketch_row<SNT>(ob, d, nrm, scale, split, out + (uint64_t)r * (split ? 2 : 1) * ld, ld);
         __syncthreads();  // Pq, ob, wa and dred are rewritten by the next record
     }
 }
@@ -498,22 +512,7 @@ __global__ void __launch_bounds__(S6T, 3) k_sketch_seg6(const uint32_t* __restri
 #pragma unroll
         for (int w = 0; w < S6W; w++) nrm += dred[w];
         const float scale = nrm > 0.0 ? (float)sqrt((double)n_used / nrm) : 1.0f;
-        float* orow = out + (uint64_t)r * (split ? 2 : 1) * ld;
-        if (split) {
-            float* lrow = orow + ld;
-            for (uint64_t b = threadIdx.x; b < ld; b += S6T) {
-                float hi = 0.f, lo = 0.f;
-                if (b < d) {
-                    const float v = nrm > 0.0 ? ob[b] * scale : ob[b];
-                    hi = to_tf32(v);
-                    lo = to_tf32(v - hi);
-                }
-                orow[b] = hi;
-                lrow[b] = lo;
-            }
-        } else {
-            for (uint64_t b = threadIdx.x; b < ld; b += S6T) orow[b] = b < d ? (nrm > 0.0 ? ob[b] * scale : ob[b]) : 0.f;
-        }
+        write_sketch_row<S6T>(ob, d, nrm, scale, split, out + (uint64_t)r * (split ? 2 : 1) * ld, ld);
         __syncthreads();  // PQ, Rs, ob, wa and dred are rewritten by the next record
     }
 }
