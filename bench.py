@@ -222,6 +222,7 @@ def run_sketch_workload(args, ctx, stream):
                "ms_per_step": 1e3 * t / args.steps, "n_pairs": npairs,
                "exact_int8_pairs_per_s": npairs / t_ex,
                "sketch_kernel_ms": 1e3 * sk_s, "sketch_gram_ms": 1e3 * gram_s, "decode_ms": 1e3 * perf.norm_secs,
+               "device_ms_per_call": float(np.mean([o[2].device_ms for o in outs])),
                "sketch_roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                                    "frac": achieved / hbm, "algorithmic_bytes": alg_bytes, "peak_source": src},
                "vs_exact": {"pearson_r": float(np.corrcoef(sk, exact)[0, 1]),
