@@ -205,7 +205,8 @@ def run_sketch_workload(args, ctx, stream):
     t_ex, outs = _timed_passes(ctx, stream, lambda: run_l2(ctx, snps, panel, wm, 200, snp_level_masking=True,
                                                            precision="int8", yes_really=True), 1, 1)
     exact = outs[0][0][:, 0]
-    hbm, _, src = measured_peaks()
+    hbm, bf16, src = measured_peaks()
+    tf32_peak = bf16 / 2.0
     for d in [int(x) for x in args.sketch_d.split(",")]:
         t, outs = _timed_passes(ctx, stream, lambda: run_l2(ctx, snps, panel, wm, 200, snp_level_masking=True,
                                                             sketch=d, yes_really=True), args.warmup, args.steps)
@@ -225,6 +226,17 @@ def run_sketch_workload(args, ctx, stream):
                "device_ms_per_call": float(np.mean([o[2].device_ms for o in outs])),
                "sketch_roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                                    "frac": achieved / hbm, "algorithmic_bytes": alg_bytes, "peak_source": src},
+               # the TF32 band Gram: every tile computes 64 x 128 record pairs over hi/lo rows
+               # (4 products of round_up(d, 32) terms per pair, 8 flops per term); useful
+               # work is 2 d flops per in-band pair
+               "sketch_gram_roofline": {"bound": "tensor (TF32)", "unit": "TFLOP/s",
+                                        "achieved": 8.0 * ((d + 31) // 32 * 32) * 64 * 128 * perf.n_tiles
+                                        / gram_s / 1e12,
+                                        "peak": tf32_peak, "frac": 8.0 * ((d + 31) // 32 * 32) * 64 * 128
+                                        * perf.n_tiles / gram_s / 1e12 / tf32_peak,
+                                        "useful_tflops": 2.0 * d * npairs / gram_s / 1e12,
+                                        "tiles": int(perf.n_tiles), "peak_source": src,
+                                        "note": "peak = half the bf16 dense burst (dense TF32 is half rate)"},
                "vs_exact": {"pearson_r": float(np.corrcoef(sk, exact)[0, 1]),
                             "max_abs_err": float(np.max(np.abs(sk - exact))),
                             "mean_abs_err": float(np.mean(np.abs(sk - exact))),

@@ -415,13 +415,18 @@ static cudaError_t launch_tc(const void* ops, CUtensorMapDataType dt, uint64_t e
     const size_t cbytes = sizeof(double) * 4 * TB;
     int64_t grid = n_tiles < sms ? n_tiles : sms;
     if (dbg) grid = 1;
-    // eight epilogue warps where the epilogue outweighs the MMAs
+    // more epilogue warps where the epilogue outweighs the MMAs: sixteen for
+    // the sketch forms with one annotation column (the f64 quadratic
+    // correction per pair), eight for INT8 rows under 32,768 individuals
     const bool wide = MODE != 0 || ld_elems * elem_bytes < 32768;
     if (ep.K == 1) {
         const size_t smem = 1024 + 4 * (size_t)(A_BYTES + B_BYTES) + ctrl + cbytes;
-        if (MODE != 0 || wide)
-            return run_tc<4, MODE, 8>(tmA, tmB, num_kb, tiles, n_tiles, ep, dbg, smem, grid, stream);
-        return run_tc<4, MODE, MODE == 0 ? 4 : 8>(tmA, tmB, num_kb, tiles, n_tiles, ep, dbg, smem, grid, stream);
+        if constexpr (MODE != 0) {
+            return run_tc<4, MODE, 16>(tmA, tmB, num_kb, tiles, n_tiles, ep, dbg, smem, grid, stream);
+        } else {
+            if (wide) return run_tc<4, MODE, 8>(tmA, tmB, num_kb, tiles, n_tiles, ep, dbg, smem, grid, stream);
+            return run_tc<4, MODE, 4>(tmA, tmB, num_kb, tiles, n_tiles, ep, dbg, smem, grid, stream);
+        }
     }
     const size_t smem = 1024 + 3 * (size_t)(A_BYTES + B_BYTES) + ctrl + cbytes + sizeof(float) * TA * RLD;
     if (MODE != 0 || wide)
