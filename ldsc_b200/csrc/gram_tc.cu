@@ -429,9 +429,12 @@ static cudaError_t launch_tc(const void* ops, CUtensorMapDataType dt, uint64_t e
         }
     }
     const size_t smem = 1024 + 3 * (size_t)(A_BYTES + B_BYTES) + ctrl + cbytes + sizeof(float) * TA * RLD;
-    if (MODE != 0 || wide)
+    if constexpr (MODE != 0) {
         return run_tc<3, MODE, 8>(tmA, tmB, num_kb, tiles, n_tiles, ep, dbg, smem, grid, stream);
-    return run_tc<3, MODE, MODE == 0 ? 4 : 8>(tmA, tmB, num_kb, tiles, n_tiles, ep, dbg, smem, grid, stream);
+    } else {
+        if (wide) return run_tc<3, MODE, 8>(tmA, tmB, num_kb, tiles, n_tiles, ep, dbg, smem, grid, stream);
+        return run_tc<3, MODE, 4>(tmA, tmB, num_kb, tiles, n_tiles, ep, dbg, smem, grid, stream);
+    }
 }
 
 cudaError_t launch_gram_i8(const uint8_t* ops, uint64_t ld, int64_t m, const Tile* tiles, int64_t n_tiles,
