@@ -131,6 +131,9 @@ struct ldsc_ctx {
     // partitioned h2
     DevBuf p_l2, p_w, p_y, p_n, p_m, p_rjobs, p_seps, p_n1, p_cnt, p_jobs, p_st, p_xtot, p_part, p_gram, p_tot,
         p_sol, p_res;
+    // the host plan of the last l2 call, kept so the next one reuses its pages
+    LeftLimits plan_left;
+    std::vector<Tile> plan_tiles;
     // whole-file entry: staged file rows, the pitched panel, per-chunk events
     DevBuf bed_stage, bed_rows;
     std::vector<cudaEvent_t> feed_ev;
@@ -776,8 +779,8 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
     }
 
     // ---- host plan: left limits, band tiles, contraction lists ----
-    LeftLimits L;
-    std::vector<Tile> tiles;
+    LeftLimits& L = ctx->plan_left;
+    std::vector<Tile>& tiles = ctx->plan_tiles;
     const int32_t n_right = (int32_t)((m + tb - 1) / tb), n_left = (int32_t)((m + ta - 1) / ta);
     auto plan = [&]() -> int {
         std::string perr;
@@ -787,7 +790,7 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
         if (L.any_full && !a->yes_really)
             std::printf("WARNING: LD window spans the entire chromosome. Use --yes-really to silence this warning.\n");
         pf.n_pairs = L.n_pairs;
-        tiles = band_tiles(L.left, ta, tb);
+        band_tiles(L.left, ta, tb, &tiles);
         pf.n_tiles = tiles.size();
         CK(ctx->left.ensure(sizeof(int64_t) * nmom));
         CK(ctx->tiles.ensure(sizeof(Tile) * (tiles.size() + 1)));

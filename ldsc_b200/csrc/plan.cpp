@@ -5,6 +5,66 @@
 
 namespace ldsc {
 
+namespace {
+
+// bl over one chromosome's records [start, start + len) by the reference's
+// two-pointer walk: for each i, j moves forward while |x_i - x_j| > wind.
+template <typename Coord>
+void lefts_walk(int64_t start, int64_t len, double wind, Coord coord, int64_t* bl) {
+    int64_t j = 0;
+    for (int64_t i = 0; i < len; i++) {
+        const double ci = coord(start + i);
+        while (j < len && std::fabs(ci - coord(start + j)) > wind) j++;
+        bl[start + i] = start + j;
+    }
+}
+
+// The same result when the coordinates are non-decreasing and wind >= 0.
+// Then x_i - x_j >= 0 for j <= i, the walk never passes i, and "x_i - x_j >
+// wind" holds for a prefix of j (rounding is monotone), so walk i's j is the
+// first j where it fails: a binary search gives it at any i.  The range is
+// cut into WALKERS segments, each started by that search and then walked as
+// in lefts_walk; the segments' walks are interleaved in one loop, so their
+// dependent compare-and-advance chains overlap in the core.
+template <typename Coord>
+void lefts_sorted(int64_t start, int64_t len, double wind, Coord coord, int64_t* bl) {
+    constexpr int WALKERS = 8;
+    int64_t wi[WALKERS], wj[WALKERS], we[WALKERS];
+    for (int w = 0; w < WALKERS; w++) {
+        const int64_t i0 = len * w / WALKERS, i1 = len * (w + 1) / WALKERS;
+        wi[w] = i0;
+        we[w] = i1;
+        int64_t lo = 0, hi = i0;  // first j in [0, i0] with !(x_i0 - x_j > wind)
+        if (i0 < i1) {
+            const double ci = coord(start + i0);
+            while (lo < hi) {
+                const int64_t mid = lo + (hi - lo) / 2;
+                if (ci - coord(start + mid) > wind)
+                    lo = mid + 1;
+                else
+                    hi = mid;
+            }
+        }
+        wj[w] = lo;
+    }
+    for (;;) {
+        bool busy = false;
+#pragma GCC unroll 8
+        for (int w = 0; w < WALKERS; w++) {
+            if (wi[w] < we[w]) {
+                busy = true;
+                const bool adv = coord(start + wi[w]) - coord(start + wj[w]) > wind;
+                bl[start + wi[w]] = start + wj[w];
+                wj[w] += adv;
+                wi[w] += !adv;
+            }
+        }
+        if (!busy) break;
+    }
+}
+
+}  // namespace
+
 bool block_lefts(int64_t m, const uint8_t* chr, const double* cm, const uint32_t* bp, int mode,
                  double wind, uint64_t half, int64_t* bl) {
     bool any_full = false;
@@ -19,13 +79,18 @@ bool block_lefts(int64_t m, const uint8_t* chr, const double* cm, const uint32_t
             for (int64_t i = 0; i < len; i++)
                 bl[start + i] = start + (i > (int64_t)half ? i - (int64_t)half : 0);
         } else {
-            auto coord = [&](int64_t r) { return mode == 0 ? cm[r] : (double)bp[r] / 1000.0; };
-            int64_t j = 0;
-            for (int64_t i = 0; i < len; i++) {
-                const double ci = coord(start + i);
-                while (j < len && std::fabs(ci - coord(start + j)) > wind) j++;
-                bl[start + i] = start + j;
-            }
+            auto run = [&](auto coord) {
+                bool sorted = wind >= 0.0;
+                for (int64_t r = start + 1; r < end && sorted; r++) sorted = coord(r) >= coord(r - 1);
+                if (sorted && len >= 64)
+                    lefts_sorted(start, len, wind, coord, bl);
+                else
+                    lefts_walk(start, len, wind, coord, bl);
+            };
+            if (mode == 0)
+                run([cm](int64_t r) { return cm[r]; });
+            else
+                run([bp](int64_t r) { return (double)bp[r] / 1000.0; });
             if (len > 0 && bl[end - 1] == start) any_full = true;
         }
         start = end;
@@ -48,10 +113,11 @@ bool left_limits(int64_t m, const uint8_t* chr, const double* cm, const uint32_t
         *err = "missing chr / cm / bp arrays for the window mode";
         return false;
     }
-    out->left.assign((size_t)m, 0);
+    out->left.resize((size_t)m);
+    out->bl.resize((size_t)m);
     out->n_pairs = 0;
     out->chunks = 0;
-    std::vector<int64_t> bl((size_t)m);
+    std::vector<int64_t>& bl = out->bl;
     out->any_full = block_lefts(m, chr, cm, bp, mode, wind, half, bl.data());
     // chunking groups: each chromosome (per-chromosome mode) or everything
     int64_t g0 = 0;
@@ -83,6 +149,13 @@ bool left_limits(int64_t m, const uint8_t* chr, const double* cm, const uint32_t
 
 std::vector<Tile> band_tiles(const std::vector<int64_t>& left, int ta, int tb) {
     std::vector<Tile> tiles;
+    band_tiles(left, ta, tb, &tiles);
+    return tiles;
+}
+
+void band_tiles(const std::vector<int64_t>& left, int ta, int tb, std::vector<Tile>* out) {
+    std::vector<Tile>& tiles = *out;
+    tiles.clear();
     const int64_t m = (int64_t)left.size();
     for (int64_t j0 = 0; j0 < m; j0 += tb) {
         const int64_t j1 = j0 + tb < m ? j0 + tb : m;
@@ -103,7 +176,6 @@ std::vector<Tile> band_tiles(const std::vector<int64_t>& left, int ta, int tb) {
             if (any) tiles.push_back(Tile{(uint32_t)a, (uint32_t)(j0 / tb)});
         }
     }
-    return tiles;
 }
 
 // ---- fastrand 2.3.0 WyRand (independent restatement of the published

@@ -23,8 +23,10 @@ bool block_lefts(int64_t m, const uint8_t* chr, const double* cm, const uint32_t
 //             cs - ceil((cs - bl[cs]) / c) * c with cs the chunk's first
 //             record (compute.rs:1164-1184, 1288-1299); chunks start at each
 //             chromosome in per-chromosome mode, at record 0 for --global-pass.
+// A LeftLimits reused across calls keeps its storage (no fresh pages per call).
 struct LeftLimits {
     std::vector<int64_t> left;
+    std::vector<int64_t> bl;  // block lefts (scratch)
     uint64_t n_pairs = 0;
     uint64_t chunks = 0;
     bool any_full = false;
@@ -33,8 +35,10 @@ bool left_limits(int64_t m, const uint8_t* chr, const double* cm, const uint32_t
                  double wind, uint64_t half, uint32_t chunk, bool masking, bool global_pass,
                  LeftLimits* out, std::string* err);
 
-// Band tiles of ta x tb records covering every pair left[j] <= k < j.
+// Band tiles of ta x tb records covering every pair left[j] <= k < j; the
+// second form refills *out, keeping its storage.
 std::vector<Tile> band_tiles(const std::vector<int64_t>& left, int ta, int tb);
+void band_tiles(const std::vector<int64_t>& left, int ta, int tb, std::vector<Tile>* out);
 
 // fastrand 2.3.0 WyRand stream as used by CountSketchProj::new
 // (src/l2/compute.rs:179-184): n bucket draws u32(..d), then n bool draws.

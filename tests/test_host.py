@@ -82,6 +82,31 @@ def test_left_limits_and_pair_counts_match_oracle(lib):
         assert pair_count(snps, wm, chunk, masking, not per_chr) == int(z[f"pairs_{name}"]), name
 
 
+def test_left_limits_on_tied_and_unsorted_coordinates(lib):
+    """Window limits for sorted coordinates with many ties (the interleaved
+    sorted-coordinate walk) and for unsorted ones (the plain two-pointer
+    walk), in cM and kb modes, against the Python restatement."""
+    from ldsc_b200.api import WindowMode, left_limits
+    from ldsc_b200.plink import BimTable
+    from test_oracle import py_left_limits
+    rng = np.random.default_rng(17)
+    m = 3000
+    chr_ = np.repeat(np.array([1, 2, 5], dtype=np.uint8), [1700, 40, 1260])
+    tied = np.round(np.cumsum(rng.exponential(0.004, m)), 2)           # sorted, many equal values
+    shuffled = tied.copy()
+    shuffled[1740:] = rng.permutation(shuffled[1740:])                  # chromosome 5 unsorted
+    bp = np.sort(rng.integers(0, 3_000_000, m)).astype(np.uint32)
+    bp[:1700] = np.sort(rng.integers(0, 900, 1700) * 1000)              # kb ties
+    for cm in (tied, shuffled):
+        snps = BimTable(chr_, [f"rs{i}" for i in range(m)], cm, bp, np.arange(m, dtype=np.int64))
+        for mode, wind in (("cm", 0.5), ("cm", 0.0), ("kb", 40.0)):
+            wm = WindowMode.Cm(wind) if mode == "cm" else WindowMode.Kb(wind)
+            for masking in (True, False):
+                got = left_limits(snps, wm, 100, masking, False)
+                exp = py_left_limits(chr_, cm, bp, mode, wind, 0, 100, masking, True)
+                assert np.array_equal(got, exp), (mode, wind, masking)
+
+
 def test_countsketch_hash_restatements_agree(lib):
     """The engine's and the oracle's restatements of fastrand's WyRand stream
     (written independently) produce the same buckets and signs."""
