@@ -512,7 +512,7 @@ struct RowFeed {
     ldsc_ctx* ctx = nullptr;
     const uint8_t* host = nullptr;  // file body (after the 3 magic bytes)
     uint64_t bpr = 0, pitch = 0, rows = 0, per = 0;
-    int nchunks = 0, issued = 0;
+    int nchunks = 0, issued = 0, queued = 0;
     uint8_t* dst = nullptr;
 
     bool started = false;
@@ -537,28 +537,32 @@ struct RowFeed {
         dst = c->bed_rows.as<uint8_t>();
         return LDSC_OK;
     }
-    // queue every chunk's copy (after the small uploads already on the compute
-    // stream, so those are not held behind the file)
-    int start(cudaStream_t s) {
+    // queue the copies of chunks [queued, k_end) (after the small uploads
+    // already on the copy stream, so those are not held behind the file);
+    // start() queues all of them
+    int start_until(cudaStream_t s, int k_end) {
         ldsc_ctx* c = ctx;
-        if (started) return LDSC_OK;
-        started = true;
-        // the staging buffer may still be read by earlier work on the compute stream
-        CK(cudaEventRecord(c->feed_go, s));
-        CK(cudaStreamWaitEvent(c->copy, c->feed_go, 0));
-        CK(cudaEventRecord(c->feed_t0, c->copy));
-        for (int k = 0; k < nchunks; k++) {
+        if (!started) {
+            started = true;
+            // the staging buffer may still be read by earlier work on the compute stream
+            CK(cudaEventRecord(c->feed_go, s));
+            CK(cudaStreamWaitEvent(c->copy, c->feed_go, 0));
+            CK(cudaEventRecord(c->feed_t0, c->copy));
+        }
+        for (; queued < std::min(k_end, nchunks); queued++) {
+            const int k = queued;
             const uint64_t r0 = (uint64_t)k * per, r1 = row_end(k);
             CK(cudaMemcpyAsync(c->bed_stage.as<uint8_t>() + r0 * bpr, host + r0 * bpr, (r1 - r0) * bpr,
                                cudaMemcpyHostToDevice, c->copy));
             CK(cudaEventRecord(c->feed_ev[k], c->copy));
+            if (k == nchunks - 1) CK(cudaEventRecord(c->feed_t1, c->copy));
         }
-        CK(cudaEventRecord(c->feed_t1, c->copy));
         return LDSC_OK;
     }
+    int start(cudaStream_t s) { return start_until(s, nchunks); }
     int issue_until(int k_end, cudaStream_t s) {  // chunks [issued, k_end)
         ldsc_ctx* c = ctx;
-        if (!started) {
+        if (queued < nchunks) {  // every waited-on chunk's copy (and event) is queued first
             int rc = start(s);
             if (rc != LDSC_OK) return rc;
         }
@@ -851,7 +855,11 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
     // whose records all lie in chunks [0, k] run while later chunks copy.
     const bool stream_gram = chunked && exact_i8 && K == 1;
     if (stream_gram) {
-        int rc = plan();
+        // the first chunk's copy runs while the host plans; the plan's uploads
+        // queue behind that chunk only
+        int rc = feed->start_until(s, 1);
+        if (rc != LDSC_OK) return rc;
+        rc = plan();
         if (rc != LDSC_OK) return rc;
         ep.left = ctx->left.as<int64_t>();
         ep.rtiles = nullptr;
