@@ -94,11 +94,11 @@ __global__ void __launch_bounds__(NT) k_sketch_permute(PanelView p, const int32_
 // per lane (coalesced loads, branch-free popcounts); one warp scan of the
 // packed (bits, missing) counts gives the prefix at the start of every quad,
 // kept in shared memory.  (2) Boundaries: after a block scan over the warps,
-// thread t takes the buckets [d t / NT, d (t+1) / NT) and walks their
+// thread t takes the buckets [d t / SNT, d (t+1) / SNT) and walks their
 // boundaries in order; each prefix is the quad prefix, plus the offset of the
 // warp that streamed the quad, plus popcounts inside the quad (re-read from
 // L1/L2).  Thread t's boundary positions come from a thread-major table built
-// once per layout (entry i * NT + t = its i-th boundary, with the owning warp
+// once per layout (entry i * SNT + t = its i-th boundary, with the owning warp
 // in the top bits), so their loads are coalesced.  Each bucket's value is
 // formed on the spot.  No atomics, and nothing needs clearing between
 // records.
