@@ -183,7 +183,7 @@ __global__ void __launch_bounds__(SNT, 8) k_sketch_seg(const uint32_t* __restric
     float* ob = reinterpret_cast<float*>(sh + 2 * ((quads + 1) & ~1u));  // bucket values
     __shared__ int32_t wa[SNW], wm[SNW], wt[SNW];
     __shared__ int2 woff[SNW];  // (bits, missing) before each warp's block
-    __shared__ double dred[SNW];
+    __shared__ double dred[SNW], rconst[2];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t wq0 = (uint32_t)((uint64_t)quads * warp / SNW), wq1 = (uint32_t)((uint64_t)quads * (warp + 1) / SNW);
     const uint32_t b0 = seg_b<SNT>(d, threadIdx.x), nbd = seg_count<SNT>(d, threadIdx.x);
@@ -245,12 +245,15 @@ __global__ void __launch_bounds__(SNT, 8) k_sketch_seg(const uint32_t* __restric
                 st.q4[r] = G + 14 * TT;
             }
         }
-        // normalize_col_f32_with_stats constants (src/l2/normalize.rs:115-154)
-        const double dmean = N > 0 ? (double)G / (double)N : 0.0;
-        const double css = (double)(G + 2 * TT) - (double)N * dmean * dmean;
-        const double sd = sqrt(css / (double)n_used);
-        const double mean = (double)(float)dmean;
-        const double inv = sd > 0.0 ? (double)(float)(1.0 / sd) : 0.0;
+        // normalize_col_f32_with_stats constants (src/l2/normalize.rs:115-154),
+        // formed once and read by every thread after the barrier below
+        if (threadIdx.x == 0) {
+            const double dmean = N > 0 ? (double)G / (double)N : 0.0;
+            const double css = (double)(G + 2 * TT) - (double)N * dmean * dmean;
+            const double sd = sqrt(css / (double)n_used);
+            rconst[0] = (double)(float)dmean;
+            rconst[1] = sd > 0.0 ? (double)(float)(1.0 / sd) : 0.0;
+        }
         if (threadIdx.x < SNW) {
             int32_t oa = 0, om = 0;
 #pragma unroll
@@ -262,6 +265,7 @@ __global__ void __launch_bounds__(SNT, 8) k_sketch_seg(const uint32_t* __restric
             woff[threadIdx.x] = make_int2(oa, om);
         }
         __syncthreads();
+        const double mean = rconst[0], inv = rconst[1];
         // ---- phase 2: this thread's buckets ----
         // Boundaries in groups of four: the group's table entries are loaded
         // one group ahead and its four quads are loaded together.
@@ -379,7 +383,7 @@ __global__ void __launch_bounds__(S6T, 3) k_sketch_seg6(const uint32_t* __restri
     uint4* Rs = sh6 + quads;  // the quads
     float* ob = reinterpret_cast<float*>(sh6 + 2 * (size_t)quads);
     __shared__ int32_t wa[S6W], wm[S6W], wt[S6W];
-    __shared__ double dred[S6W];
+    __shared__ double dred[S6W], rconst[2];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t wq0 = (uint32_t)((uint64_t)quads * warp / S6W), wq1 = (uint32_t)((uint64_t)quads * (warp + 1) / S6W);
     const uint32_t b0 = seg_b<S6T>(d, threadIdx.x), nbd = seg_count<S6T>(d, threadIdx.x);
@@ -447,11 +451,13 @@ __global__ void __launch_bounds__(S6T, 3) k_sketch_seg6(const uint32_t* __restri
                 st.q4[r] = G + 14 * TT;
             }
         }
-        const double dmean = N > 0 ? (double)G / (double)N : 0.0;
-        const double css = (double)(G + 2 * TT) - (double)N * dmean * dmean;
-        const double sd = sqrt(css / (double)n_used);
-        const double mean = (double)(float)dmean;
-        const double inv = sd > 0.0 ? (double)(float)(1.0 / sd) : 0.0;
+        if (threadIdx.x == 0) {  // the record's constants, read after the barrier below
+            const double dmean = N > 0 ? (double)G / (double)N : 0.0;
+            const double css = (double)(G + 2 * TT) - (double)N * dmean * dmean;
+            const double sd = sqrt(css / (double)n_used);
+            rconst[0] = (double)(float)dmean;
+            rconst[1] = sd > 0.0 ? (double)(float)(1.0 / sd) : 0.0;
+        }
         // block-absolute quad prefixes
         if (offA | offM)
             for (uint32_t q = wq0 + lane; q < wq1; q += 32) {
@@ -460,6 +466,7 @@ __global__ void __launch_bounds__(S6T, 3) k_sketch_seg6(const uint32_t* __restri
                 *e = make_uint2(v.x + (uint32_t)offA, v.y + (uint32_t)offM);
             }
         __syncthreads();
+        const double mean = rconst[0], inv = rconst[1];
         // ---- phase 2 ----
         double part = 0.0;
         if (nbd) {
