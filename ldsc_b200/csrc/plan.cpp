@@ -80,8 +80,8 @@ bool block_lefts(int64_t m, const uint8_t* chr, const double* cm, const uint32_t
                 bl[start + i] = start + (i > (int64_t)half ? i - (int64_t)half : 0);
         } else {
             auto run = [&](auto coord) {
-                bool sorted = wind >= 0.0;
-                for (int64_t r = start + 1; r < end && sorted; r++) sorted = coord(r) >= coord(r - 1);
+                bool sorted = wind >= 0.0;  // NaN coordinates or window fail the comparisons
+                for (int64_t r = start + 1; r < end; r++) sorted &= coord(r) >= coord(r - 1);
                 if (sorted && len >= 64)
                     lefts_sorted(start, len, wind, coord, bl);
                 else
@@ -128,20 +128,26 @@ bool left_limits(int64_t m, const uint8_t* chr, const double* cm, const uint32_t
             while (g1 < m && chr[g1] == chr[g0]) g1++;
         }
         const int64_t c = chunk;
+        // locals, so the loop below does not go through *out on every record
+        int64_t* left = out->left.data();
+        const int64_t* blp = bl.data();
+        uint64_t pairs = 0, chunks = 0;
         for (int64_t cs = g0; cs < g1; cs += c) {
             const int64_t ce = cs + c < g1 ? cs + c : g1;
-            out->chunks++;
+            chunks++;
             // block_sizes[cs] within the group (compute.rs:1164-1173, 1288-1292)
-            const int64_t dist = cs - bl[cs];
+            const int64_t dist = cs - blp[cs];
             int64_t b = dist == 0 ? 0 : ((dist + c - 1) / c) * c;
             if (b > cs - g0) b = cs - g0;
             const int64_t a_left = cs - b;
             for (int64_t j = cs; j < ce; j++) {
-                const int64_t L = masking ? bl[j] : a_left;
-                out->left[j] = L;
-                out->n_pairs += (uint64_t)(j - L);
+                const int64_t L = masking ? blp[j] : a_left;
+                left[j] = L;
+                pairs += (uint64_t)(j - L);
             }
         }
+        out->n_pairs += pairs;
+        out->chunks += chunks;
         g0 = g1;
     }
     return true;
