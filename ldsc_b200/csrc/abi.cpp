@@ -504,8 +504,9 @@ int sketch_prepare(ldsc_ctx* ctx, const ldsc_panel* panel, uint64_t n_used, uint
     return LDSC_OK;
 }
 
-// Streams a BED body from host memory into the pitched panel: every chunk's
-// copy is queued at once on the context's copy stream, and issue(c) makes the
+// Streams a BED body from host memory into the pitched panel: the chunks'
+// copies are queued on the context's copy stream (all at once, or the first
+// one ahead of the host plan and the rest after it), and issue(c) makes the
 // compute stream wait for chunk c and re-pitch it, so decoding chunk c
 // overlaps the copies of the chunks after it.
 struct RowFeed {
