@@ -412,9 +412,9 @@ int ldsc_server_destroy(ldsc_server *srv);
 
 /* No counterpart in the reference: this entry point exists for callers that
  * cannot allocate device memory -- a host that owns all device memory through
- * its own arena, code that runs while a stream is being captured into a CUDA
- * graph (cudaMalloc cannot be captured), or a latency-critical request loop in
- * which an allocation would synchronise the device.
+ * its own arena (an allocation behind its back breaks its accounting), or a
+ * latency-critical request loop in which an allocation or free would
+ * synchronise the device.
  *
  * It runs the INT8-exact l2 pass (all-ones annotation, K = 1) on device
  * buffers the caller owns and allocates nothing: all scratch lives in one
@@ -425,12 +425,17 @@ int ldsc_server_destroy(ldsc_server *srv);
  *   left     HOST array of n_snp window limits (ldsc_l2_left_limits)
  *   d_l2     device output, n_snp doubles;  d_maf  device output, n_snp doubles
  *   stream   cudaStream_t to run on (NULL = the legacy default stream)
- * Requests whose scratch (about 2 * n_snp * round_up(n_indiv, 128) bytes plus
- * 48 bytes per SNP) exceeds the array are rejected with LDSC_E_INVALID.  All
- * calls share the array, which keeps the last call's contents; calls that
- * overlap on the GPU race.  The first call on a device looks up the array's
- * address and should come before any stream capture.  The call waits for its
- * own work before returning.  Messages: ldsc_noalloc_last_error(). */
+ * Requests whose scratch exceeds the array are rejected with LDSC_E_INVALID.
+ * The scratch is 2 * n_snp * round_up(n_indiv, 128) bytes of operands, 52
+ * bytes per SNP of statistics and limits, 8 bytes per band tile (64 x 128
+ * records) and a 16-byte error word, each of its 11 parts starting on a
+ * 256-byte boundary.  All calls share the array, which keeps the last call's
+ * contents; calls that overlap on the GPU race.  The call runs on the current
+ * device, to which d_rows, d_l2, d_maf and the stream must belong.  The first
+ * call on a device looks up the array's address, keeps it for the life of the
+ * process, and should come before any stream capture; after a device reset
+ * the library must be reloaded.  The call waits for its own work before
+ * returning.  Messages: ldsc_noalloc_last_error(). */
 #define LDSC_NOALLOC_SCRATCH_BYTES (64u * 1024u * 1024u)
 
 int ldsc_l2_int8_noalloc(const uint8_t *d_rows, uint64_t pitch, uint64_t n_indiv, uint64_t n_snp,

@@ -2,22 +2,26 @@
 //
 // Some callers cannot call cudaMalloc: a host that owns all device memory
 // through its own arena (a JVM / Rust / serving runtime with a fixed memory
-// budget), code that runs while a stream is being captured into a CUDA graph
-// (cudaMalloc is not capturable), and latency-critical request loops where an
-// allocation would synchronise the device.  ldsc_l2_int8_noalloc() serves
-// them: the caller passes device buffers for the inputs and outputs, and the
-// kernels' scratch (INT8 genotype/mask operands, per-SNP statistics, the tile
-// list, the error word) lives in one file-scope device array of fixed size,
+// budget, where an allocation behind its back breaks its accounting), and
+// latency-critical request loops where an allocation or free would
+// synchronise the device.  ldsc_l2_int8_noalloc() serves them: the caller
+// passes device buffers for the inputs and outputs, and the kernels' scratch
+// (INT8 genotype/mask operands, per-SNP statistics, the tile list, the error
+// word) lives in one file-scope device array of fixed size,
 // LDSC_NOALLOC_SCRATCH_BYTES.  Every GPU that loads this library holds that
 // array until the process exits.
 //
 // The array is shared by every call on a device and keeps the last call's
 // contents: calls that overlap on the GPU (different streams, or host threads
 // without ordering) race on it.  Each call clears what must start at zero (the
-// error word) and overwrites everything else it reads.  The first call on a
-// device looks up the array's device address (cudaGetSymbolAddress, once per
-// device, with that device current); make that first call before any stream
-// capture begins.
+// error word) and overwrites everything else it reads.  The call runs on the
+// current device: the caller's buffers and stream must belong to it.  The
+// first call on a device looks up the array's device address
+// (cudaGetSymbolAddress, once per device, with that device current) and keeps
+// it for the life of the process; make that first call before any stream
+// capture begins.  A device reset (cudaDeviceReset) ends the context that
+// address belongs to, so after one the library must be unloaded and loaded
+// again before this entry point is used.
 #include <cuda_runtime.h>
 
 #include <cstdio>

@@ -216,10 +216,19 @@ def test_ctypes_mirror_matches_the_header_layout(tmp_path):
 
 
 def test_rust_binding_fields_match_the_header():
-    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    text = open(os.path.join(ROOT, "include", "ldsc_b200.rs")).read()
     hs = header_structs()
     found = dict(re.findall(r"pub struct (Ldsc\w+)\s*\{(.*?)\}", text, flags=re.S))
     for rname, cname in _RUST.items():
         assert rname in found, rname
         fields = re.findall(r"pub (\w+)\s*:", found[rname])
         assert fields == hs[cname], (rname, fields, hs[cname])
+
+
+def test_rust_binding_functions_are_declared_in_the_header():
+    rs = open(os.path.join(ROOT, "include", "ldsc_b200.rs")).read()
+    h = open(os.path.join(ROOT, "include", "ldsc_b200.h")).read()
+    names = re.findall(r"pub fn (ldsc_\w+)\(", rs)
+    assert len(names) >= 10
+    for name in names:
+        assert re.search(r"\b" + name + r"\s*\(", h), name

@@ -1,8 +1,8 @@
 """The allocation-free INT8 l2 entry point (ldsc_l2_int8_noalloc).
 
 It serves callers that cannot allocate device memory (hosts that own all device
-memory through their own arena, code running during a CUDA-graph stream
-capture, latency-critical request loops).  Its scratch is a static device
+memory through their own arena, latency-critical request loops in which an
+allocation would synchronise the device).  Its scratch is a static device
 array inside the library; inputs and outputs are the caller's device buffers.
 
 This file is collected last on purpose: if it fails, a run that stops at the
@@ -100,6 +100,36 @@ def test_noalloc_reuses_scratch_across_shapes(ctx):
     assert _relerr(l2b, ref_b) < TOL
     assert _relerr(l2a1, ref_a) < TOL
     assert _relerr(l2a2, ref_a) < TOL
+
+
+def test_noalloc_call_leaves_device_memory_unchanged(ctx):
+    """After a first call on the device, a call changes neither the device's
+    free memory nor torch's allocations: the entry point allocates nothing."""
+    import torch
+    lib = ctx.lib
+    z = np.load(os.path.join(GOLDEN, "small_panel.npz"))
+    n = int(z["n_indiv"])
+    rows, pitch = _device_rows(z["body"], n)
+    _, _, left = _case(ctx, z["body"], n, z["chr"], z["cm"], z["bp"], True, 50)
+    left = np.ascontiguousarray(left, dtype=np.int64)
+    m = len(left)
+    l2 = torch.zeros(m, dtype=torch.float64, device="cuda")
+    maf = torch.zeros(m, dtype=torch.float64, device="cuda")
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def call():
+        rc = lib.ldsc_l2_int8_noalloc(C.c_void_p(rows.data_ptr()), pitch, n, m, left.ctypes.data,
+                                      C.c_void_p(l2.data_ptr()), C.c_void_p(maf.data_ptr()), stream)
+        assert rc == 0
+        torch.cuda.synchronize()
+
+    call()   # first call on the device: symbol lookup, kernels loaded
+    free0, _ = torch.cuda.mem_get_info()
+    alloc0 = torch.cuda.memory_allocated()
+    call()
+    free1, _ = torch.cuda.mem_get_info()
+    assert torch.cuda.memory_allocated() == alloc0
+    assert free1 >= free0
 
 
 def test_noalloc_rejects_requests_beyond_the_scratch(ctx):
