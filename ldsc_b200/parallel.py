@@ -20,7 +20,7 @@ The call's own rows outside the core (the halos) are discarded.  Chromosomes
 are independent (src/l2/mod.rs:477-553), so a core that holds whole
 chromosomes needs no halo.  The only exchange between ranks is the final
 gather of the l2 rows (`gather_l2`), the step the reference's single process
-does not need.
+does not need: one tensor all-gather of the padded core rows.
 """
 from __future__ import annotations
 
@@ -145,35 +145,51 @@ def core_rows(l2_call: np.ndarray, sh: Shard) -> np.ndarray:
 
 
 def run_sharded(compute: Callable[[BimTable], np.ndarray], snps: BimTable, plan: Sequence[Shard], rank: int,
-                group=None, dst: Optional[int] = 0) -> Optional[np.ndarray]:
-    """Compute this rank's shard with `compute(records) -> l2 rows` and gather
-    the full M x K l2 on rank `dst` (every rank when dst is None)."""
+                group=None, dst: Optional[int] = 0, n_annot: int = 1) -> Optional[np.ndarray]:
+    """Compute this rank's shard with `compute(records) -> l2 rows` (numpy,
+    or a torch tensor of shape (call records, K)) and gather the full M x K
+    l2 on rank `dst` (every rank when dst is None)."""
     sh = plan[rank]
     part = None
     if sh.call_hi > sh.call_lo:
-        part = core_rows(np.asarray(compute(shard_records(snps, sh))), sh)
-    return gather_l2(part, plan, rank, group, dst)
+        out = compute(shard_records(snps, sh))
+        if not hasattr(out, "is_cuda"):
+            out = np.asarray(out)
+        part = core_rows(out, sh)
+    return gather_l2(part, plan, rank, group, dst, n_annot)
 
 
-def gather_l2(part: Optional[np.ndarray], plan: Sequence[Shard], rank: int, group=None,
-              dst: Optional[int] = 0) -> Optional[np.ndarray]:
-    """Assemble the core rows of every rank (torch.distributed object
-    collectives: any backend)."""
+def gather_l2(part, plan: Sequence[Shard], rank: int, group=None, dst: Optional[int] = 0, n_annot: int = 1):
+    """Assemble the core rows of every rank with one tensor all-gather.
+
+    ``part`` is this rank's core rows (core_hi - core_lo) x K, as a numpy
+    array or a torch tensor (a CUDA tensor stays on the device).  Every rank
+    pads its rows to the plan's largest core, so the collective moves equal
+    f64 blocks; with the NCCL backend the blocks are CUDA tensors and the
+    exchange runs over NVLink, with gloo they are CPU tensors.  Returns the
+    M x K l2 as numpy on rank ``dst`` (every rank when dst is None), else
+    None; ranks whose core is empty pass part=None."""
+    import torch
     import torch.distributed as dist
     world = len(plan)
-    payload = (plan[rank].core_lo, part)
-    if dst is None:
-        parts = [None] * world
-        dist.all_gather_object(parts, payload, group=group)
-    else:
-        parts = [None] * world if rank == dst else None
-        dist.gather_object(payload, parts, dst=dst, group=group)
-        if rank != dst:
-            return None
+    nccl = dist.get_backend(group) == "nccl"
+    dev = torch.device("cuda", torch.cuda.current_device()) if nccl else torch.device("cpu")
+    rows = max(s.core_hi - s.core_lo for s in plan)
+    if part is not None:
+        t = part if isinstance(part, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(part))
+        t = t.to(device=dev, dtype=torch.float64).reshape(t.shape[0], -1)
+        n_annot = t.shape[1]
+    block = torch.zeros((max(rows, 1), n_annot), dtype=torch.float64, device=dev)
+    if part is not None and t.shape[0]:
+        block[: t.shape[0]] = t
+    blocks = [torch.empty_like(block) for _ in range(world)]
+    dist.all_gather(blocks, block, group=group)
+    if dst is not None and rank != dst:
+        return None
     m = max(s.core_hi for s in plan)
-    k = next((p.shape[1] for _, p in parts if p is not None), 1)
-    out = np.zeros((m, k), dtype=np.float64)
-    for lo, p in parts:
-        if p is not None:
-            out[lo: lo + p.shape[0]] = p
+    out = np.zeros((m, n_annot), dtype=np.float64)
+    for sh, b in zip(plan, blocks):
+        n = sh.core_hi - sh.core_lo
+        if n:
+            out[sh.core_lo: sh.core_hi] = b[:n].cpu().numpy()
     return out

@@ -40,6 +40,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <time.h>
 #ifdef _OPENMP
 #include <omp.h>
 #endif
@@ -322,36 +323,70 @@ static inline v8f ld8f(const float *p) {
     return v;
 }
 
-/* 2 x 4 register block of column dot products, vectorised along the
- * individual axis; tail handled in scalar.  Summation order differs from
- * faer's, as any blocked GEMM's would. */
+/* Cache-blocked column Gram.  Each thread owns a macro tile of GB_W A columns
+ * x GB_C B columns and walks the individual axis in chunks of GB_K: a chunk
+ * of the macro tile's columns (GB_W + GB_C columns x 2 KB) stays in the
+ * core's L2 while every 3 x 4 register block of the tile reads it, so a
+ * column is fetched from memory once per chunk instead of once per register
+ * block.  Within a block the dot products are vectorised along the
+ * individual axis; tails are scalar.  Summation order differs from faer's,
+ * as any blocked GEMM's would. */
+#ifndef GB_W
+#define GB_W 48
+#endif
+#ifndef GB_C
+#define GB_C 16
+#endif
+#ifndef GB_K
+#define GB_K 256
+#endif
+
 static void gram_f64(int64_t n, int64_t w, int64_t c, double *const *acol, double *const *bcol,
                      double *out) {
-    int64_t nv = n & ~(int64_t)3;
-#pragma omp parallel for collapse(2) schedule(dynamic, 2)
-    for (int64_t jb = 0; jb < c; jb += 4) {
-        for (int64_t ib = 0; ib < w; ib += 2) {
-            int64_t ie = ib + 2 < w ? ib + 2 : w;
-            int64_t je = jb + 4 < c ? jb + 4 : c;
-            const double *ap[2], *bp[4];
-            for (int t = 0; t < 2; t++) ap[t] = acol[ib + t < ie ? ib + t : ib];
-            for (int t = 0; t < 4; t++) bp[t] = bcol[jb + t < je ? jb + t : jb];
-            v4d acc[2][4];
-            memset(acc, 0, sizeof(acc));
-            for (int64_t k = 0; k < nv; k += 4) {
-                v4d a0 = ld4d(ap[0] + k), a1 = ld4d(ap[1] + k);
-                v4d b0 = ld4d(bp[0] + k), b1 = ld4d(bp[1] + k);
-                v4d b2 = ld4d(bp[2] + k), b3 = ld4d(bp[3] + k);
-                acc[0][0] += a0 * b0; acc[0][1] += a0 * b1; acc[0][2] += a0 * b2; acc[0][3] += a0 * b3;
-                acc[1][0] += a1 * b0; acc[1][1] += a1 * b1; acc[1][2] += a1 * b2; acc[1][3] += a1 * b3;
-            }
-            for (int64_t i = ib; i < ie; i++)
-                for (int64_t j = jb; j < je; j++) {
-                    v4d v = acc[i - ib][j - jb];
-                    double s = (v[0] + v[1]) + (v[2] + v[3]);
-                    for (int64_t k = nv; k < n; k++) s += ap[i - ib][k] * bp[j - jb][k];
-                    out[i + j * w] = s;
+    const int64_t nwt = (w + GB_W - 1) / GB_W, nct = (c + GB_C - 1) / GB_C;
+#pragma omp parallel for collapse(2) schedule(dynamic, 1)
+    for (int64_t ct = 0; ct < nct; ct++) {
+        for (int64_t wt = 0; wt < nwt; wt++) {
+            const int64_t i0 = wt * GB_W, i1 = i0 + GB_W < w ? i0 + GB_W : w;
+            const int64_t j0 = ct * GB_C, j1 = j0 + GB_C < c ? j0 + GB_C : c;
+            double tile[GB_W * GB_C];
+            memset(tile, 0, sizeof(tile));
+            for (int64_t k0 = 0; k0 < n; k0 += GB_K) {
+                const int64_t k1 = k0 + GB_K < n ? k0 + GB_K : n;
+                const int64_t kv = k0 + ((k1 - k0) & ~(int64_t)3);
+                for (int64_t jb = j0; jb < j1; jb += 4) {
+                    for (int64_t ib = i0; ib < i1; ib += 3) {
+                        /* 3 x 4 register block: 12 accumulators, 3 A vectors, 1 B vector */
+                        const int64_t ie = ib + 3 < i1 ? ib + 3 : i1;
+                        const int64_t je = jb + 4 < j1 ? jb + 4 : j1;
+                        const double *ap[3], *bp[4];
+                        for (int t = 0; t < 3; t++) ap[t] = acol[ib + t < ie ? ib + t : ib];
+                        for (int t = 0; t < 4; t++) bp[t] = bcol[jb + t < je ? jb + t : jb];
+                        v4d acc[3][4];
+                        memset(acc, 0, sizeof(acc));
+                        for (int64_t k = k0; k < kv; k += 4) {
+                            const v4d a0 = ld4d(ap[0] + k), a1 = ld4d(ap[1] + k), a2 = ld4d(ap[2] + k);
+                            v4d b = ld4d(bp[0] + k);
+                            acc[0][0] += a0 * b; acc[1][0] += a1 * b; acc[2][0] += a2 * b;
+                            b = ld4d(bp[1] + k);
+                            acc[0][1] += a0 * b; acc[1][1] += a1 * b; acc[2][1] += a2 * b;
+                            b = ld4d(bp[2] + k);
+                            acc[0][2] += a0 * b; acc[1][2] += a1 * b; acc[2][2] += a2 * b;
+                            b = ld4d(bp[3] + k);
+                            acc[0][3] += a0 * b; acc[1][3] += a1 * b; acc[2][3] += a2 * b;
+                        }
+                        for (int64_t i = ib; i < ie; i++)
+                            for (int64_t j = jb; j < je; j++) {
+                                v4d v = acc[i - ib][j - jb];
+                                double s = (v[0] + v[1]) + (v[2] + v[3]);
+                                for (int64_t k = kv; k < k1; k++) s += ap[i - ib][k] * bp[j - jb][k];
+                                tile[(i - i0) + (j - j0) * GB_W] += s;
+                            }
+                    }
                 }
+            }
+            for (int64_t j = j0; j < j1; j++)
+                for (int64_t i = i0; i < i1; i++) out[i + j * w] = tile[(i - i0) + (j - j0) * GB_W];
         }
     }
 }
@@ -421,7 +456,20 @@ typedef struct {
 typedef struct {
     int64_t n_pairs;         /* off-diagonal pairs contributing to l2 in this mode */
     int any_full_chr_window;
+    int64_t n_dots;          /* column dot products the chunk Grams computed (w x c + c x c per chunk) */
+    double gemm_secs;        /* wall time inside the chunk Grams */
 } oracle_l2_info;
+
+/* Work and time of the chunk Grams of the current oracle_l2 call (the chunk
+ * loop calls them one at a time; each Gram is parallel inside). */
+static int64_t g_dots;
+static double g_gemm_secs;
+
+static double wall_secs(void) {
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+}
 
 /* One compute_ldscore_global call over records [r0, r0 + m). */
 static int compute_global(const oracle_l2_args *a, int64_t r0, int64_t m, double *l2, int64_t ldl,
@@ -610,7 +658,10 @@ static int compute_global(const oracle_l2_args *a, int64_t r0, int64_t m, double
                 for (int64_t x = 0; x < c * c; x++) r2u_bb[x] = (double)bb[x];
             } else {
                 double *bb = (double *)gbuf;
+                const double t0 = wall_secs();
                 gram_f64(gemm_n, c, c, (double *const *)bcol, (double *const *)bcol, bb);
+                g_gemm_secs += wall_secs() - t0;
+                g_dots += c * c;
                 for (int64_t x = 0; x < c * c; x++) r2u_bb[x] = bb[x];
             }
             /* fill: diagonal 1, off-diagonal from the (k, j) entry, symmetric */
@@ -675,7 +726,10 @@ static int compute_global(const oracle_l2_args *a, int64_t r0, int64_t m, double
                     for (int64_t x = 0; x < w * c; x++) r2u_ab[x] = (double)ab[x];
                 } else {
                     double *ab = (double *)gbuf;
+                    const double t0 = wall_secs();
                     gram_f64(gemm_n, w, c, (double *const *)acol, (double *const *)bcol, ab);
+                    g_gemm_secs += wall_secs() - t0;
+                    g_dots += w * c;
                     for (int64_t x = 0; x < w * c; x++) r2u_ab[x] = ab[x];
                 }
                 for (int64_t j = 0; j < c; j++)
@@ -759,6 +813,8 @@ int oracle_l2(const oracle_l2_args *a, double *l2_out, double *maf_out, oracle_l
     memset(l2_out, 0, sizeof(double) * (size_t)(a->m * K));
     int64_t pairs = 0;
     int any_full = 0;
+    g_dots = 0;
+    g_gemm_secs = 0.0;
     if (!a->per_chr) {
         int rc = compute_global(a, 0, a->m, l2_out, a->m, maf_out, &pairs, &any_full, err, errlen);
         if (rc) return rc;
@@ -776,6 +832,8 @@ int oracle_l2(const oracle_l2_args *a, double *l2_out, double *maf_out, oracle_l
     if (info) {
         info->n_pairs = pairs;
         info->any_full_chr_window = any_full;
+        info->n_dots = g_dots;
+        info->gemm_secs = g_gemm_secs;
     }
     return OR_OK;
 }

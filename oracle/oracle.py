@@ -56,7 +56,8 @@ class _Args(C.Structure):
 
 
 class _Info(C.Structure):
-    _fields_ = [("n_pairs", C.c_int64), ("any_full_chr_window", C.c_int)]
+    _fields_ = [("n_pairs", C.c_int64), ("any_full_chr_window", C.c_int), ("n_dots", C.c_int64),
+                ("gemm_secs", C.c_double)]
 
 
 MODE = {"cm": 0, "kb": 1, "snp": 2}
@@ -89,8 +90,10 @@ class OracleL2Args:
     n_threads: int = 0
 
 
-def oracle_l2(a: OracleL2Args):
-    """Returns (l2 [m x K], maf [m], n_pairs, any_full_chr_window)."""
+def oracle_l2(a: OracleL2Args, work: Optional[dict] = None):
+    """Returns (l2 [m x K], maf [m], n_pairs, any_full_chr_window).  With a
+    ``work`` dict, also fills in the f64 chunk Grams' dot products computed
+    (``n_dots``) and their wall time (``gemm_secs``)."""
     lib = _load()
     m = len(a.chr)
     bpr = (a.n_file_indiv + 3) // 4
@@ -131,6 +134,9 @@ def oracle_l2(a: OracleL2Args):
                        C.byref(info), err, 512)
     if rc != 0:
         raise ValueError(err.value.decode())
+    if work is not None:
+        work["n_dots"] = int(info.n_dots)
+        work["gemm_secs"] = float(info.gemm_secs)
     return l2, maf, int(info.n_pairs), bool(info.any_full_chr_window)
 
 

@@ -1,7 +1,8 @@
 """Sharded l2 over two ranks (gloo, CPU).  The compute step is the C oracle
 standing in for each rank's GPU call; what is tested is the plan (cores
 balanced by pair count, halos from the left limits, aligned to the chunk grid
-without per-SNP windows) and the gather, against one unsharded oracle run.
+without per-SNP windows) and the tensor all-gather of the core rows, against
+one unsharded oracle run.
 src/l2/mod.rs:477-553 (chromosomes are independent),
 src/l2/compute.rs:1164-1184 (chunk windows), 1855-1867 (per-SNP windows)."""
 import os
@@ -40,6 +41,12 @@ def _worker(rank, world, port, masking, result_path):
             return l2
 
         out = run_sharded(compute, snps, plan, rank)
+        # the gather also takes torch tensors, and every rank can receive the result
+        import torch
+        every = run_sharded(lambda rec: torch.from_numpy(compute(rec)), snps, plan, rank, dst=None)
+        np.testing.assert_array_equal(every, out if rank == 0 else every)
+        if rank == 1:
+            np.save(result_path + ".rank1.npy", every)
         if rank == 0:
             np.save(result_path, out)
             np.save(result_path + ".plan.npy", np.array([[s.core_lo, s.core_hi, s.call_lo, s.call_hi] for s in plan]))
@@ -62,6 +69,7 @@ def test_two_ranks_equal_one_run(tmp_path, masking):
     mp.spawn(_worker, args=(2, _free_port(), masking, res), nprocs=2, join=True)
     got = np.load(res)
     plan = np.load(res + ".plan.npy")
+    np.testing.assert_array_equal(np.load(res + ".rank1.npy"), got)
     spec, body, chr_, cm, bp = _panel()
     ref, _, _, _ = oracle_l2(OracleL2Args(bed_body=body, n_file_indiv=spec.n_indiv, chr=chr_, cm=cm, bp=bp,
                                           chunk_c=200, masking=masking))
