@@ -88,6 +88,9 @@ typedef struct {
     uint32_t gram_kind;         /* 0 fp64, 1 int8 tcgen05, 2 fp32 sketch */
     double device_ms;           /* whole call, device time */
     double contract_secs;       /* K > 1: the annotation contraction passes (inside ab_dot_secs) */
+    double layout_secs;         /* --sketch: wall time spent building the CountSketch layout (hash,
+                                   bucket-major order, panel rows rewritten in it); 0 when this call
+                                   reused a layout built earlier */
 } ldsc_perf;
 
 /* Arguments of one l2 computation.  Record i of the call is BED row
@@ -140,8 +143,17 @@ int ldsc_abi_version(void);
 
 /* Create a context on CUDA device `device` (the reference creates one
  * GpuContext per run and shares it across chromosomes: src/l2/mod.rs:410-436).
- * flags: reserved, pass 0. */
+ * flags: 0, or LDSC_CTX_STAGED_OPERANDS. */
 int ldsc_ctx_create(int device, uint32_t flags, ldsc_ctx **out);
+
+/* Context flag: run the INT8-exact form as two passes -- decode the panel
+ * into INT8 genotype / mask operand rows in device memory (2 bytes per
+ * individual per SNP), then the band Gram over them -- instead of the default
+ * fused Gram, which stages the packed 2-bit rows and expands them in shared
+ * memory.  Results agree to rounding (the same integer sums); the fused form
+ * needs no operand buffer.  Runs with --keep, or whose records are not
+ * consecutive panel rows, always take the two-pass form. */
+#define LDSC_CTX_STAGED_OPERANDS 1u
 int ldsc_ctx_destroy(ldsc_ctx *ctx);
 
 /* Launch this context's work on an existing cudaStream_t (NULL = the

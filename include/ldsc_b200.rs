@@ -15,7 +15,7 @@ pub struct LdscPerf { pub m: u64, pub n_indiv: u64, pub bed_read_secs: f64, pub 
                       pub sketch_secs: f64, pub bb_dot_secs: f64, pub ab_dot_secs: f64,
                       pub ring_store_secs: f64, pub n_pairs: u64, pub n_tiles: u64,
                       pub kernel_launches: u32, pub gram_kind: u32, pub device_ms: f64,
-                      pub contract_secs: f64 }
+                      pub contract_secs: f64, pub layout_secs: f64 }
 
 #[repr(C)]
 pub struct LdscL2Args {

@@ -31,6 +31,7 @@ STATUS_NAMES = {
 
 WINDOW_CM, WINDOW_KB, WINDOW_SNP = 0, 1, 2
 PRECISION_FP64, PRECISION_INT8 = 0, 1
+CTX_STAGED_OPERANDS = 1   # context flag: INT8 form through materialised operand rows
 
 
 class Progress(C.Structure):
@@ -48,7 +49,8 @@ class Perf(C.Structure):
                 ("bb_dot_secs", C.c_double), ("ab_dot_secs", C.c_double),
                 ("ring_store_secs", C.c_double), ("n_pairs", C.c_uint64),
                 ("n_tiles", C.c_uint64), ("kernel_launches", C.c_uint32),
-                ("gram_kind", C.c_uint32), ("device_ms", C.c_double), ("contract_secs", C.c_double)]
+                ("gram_kind", C.c_uint32), ("device_ms", C.c_double), ("contract_secs", C.c_double),
+                ("layout_secs", C.c_double)]
 
 
 class L2Args(C.Structure):

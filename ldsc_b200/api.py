@@ -65,6 +65,7 @@ class L2Perf:
     gram_kind: str
     device_ms: float
     contract_secs: float = 0.0
+    layout_secs: float = 0.0
 
 
 def _perf(p: L.Perf) -> L2Perf:
@@ -72,16 +73,19 @@ def _perf(p: L.Perf) -> L2Perf:
                   None if p.sketch_secs < 0 else p.sketch_secs, p.bb_dot_secs, p.ab_dot_secs,
                   p.ring_store_secs, int(p.n_pairs), int(p.n_tiles), int(p.kernel_launches),
                   {0: "fp64", 1: "int8", 2: "fp32-sketch"}.get(int(p.gram_kind), "?"),
-                  p.device_ms, p.contract_secs)
+                  p.device_ms, p.contract_secs, p.layout_secs)
 
 
 class Context:
     """One engine context on a CUDA device (GpuContext, src/gpu.rs:92-130)."""
 
-    def __init__(self, device: int = 0):
+    def __init__(self, device: int = 0, staged_operands: bool = False):
+        """staged_operands: run the INT8 form as decode-to-operand-rows then
+        Gram (LDSC_CTX_STAGED_OPERANDS) instead of the fused packed-row Gram."""
         self.lib = L.load()
         h = C.c_void_p()
-        rc = self.lib.ldsc_ctx_create(int(device), 0, C.byref(h))
+        flags = L.CTX_STAGED_OPERANDS if staged_operands else 0
+        rc = self.lib.ldsc_ctx_create(int(device), flags, C.byref(h))
         if rc != L.LDSC_OK:
             raise LdscError(rc, f"could not create a context on CUDA device {device}")
         self.h = h

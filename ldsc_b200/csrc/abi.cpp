@@ -109,6 +109,7 @@ struct SketchCache {
 
 struct ldsc_ctx {
     int device = 0;
+    uint32_t flags = 0;
     int sms = 148;
     cudaStream_t own = nullptr;
     cudaStream_t stream = nullptr;
@@ -117,7 +118,7 @@ struct ldsc_ctx {
     std::string last_error;
     uint64_t kernels = 0;
     // workspace (grow-only)
-    DevBuf ops, xf64, xsk, recrows, keep, left, tiles, annot, aeff, aeff32, l2, maf, pq, err;
+    DevBuf ops, xf64, xsk, recrows, keep, left, tiles, annot, aeff, l2, maf, pq, err;
     DevBuf st_n, st_s, st_q, st_q3, st_q4, st_mean, st_inv, st_qinv, st_kappa, packed, tsum, dbg;
     // private CountSketch layout (explicit bucket/sign arrays, or a panel
     // whose shared layout is in use under another key)
@@ -141,7 +142,7 @@ struct ldsc_ctx {
 
     std::vector<DevBuf*> workspace() {
         return {&ops, &xf64, &xsk, &recrows, &keep, &left,
-                      &tiles, &annot, &aeff, &aeff32, &l2, &maf,
+                      &tiles, &annot, &aeff, &l2, &maf,
                       &pq, &err, &st_n, &st_s, &st_q, &st_q3,
                       &st_q4, &st_mean, &st_inv, &st_qinv, &st_kappa,
                       &packed, &tsum, &dbg,
@@ -190,8 +191,7 @@ extern "C" {
 int ldsc_abi_version(void) { return LDSC_B200_ABI_VERSION; }
 
 int ldsc_ctx_create(int device, uint32_t flags, ldsc_ctx** out) {
-    (void)flags;
-    if (!out) return LDSC_E_INVALID;
+    if (!out || (flags & ~LDSC_CTX_STAGED_OPERANDS)) return LDSC_E_INVALID;
     *out = nullptr;
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
@@ -203,8 +203,26 @@ int ldsc_ctx_create(int device, uint32_t flags, ldsc_ctx** out) {
     cudaDeviceProp prop;
     if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return LDSC_E_CUDA;
     if (prop.major != 10) return LDSC_E_UNSUPPORTED;  // sm_100a kernels only
+    {
+        // every kernel of the library is loaded on this device before the
+        // context's first launch (a lazy load in the middle of a run can stall
+        // the work of other contexts on the device)
+        static std::mutex preload_mu;
+        static std::vector<int> preloaded;
+        std::lock_guard<std::mutex> g(preload_mu);
+        if (std::find(preloaded.begin(), preloaded.end(), device) == preloaded.end()) {
+            for (cudaError_t (*f)() : {preload_gram_tc, preload_gram_simt, preload_decode, preload_sketch,
+                                       preload_contract, preload_synth, preload_regress, preload_partitioned})
+                if (f() != cudaSuccess) {
+                    cudaGetLastError();
+                    return LDSC_E_CUDA;
+                }
+            preloaded.push_back(device);
+        }
+    }
     ldsc_ctx* c = new ldsc_ctx();
     c->device = device;
+    c->flags = flags;
     c->sms = prop.multiProcessorCount;
     if (cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking) != cudaSuccess) {
@@ -425,12 +443,14 @@ int ldsc_l2_workspace_bytes(const ldsc_l2_args* a, uint64_t n_indiv, uint64_t* b
     const uint64_t ntiles = band_tiles(L.left, ta, tb).size();
     uint64_t b = m * (12 + 32 + 16 * K) + 8 * m + 8 * (ntiles + 1) + 64;  // stats, l2/aeff, left, tiles
     if (d && a->sketch_maf_aware) b += 16 * m;
-    if (K > 1) b += 4 * m * K + (uint64_t)4 * ta * tb * ntiles + 8 * ntiles + 4 * (m / 64 + m / 128 + 4);
+    if (K > 1) b += (uint64_t)8 * ta * tb * ntiles + 8 * ntiles + 4 * (m / 64 + m / 128 + 4);  // f64 r2u tiles, lists
     if (a->annot && !a->annot_on_device) b += 8 * m * K;
     if (a->bed_idx) b += 8 * m;
     if (a->keep_iids) b += 8 * a->n_keep;
-    if (exact_i8) b += 2 * m * round_up(n_used, 128);
+    // INT8 operand rows only when the Gram cannot read the packed rows in place
+    if (exact_i8 && (a->bed_idx || a->keep_iids)) b += 2 * m * round_up(n_used, 128);
     else if (d) b += 8 * m * round_up(d, 32);
+    else if (exact_i8) b += 0;
     else b += 8 * m * round_up(n_used, 128);
     *bytes = b;
     return LDSC_OK;
@@ -638,12 +658,28 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
     }
     if (a->annot && a->annot_ld && a->annot_ld < (uint64_t)m)
         return fail(ctx, LDSC_E_INVALID, "annot_ld is smaller than the number of SNP records");
+    // records that are consecutive panel rows run as a row range (no record
+    // list on the device; the INT8 Gram can read the packed rows in place)
+    ldsc_l2_args as_range;
+    if (m > 0 && a->bed_idx) {
+        bool consecutive = true;
+        for (int64_t i = 1; i < m && consecutive; i++) consecutive = a->bed_idx[i] == a->bed_idx[0] + (uint64_t)i;
+        if (consecutive) {
+            as_range = *a;
+            as_range.row_begin = a->bed_idx[0];
+            as_range.bed_idx = nullptr;
+            a = &as_range;
+        }
+    }
     if (m == 0) {
         if (perf) *perf = pf;
         return LDSC_OK;
     }
 
     const bool exact_i8 = !d && a->precision == LDSC_PRECISION_INT8;
+    // the INT8 Gram reads the packed rows in place when the records are the
+    // panel rows in order and every individual is used
+    const bool fused_i8 = exact_i8 && !a->bed_idx && !a->keep_iids && !(ctx->flags & LDSC_CTX_STAGED_OPERANDS);
     const int ta = (exact_i8 || d) ? 64 : 128, tb = 128;  // tcgen05 tiles: 64 x 128 records
     pf.gram_kind = d ? 2u : (exact_i8 ? 1u : 0u);
 
@@ -669,7 +705,6 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
         CK(ctx->st_q4.ensure(4 * nmom));
         CK(ctx->st_kappa.ensure(8 * nmom));
     }
-    if (K > 1) CK(ctx->aeff32.ensure(4 * nmom * K));
     if (a->annot && !a->annot_on_device) CK(ctx->annot.ensure(8 * nmom * K));
     if (a->bed_idx) CK(ctx->recrows.ensure(8 * nmom));
     if (a->keep_iids) CK(ctx->keep.ensure(8 * a->n_keep));
@@ -760,9 +795,11 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
         {
             std::lock_guard<std::mutex> g(panel->mu);
             if (!panel->sk.matches(n_used, d, key) && panel->sk_users == 0) {
+                const auto tl0 = std::chrono::steady_clock::now();
                 hash();
                 int rc = sketch_prepare(ctx, panel, n_used, d, bucket.data(), sign.data(), a->keep_iids, key, panel->sk);
                 if (rc != LDSC_OK) return rc;
+                pf.layout_secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - tl0).count();
             }
             if (panel->sk.matches(n_used, d, key)) {
                 panel->sk_users++;
@@ -772,11 +809,13 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
         }
         if (!skc) {
             if (!(ctx->sk_panel == panel->id && ctx->sk.matches(n_used, d, key))) {
+                const auto tl0 = std::chrono::steady_clock::now();
                 if (bucket.empty()) hash();
                 ctx->sk_panel = 0;
                 int rc = sketch_prepare(ctx, panel, n_used, d, bucket.data(), sign.data(), a->keep_iids, key, ctx->sk);
                 if (rc != LDSC_OK) return rc;
                 ctx->sk_panel = panel->id;
+                pf.layout_secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - tl0).count();
             }
             skc = &ctx->sk;
         }
@@ -816,7 +855,7 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
                 idx_r[fr[tiles[t].b_blk]++] = t;
                 idx_l[fl[tiles[t].a_blk]++] = t;
             }
-            CK(ctx->rtiles.ensure(sizeof(float) * (size_t)ta * tb * tiles.size()));
+            CK(ctx->rtiles.ensure(sizeof(double) * (size_t)ta * tb * tiles.size()));
             CK(ctx->cptr_r.ensure(4 * ptr_r.size()));
             CK(ctx->cidx_r.ensure(4 * idx_r.size()));
             CK(ctx->cptr_l.ensure(4 * ptr_l.size()));
@@ -838,7 +877,6 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
     ep.qinv = st.qinv;
     ep.kappa = st.kappa;
     ep.aeff = ctx->aeff.as<double>();
-    ep.aeff32 = K > 1 ? ctx->aeff32.as<float>() : nullptr;
     ep.l2 = ctx->l2.as<double>();
     ep.m = m;
     ep.K = K;
@@ -877,7 +915,8 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
     const uint64_t ld_i8 = round_up(n_used, 128);
     const uint64_t ld_sk = round_up(d ? d : 1, 32);  // 128-byte operand rows for TMA
     int e_sk = -1;
-    if (exact_i8) CK(ctx->ops.ensure((size_t)2 * nmom * ld_i8));
+    const bool staged_i8 = exact_i8 && !fused_i8;
+    if (staged_i8) CK(ctx->ops.ensure((size_t)2 * nmom * ld_i8));
     if (chunked) {
         // records [r0, r1) whose rows arrived with chunks [0, k]
         int64_t r0 = 0;
@@ -898,8 +937,8 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
                 sc.n += r0;
                 sc.s += r0;
                 sc.q += r0;
-                uint8_t* oc = exact_i8 ? ctx->ops.as<uint8_t>() + (size_t)2 * r0 * ld_i8 : nullptr;
-                CK(launch_decode_i8(pc, rr ? rr + r0 : nullptr, r1 - r0, sel, oc, exact_i8 ? ld_i8 : 0, sc, 0, s));
+                uint8_t* oc = staged_i8 ? ctx->ops.as<uint8_t>() + (size_t)2 * r0 * ld_i8 : nullptr;
+                CK(launch_decode_i8(pc, rr ? rr + r0 : nullptr, r1 - r0, sel, oc, staged_i8 ? ld_i8 : 0, sc, 0, s));
                 ctx->kernels++;
                 if (stream_gram) {
                     sc.maf += r0;
@@ -907,15 +946,19 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
                     sc.inv_std += r0;
                     sc.qinv += r0;
                     CK(launch_finalize_stats(r1 - r0, n_used, sc, annot_dev ? annot_dev + r0 : nullptr, 1,
-                                             a->has_pq_exp, a->pq_exp, ctx->aeff.as<double>() + r0, nullptr,
+                                             a->has_pq_exp, a->pq_exp, ctx->aeff.as<double>() + r0,
                                              ctx->l2.as<double>() + r0, s, annot_ld_dev));
                     ctx->kernels++;
                     // tiles are ordered by right block; take those whose right block is complete
                     size_t t1 = t0;
                     while (t1 < tiles.size() && (r1 == m || (int64_t)(tiles[t1].b_blk + 1) * tb <= r1)) t1++;
                     if (t1 > t0) {
-                        CK(launch_gram_i8(ctx->ops.as<uint8_t>(), ld_i8, m, ctx->tiles.as<Tile>() + t0,
-                                          (int64_t)(t1 - t0), ep, nullptr, ctx->sms, s));
+                        if (fused_i8)
+                            CK(launch_gram_i8_packed(pv.rows, pv.pitch, n_used, m, ctx->tiles.as<Tile>() + t0,
+                                                     (int64_t)(t1 - t0), ep, nullptr, ctx->sms, s));
+                        else
+                            CK(launch_gram_i8(ctx->ops.as<uint8_t>(), ld_i8, m, ctx->tiles.as<Tile>() + t0,
+                                              (int64_t)(t1 - t0), ep, nullptr, ctx->sms, s));
                         ctx->kernels++;
                     }
                     t0 = t1;
@@ -924,7 +967,7 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
             r0 = r1;
         }
         ctx->kernels--;  // counted once below
-    } else if (exact_i8) {
+    } else if (staged_i8) {
         CK(launch_decode_i8(pv, rr, m, sel, ctx->ops.as<uint8_t>(), ld_i8, st, 0, s));
     } else if (d) {
         // fused: moments + CountSketch rows in one pass over the permuted panel
@@ -938,7 +981,7 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
     ctx->kernels++;
     if (!stream_gram) {
         CK(launch_finalize_stats(m, n_used, st, annot_dev, K, a->has_pq_exp, a->pq_exp, ctx->aeff.as<double>(),
-                                 K > 1 ? ctx->aeff32.as<float>() : nullptr, ctx->l2.as<double>(), s, annot_ld_dev));
+                                 ctx->l2.as<double>(), s, annot_ld_dev));
         ctx->kernels++;
     }
     const uint64_t ld_f64 = round_up(n_used, 128);
@@ -954,7 +997,7 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
         int rc = plan();
         if (rc != LDSC_OK) return rc;
         ep.left = ctx->left.as<int64_t>();
-        ep.rtiles = (K > 1 && !tiles.empty()) ? ctx->rtiles.as<float>() : nullptr;
+        ep.rtiles = (K > 1 && !tiles.empty()) ? ctx->rtiles.as<double>() : nullptr;
     }
     // ---- band Gram + epilogue ----
     const int e2 = ev.mark();
@@ -963,6 +1006,9 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
         if (d) {
             CK(launch_gram_tf32(ctx->xsk.as<float>(), ld_sk, m, ctx->tiles.as<Tile>(), (int64_t)tiles.size(), ep,
                                 maf_aware ? 1 : 0, nullptr, ctx->sms, s));
+        } else if (fused_i8) {
+            CK(launch_gram_i8_packed(pv.rows, pv.pitch, n_used, m, ctx->tiles.as<Tile>(), (int64_t)tiles.size(), ep,
+                                     nullptr, ctx->sms, s));
         } else if (exact_i8) {
             CK(launch_gram_i8(ctx->ops.as<uint8_t>(), ld_i8, m, ctx->tiles.as<Tile>(), (int64_t)tiles.size(), ep,
                               nullptr, ctx->sms, s));
@@ -973,9 +1019,9 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
         ctx->kernels++;
         e_c = ev.mark();
         if (K > 1) {
-            CK(launch_contract(ctx->rtiles.as<float>(), ta, tb, ctx->tiles.as<Tile>(), ctx->cptr_r.as<int32_t>(),
+            CK(launch_contract(ctx->rtiles.as<double>(), ta, tb, ctx->tiles.as<Tile>(), ctx->cptr_r.as<int32_t>(),
                                ctx->cidx_r.as<int32_t>(), n_right, true, ep, s));
-            CK(launch_contract(ctx->rtiles.as<float>(), ta, tb, ctx->tiles.as<Tile>(), ctx->cptr_l.as<int32_t>(),
+            CK(launch_contract(ctx->rtiles.as<double>(), ta, tb, ctx->tiles.as<Tile>(), ctx->cptr_l.as<int32_t>(),
                                ctx->cidx_l.as<int32_t>(), n_left, false, ep, s));
             ctx->kernels += 2;
         }
@@ -1193,7 +1239,8 @@ int ldsc_debug_gram_i8_tile(ldsc_ctx* ctx, const ldsc_panel* panel, uint64_t k0,
     const uint64_t ld = round_up(n, 128);
     cudaStream_t s = ctx->stream;
     CK(cudaSetDevice(ctx->device));
-    CK(ctx->ops.ensure((size_t)2 * m * ld));
+    const bool fused = !(ctx->flags & LDSC_CTX_STAGED_OPERANDS);
+    if (!fused) CK(ctx->ops.ensure((size_t)2 * m * ld));
     CK(ctx->st_n.ensure(4 * (size_t)m));
     CK(ctx->st_s.ensure(4 * (size_t)m));
     CK(ctx->st_q.ensure(4 * (size_t)m));
@@ -1217,8 +1264,8 @@ int ldsc_debug_gram_i8_tile(ldsc_ctx* ctx, const ldsc_panel* panel, uint64_t k0,
     st.mean = ctx->st_mean.as<double>();
     st.inv_std = ctx->st_inv.as<double>();
     st.qinv = ctx->st_qinv.as<double>();
-    CK(launch_decode_i8(pv, nullptr, m, sel, ctx->ops.as<uint8_t>(), ld, st, 0, s));
-    CK(launch_finalize_stats(m, n, st, nullptr, 1, 0, 0.0, ctx->aeff.as<double>(), nullptr, ctx->l2.as<double>(), s));
+    CK(launch_decode_i8(pv, nullptr, m, sel, fused ? nullptr : ctx->ops.as<uint8_t>(), fused ? 0 : ld, st, 0, s));
+    CK(launch_finalize_stats(m, n, st, nullptr, 1, 0, 0.0, ctx->aeff.as<double>(), ctx->l2.as<double>(), s));
     CK(cudaMemsetAsync(ctx->left.p, 0, 8 * (size_t)m, s));
     CK(cudaMemsetAsync(ctx->err.p, 0, 16, s));
     Tile t{(uint32_t)(k0 / 64), (uint32_t)(j0 / 128)};
@@ -1235,8 +1282,12 @@ int ldsc_debug_gram_i8_tile(ldsc_ctx* ctx, const ldsc_panel* panel, uint64_t k0,
     ep.r2u_a = 1.0;
     ep.r2u_b = 0.0;
     ep.err = ctx->err.as<unsigned int>();
-    CK(launch_gram_i8(ctx->ops.as<uint8_t>(), ld, m, ctx->tiles.as<Tile>(), 1, ep, ctx->dbg.as<int32_t>(),
-                      ctx->sms, s));
+    if (fused)
+        CK(launch_gram_i8_packed(panel->rows, panel->pitch, n, m, ctx->tiles.as<Tile>(), 1, ep,
+                                 ctx->dbg.as<int32_t>(), ctx->sms, s));
+    else
+        CK(launch_gram_i8(ctx->ops.as<uint8_t>(), ld, m, ctx->tiles.as<Tile>(), 1, ep, ctx->dbg.as<int32_t>(),
+                          ctx->sms, s));
     ctx->kernels += 3;
     unsigned int herr[4];
     CK(cudaMemcpyAsync(out, ctx->dbg.p, 4 * 128 * 256, cudaMemcpyDeviceToHost, s));

@@ -135,7 +135,7 @@ __global__ void __launch_bounds__(256) k_decode_i8(PanelView p, const uint64_t* 
 // term r2u_jj * a_j = a_j.
 __global__ void k_finalize(int64_t m, uint64_t n_indiv, RecStats st, const double* __restrict__ annot,
                            uint64_t annot_ld, int32_t K, int has_pq, double pq_exp, double* __restrict__ aeff,
-                           float* __restrict__ aeff32, double* __restrict__ l2_init) {
+                           double* __restrict__ l2_init) {
     int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= m) return;
     const int64_t n = st.n[r], s = st.s[r], q = st.q[r];
@@ -175,7 +175,6 @@ __global__ void k_finalize(int64_t m, uint64_t n_indiv, RecStats st, const doubl
         double a = annot ? annot[r + c * annot_ld] : 1.0;
         a *= pq;
         aeff[r + (int64_t)c * m] = a;
-        if (aeff32) aeff32[r * K + c] = (float)a;
         l2_init[r + (int64_t)c * m] = a;
     }
 }
@@ -258,12 +257,12 @@ cudaError_t launch_repitch(const uint8_t* src, uint64_t bpr, uint8_t* dst, uint6
 }
 
 cudaError_t launch_finalize_stats(int64_t m, uint64_t n_indiv, RecStats st, const double* annot,
-                                  int32_t K, int has_pq, double pq_exp, double* aeff, float* aeff32,
+                                  int32_t K, int has_pq, double pq_exp, double* aeff,
                                   double* l2_init, cudaStream_t stream, uint64_t annot_ld) {
     if (m <= 0) return cudaSuccess;
     k_finalize<<<(unsigned)((m + 255) / 256), 256, 0, stream>>>(m, n_indiv, st, annot,
                                                               annot_ld ? annot_ld : (uint64_t)m, K, has_pq,
-                                                              pq_exp, aeff, aeff32, l2_init);
+                                                              pq_exp, aeff, l2_init);
     return cudaGetLastError();
 }
 
@@ -272,6 +271,14 @@ cudaError_t launch_decode_f64(const PanelView& p, const uint64_t* rec_rows, int6
     if (m <= 0) return cudaSuccess;
     k_decode_f64<<<decode_grid(m), 256, 0, stream>>>(p, rec_rows, m, sel, st, x, ld);
     return cudaGetLastError();
+}
+
+cudaError_t preload_decode() {
+    cudaError_t e = preload_kernel(k_decode_i8);
+    if (e == cudaSuccess) e = preload_kernel(k_finalize);
+    if (e == cudaSuccess) e = preload_kernel(k_decode_f64);
+    if (e == cudaSuccess) e = preload_kernel(k_repitch);
+    return e;
 }
 
 }  // namespace ldsc

@@ -53,7 +53,6 @@ struct EpilogueArgs {
     const double* qinv;
     const double* kappa;      // sketch MAF-aware, else null
     const double* aeff;       // M x K column-major effective annotation (f64)
-    const float* aeff32;      // M x K row-major effective annotation (f32, K > 1 path)
     double* l2;               // M x K column-major output accumulator
     int64_t m;                // records
     int32_t K;                // annotation columns
@@ -63,7 +62,7 @@ struct EpilogueArgs {
     double n_inv_sq;          // 1 / N^2       (sketch form)
     double sketch_d;          // d as double   (sketch form)
     unsigned int* err;        // device error word (non-zero = a bounded wait gave up)
-    float* rtiles;            // K > 1: tile t's masked r2u values, ta x tb f32 at t * ta * tb
+    double* rtiles;           // K > 1: tile t's masked r2u values, ta rows (k) x tb (j) f64 at t * ta * tb
 };
 
 // ---- kernels (launchers return cudaError_t of the launch) ----
@@ -77,7 +76,7 @@ cudaError_t launch_decode_i8(const PanelView& p, const uint64_t* rec_rows, int64
 // Finalise per-record stats: maf, mean, inv_std, qinv, pq, kappa, aeff.
 cudaError_t launch_finalize_stats(int64_t m, uint64_t n_indiv, RecStats st,
                                   const double* annot, int32_t K, int has_pq, double pq_exp,
-                                  double* aeff, float* aeff32, double* l2_init,
+                                  double* aeff, double* l2_init,
                                   cudaStream_t stream, uint64_t annot_ld = 0);
 
 // Standardised f64 columns, row r of `x` = record r, `ld` doubles per row.
@@ -101,6 +100,15 @@ cudaError_t launch_gram_f64(const double* x, uint64_t ld, uint64_t kdim, const T
 cudaError_t launch_gram_i8(const uint8_t* ops, uint64_t ld, int64_t m, const Tile* tiles,
                            int64_t n_tiles, const EpilogueArgs& ep, int32_t* dbg, int sms,
                            cudaStream_t stream);
+
+// Fused INT8 band Gram over the packed BED rows themselves (record r at
+// rows + r * pitch, all n_indiv individuals): the kernel stages 2-bit rows by
+// TMA and expands them into the G / M operand tiles in shared memory, so no
+// operand rows exist in device memory.  Same tiles, epilogue and results as
+// launch_gram_i8; the per-record n / s / qinv come from a moments-only decode.
+cudaError_t launch_gram_i8_packed(const uint8_t* rows, uint64_t pitch, uint64_t n_indiv, int64_t m, const Tile* tiles,
+                                  int64_t n_tiles, const EpilogueArgs& ep, int32_t* dbg, int sms,
+                                  cudaStream_t stream);
 
 // CountSketch, step 1 (once per panel, sketch dimension and individual set):
 // rewrite every panel row in bucket-major individual order, perm[p] = FAM
@@ -146,9 +154,27 @@ cudaError_t launch_gram_f32(const float* x, uint64_t ld, uint64_t kdim, const Ti
 //   by right block:  l2[j, C] += sum over tiles of block, sum_k R[k][j] a[k, C]
 //   by left block:   l2[k, C] += sum over tiles of block, sum_j R[k][j] a[j, C]
 // ptr/idx: CSR lists of tile indices per right block (by_right) or per left block.
-cudaError_t launch_contract(const float* rtiles, int ta, int tb, const Tile* tiles, const int32_t* ptr,
+cudaError_t launch_contract(const double* rtiles, int ta, int tb, const Tile* tiles, const int32_t* ptr,
                             const int32_t* idx, int32_t nblocks, bool by_right, const EpilogueArgs& ep,
                             cudaStream_t stream);
+
+// Load a kernel's code on the current device now.  With lazy module loading
+// (the CUDA 12 default) a kernel is loaded at its first launch, which can
+// stall work already running on the device; contexts load every kernel of the
+// library when they are created (preload_* below, one per source file).
+template <typename F>
+cudaError_t preload_kernel(F* kernel) {
+    cudaFuncAttributes a;
+    return cudaFuncGetAttributes(&a, reinterpret_cast<const void*>(kernel));
+}
+cudaError_t preload_gram_tc();
+cudaError_t preload_gram_simt();
+cudaError_t preload_decode();
+cudaError_t preload_sketch();
+cudaError_t preload_contract();
+cudaError_t preload_synth();
+cudaError_t preload_regress();
+cudaError_t preload_partitioned();
 
 // Synthetic panel generator (founder mosaic, counter-based RNG).
 cudaError_t launch_synth(uint8_t* rows, uint64_t pitch, uint64_t n_indiv, uint64_t n_snp,

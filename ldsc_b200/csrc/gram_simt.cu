@@ -37,7 +37,6 @@ __device__ __forceinline__ void cp_elem(T* dst, const T* src, bool valid) {
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
-constexpr int RLD = TB + 1;  // padded row stride of the staged R tile
 
 template <int MODE>
 __device__ __forceinline__ double correct(double v, int64_t k, int64_t j, const EpilogueArgs& ep) {
@@ -155,29 +154,21 @@ __global__ void __launch_bounds__(NT, 1)
             }
             __syncthreads();
         } else {
-            float* Rs = reinterpret_cast<float*>(smem_raw);  // [TA][RLD]
+            // K > 1: the masked r2u tile goes to global memory in f64 (row k of
+            // TB values) for the banded annotation contraction (contract.cu);
+            // the 16 lanes of a row store 128 contiguous bytes
+            double* dst = ep.rtiles + (size_t)t * TA * TB;
 #pragma unroll
             for (int i = 0; i < 8; i++) {
                 const int64_t k = k0 + ty + 16 * i;
 #pragma unroll
                 for (int l = 0; l < 8; l++) {
                     const int64_t j = j0 + tx + 16 * l;
-                    float r = 0.f;
-                    if (pair_in_band(k, j, m, ep.left))
-                        r = (float)correct<MODE>((double)acc[i][l], k, j, ep);
-                    Rs[(ty + 16 * i) * RLD + tx + 16 * l] = r;
+                    double r = 0.0;
+                    if (pair_in_band(k, j, m, ep.left)) r = correct<MODE>((double)acc[i][l], k, j, ep);
+                    dst[(ty + 16 * i) * TB + tx + 16 * l] = r;
                 }
             }
-            __syncthreads();
-            // K > 1: the masked r2u tile goes to global memory for the banded
-            // annotation contraction (contract.cu)
-            float4* dst = reinterpret_cast<float4*>(ep.rtiles + (size_t)t * TA * TB);
-            for (int q = tid; q < TA * TB / 4; q += NT) {
-                const int e = q * 4, rr = e / TB, cc = e % TB;
-                dst[q] = make_float4(Rs[rr * RLD + cc], Rs[rr * RLD + cc + 1], Rs[rr * RLD + cc + 2],
-                                     Rs[rr * RLD + cc + 3]);
-            }
-            __syncthreads();
         }
     }
 }
@@ -188,10 +179,8 @@ cudaError_t launch(const T* x, uint64_t ld, uint64_t kdim, const Tile* tiles, in
     if (n_tiles <= 0) return cudaSuccess;
     size_t op_bytes = sizeof(T) * NSTAGE * (TA + TB) * SK;
     size_t cpart_bytes = sizeof(double) * 16 * TB;
-    size_t r_bytes = ep.K > 1 ? sizeof(float) * TA * RLD : 0;
     size_t smem = op_bytes;
     if (cpart_bytes > smem) smem = cpart_bytes;
-    if (r_bytes > smem) smem = r_bytes;
     cudaError_t e = cudaFuncSetAttribute(k_gram_simt<T, MODE>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -212,6 +201,13 @@ cudaError_t launch_gram_f32(const float* x, uint64_t ld, uint64_t kdim, const Ti
                             cudaStream_t stream) {
     if (maf_aware) return launch<float, 2>(x, ld, kdim, tiles, n_tiles, ep, sms, stream);
     return launch<float, 1>(x, ld, kdim, tiles, n_tiles, ep, sms, stream);
+}
+
+cudaError_t preload_gram_simt() {
+    cudaError_t e = preload_kernel(k_gram_simt<double, 0>);
+    if (e == cudaSuccess) e = preload_kernel(k_gram_simt<float, 1>);
+    if (e == cudaSuccess) e = preload_kernel(k_gram_simt<float, 2>);
+    return e;
 }
 
 }  // namespace ldsc

@@ -32,10 +32,22 @@
 //   warps 2-5  epilogue: tcgen05.ld of the accumulator, exact r^2, band mask,
 //              l2 accumulation; accumulator double-buffering overlaps the
 //              epilogue of tile t with the MMAs of tile t+1.  Where the
-//              epilogue outweighs the MMAs -- the sketch forms (short K, a
-//              heavier per-pair correction) and INT8 rows of fewer than
-//              32,768 individuals -- warps 2-9 do it: two warps per TMEM lane
-//              quarter, each on half the columns.
+//              epilogue outweighs the MMAs -- INT8 rows of fewer than 32,768
+//              individuals, and the sketch forms (short K, a heavier per-pair
+//              correction) -- warps 2-9 (2-17) do it: two (four) warps per
+//              TMEM lane quarter, each on a share of the columns.  With K > 1
+//              annotation columns the epilogue stores each tile's masked r2u
+//              values (f64) for the contraction passes of contract.cu.
+// Fused INT8 form (the operand rows are never written to HBM): warp 0 stages
+// the packed 2-bit BED rows themselves by TMA -- 32 bytes per record per 128
+// individuals, 6 KB per stage for the 64 + 128 records of a tile instead of
+// 48 KB of operand rows -- and four converter warps expand each packed stage
+// in shared memory into the 128-byte-swizzled G / M operand tiles the MMA warp
+// reads, with a proxy fence before they hand the stage over.  The K order of
+// individuals inside a 16-byte chunk is permuted (evens, then odds) the same
+// way in every row, which leaves every product sum unchanged; individuals past
+// N read as missing.
+//
 // Every mbarrier wait is bounded; on timeout the kernel records an error word,
 // drains its own in-flight copies / MMAs (bounded), frees TMEM and returns.
 #include <cuda.h>
@@ -53,9 +65,13 @@ constexpr int TA = 64;             // left records per tile (A rows = 128)
 constexpr int TB = 128;            // right records per tile (B rows = 256)
 constexpr int A_BYTES = 128 * 128; // one stage of A
 constexpr int B_BYTES = 256 * 128; // one stage of B
-// threads per CTA: TMA and MMA warps + ew epilogue warps (4 or 8)
-__host__ __device__ constexpr int gram_threads(int ew) { return 64 + 32 * ew; }
-constexpr int RLD = TB + 1;
+// fused form: packed ring of 2-bit rows, 128 individuals (32 bytes) per record per stage
+constexpr int P_STAGES = 4;
+constexpr int PA_BYTES = TA * 32;
+constexpr int P_BYTES = (TA + TB) * 32;
+constexpr int CONV_WARPS = 4;
+// threads per CTA: TMA and MMA warps + ew epilogue warps (4, 8 or 16) + cw converter warps
+__host__ __device__ constexpr int gram_threads(int ew, int cw) { return 64 + 32 * ew + 32 * cw; }
 constexpr uint64_t WAIT_LIMIT_NS = 2000000000ull;  // 2 s per wait
 
 __device__ __forceinline__ int64_t shfl_xor_i64(int64_t v, int mask) {
@@ -63,6 +79,34 @@ __device__ __forceinline__ int64_t shfl_xor_i64(int64_t v, int mask) {
     lo = __shfl_xor_sync(0xFFFFFFFFu, lo, mask);
     hi = __shfl_xor_sync(0xFFFFFFFFu, hi, mask);
     return ((int64_t)hi << 32) | (uint32_t)lo;
+}
+
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Genotype and non-missing bytes of 16 individuals from their code word
+// (count-A1 codes, src/bed.rs:470-521: 00 -> 2, 01 -> missing, 10 -> 1,
+// 11 -> 0).  Byte order in the chunk: individuals 0,2,..,14 then 1,3,..,15.
+__device__ __forceinline__ void expand_chunk(uint32_t w, uint4& g, uint4& mk) {
+    constexpr uint32_t TG = 0x00010002u;           // code c -> byte c of TG
+    constexpr uint32_t TM = 0x01010001u;
+    const uint32_t se = w & 0x33333333u;           // nibble i: code of individual 2i
+    const uint32_t so = (w >> 2) & 0x33333333u;    // nibble i: code of individual 2i + 1
+    const uint32_t se2 = se >> 16, so2 = so >> 16;
+    g.x = __byte_perm(TG, 0u, se);
+    g.y = __byte_perm(TG, 0u, se2);
+    g.z = __byte_perm(TG, 0u, so);
+    g.w = __byte_perm(TG, 0u, so2);
+    mk.x = __byte_perm(TM, 0u, se);
+    mk.y = __byte_perm(TM, 0u, se2);
+    mk.z = __byte_perm(TM, 0u, so);
+    mk.w = __byte_perm(TM, 0u, so2);
+}
+
+// Byte offset of 16-byte chunk c of row R in a K-major 128-byte-swizzled tile.
+__device__ __forceinline__ uint32_t sw128_off(int R, int c) {
+    return (uint32_t)((R >> 3) * 1024 + (R & 7) * 128 + ((c ^ (R & 7)) << 4));
 }
 
 // MODE 0: INT8 exact r^2; 1: TF32 sketch, quadratic correction; 2: same, MAF-aware.
@@ -77,11 +121,15 @@ __device__ __forceinline__ double sketch_r2u(float val, int64_t k, int64_t j, co
     return r2 * ep.r2u_a + ep.r2u_b;
 }
 
-template <int STAGES, int MODE, int EW>
-__global__ void __launch_bounds__(gram_threads(EW), 1)
+// CW = 0: A / B operand rows staged by TMA.  CW > 0 (INT8 only): packed 2-bit
+// rows staged by TMA (tmA / tmB map the BED rows, boxes of 32 bytes x 64 / 128
+// rows) and expanded by CW converter warps; n_indiv masks the last stage.
+template <int STAGES, int MODE, int EW, int CW>
+__global__ void __launch_bounds__(gram_threads(EW, CW), 1)
     k_gram_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
               int num_kb, const Tile* __restrict__ tiles, int64_t n_tiles, EpilogueArgs ep,
-              int32_t* __restrict__ dbg) {
+              int32_t* __restrict__ dbg, uint64_t n_indiv) {
+    static_assert(CW == 0 || MODE == 0, "the fused form is INT8 only");
     // elements per 128-byte stage row: 128 (INT8) or 32 (TF32); TMA x is in elements
     constexpr int KSTEP = MODE == 0 ? 128 : 32;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -89,21 +137,27 @@ __global__ void __launch_bounds__(gram_threads(EW), 1)
     uint8_t* smem = smem_raw + pad;
     uint8_t* sA = smem;
     uint8_t* sB = sA + STAGES * A_BYTES;
-    uint64_t* full = reinterpret_cast<uint64_t*>(sB + STAGES * B_BYTES);
+    uint8_t* sP = sB + STAGES * B_BYTES;   // fused form: packed ring
+    uint64_t* full = reinterpret_cast<uint64_t*>(sP + (CW > 0 ? P_STAGES * P_BYTES : 0));
     uint64_t* empty = full + STAGES;
-    uint64_t* tfull = empty + STAGES;   // [2]
+    uint64_t* pfull = empty + STAGES;   // [P_STAGES], fused form
+    uint64_t* pempty = pfull + P_STAGES;
+    uint64_t* tfull = pempty + P_STAGES;   // [2]
     uint64_t* tempty = tfull + 2;       // [2]
     uint64_t* drain = tempty + 2;       // [1]
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
     double* cpart = reinterpret_cast<double*>(drain + 2);  // [4][TB]
-    float* Rs = reinterpret_cast<float*>(cpart + 4 * TB);  // [TA][RLD], K > 1 only
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; s++) {
-            mbar_init(&full[s], 1);
+            mbar_init(&full[s], CW > 0 ? CW : 1);   // TMA transaction, or one arrival per converter warp
             mbar_init(&empty[s], 1);
+        }
+        for (int s = 0; s < P_STAGES; s++) {
+            mbar_init(&pfull[s], 1);
+            mbar_init(&pempty[s], CW > 0 ? CW : 1);
         }
         for (int b = 0; b < 2; b++) {
             mbar_init(&tfull[b], 1);
@@ -131,21 +185,32 @@ __global__ void __launch_bounds__(gram_threads(EW), 1)
             bool ok = true;
             uint32_t armed = 0;        // bit s: stage s has a load in flight we may need to drain
             uint32_t armed_par = 0;    // bit s: parity of that load's phase
+            // the ring this warp fills: operand stages, or packed stages in the fused form
+            constexpr int RING = CW > 0 ? P_STAGES : STAGES;
+            uint64_t* rfull = CW > 0 ? pfull : full;
+            uint64_t* rempty = CW > 0 ? pempty : empty;
             for (int64_t t = blockIdx.x; t < n_tiles && ok; t += gridDim.x) {
                 const Tile tl = tiles[t];
-                const int32_t ya = (int32_t)tl.a_blk * (2 * TA);
-                const int32_t yb = (int32_t)tl.b_blk * (2 * TB);
+                // operand rows: two per record; packed rows: one per record
+                const int32_t ya = (int32_t)tl.a_blk * (CW > 0 ? TA : 2 * TA);
+                const int32_t yb = (int32_t)tl.b_blk * (CW > 0 ? TB : 2 * TB);
                 for (int kb = 0; kb < num_kb; kb++) {
-                    if (!mbar_wait(&empty[stage], phase ^ 1, WAIT_LIMIT_NS)) {
+                    if (!mbar_wait(&rempty[stage], phase ^ 1, WAIT_LIMIT_NS)) {
                         ok = false;
                         break;
                     }
-                    mbar_arrive_expect_tx(&full[stage], A_BYTES + B_BYTES);
-                    tma_load_2d(sA + stage * A_BYTES, &tmA, &full[stage], kb * KSTEP, ya);
-                    tma_load_2d(sB + stage * B_BYTES, &tmB, &full[stage], kb * KSTEP, yb);
+                    if constexpr (CW > 0) {
+                        mbar_arrive_expect_tx(&rfull[stage], P_BYTES);
+                        tma_load_2d(sP + stage * P_BYTES, &tmA, &rfull[stage], kb * 32, ya);
+                        tma_load_2d(sP + stage * P_BYTES + PA_BYTES, &tmB, &rfull[stage], kb * 32, yb);
+                    } else {
+                        mbar_arrive_expect_tx(&rfull[stage], A_BYTES + B_BYTES);
+                        tma_load_2d(sA + stage * A_BYTES, &tmA, &rfull[stage], kb * KSTEP, ya);
+                        tma_load_2d(sB + stage * B_BYTES, &tmB, &rfull[stage], kb * KSTEP, yb);
+                    }
                     armed |= 1u << stage;
                     armed_par = (armed_par & ~(1u << stage)) | (phase << stage);
-                    if (++stage == STAGES) {
+                    if (++stage == RING) {
                         stage = 0;
                         phase ^= 1;
                     }
@@ -154,8 +219,8 @@ __global__ void __launch_bounds__(gram_threads(EW), 1)
             if (!ok) {
                 atomicOr(ep.err, 1u);
                 // our copies in flight must land before the CTA's smem is released
-                for (int s = 0; s < STAGES; s++)
-                    if (armed & (1u << s)) mbar_wait(&full[s], (armed_par >> s) & 1u, WAIT_LIMIT_NS);
+                for (int s = 0; s < RING; s++)
+                    if (armed & (1u << s)) mbar_wait(&rfull[s], (armed_par >> s) & 1u, WAIT_LIMIT_NS);
             }
         }
     } else if (warp == 1) {
@@ -211,6 +276,79 @@ __global__ void __launch_bounds__(gram_threads(EW), 1)
                 // all of this thread's MMAs complete before TMEM is freed
                 umma_commit(drain);
                 mbar_wait(drain, 0, WAIT_LIMIT_NS);
+            }
+        }
+    } else if (CW > 0 && warp >= 2 + EW) {
+        // ------------------------------------------------ converters (fused form)
+        // Thread ct takes 16-individual word wd of the stage's packed rows for
+        // records ct / 8 + RPP * i: the warp reads 128 contiguous packed bytes
+        // per pass, and each 8-thread phase of a 16-byte store fills one whole
+        // 128-byte operand row (no bank conflicts).
+        constexpr int RPP = 32 * (CW > 0 ? CW : 1) / 8;   // records per pass
+        constexpr int NPASS = (TA + TB) / RPP;
+        constexpr int APASS = TA / RPP;              // passes that fill the A tile
+        static_assert((TA + TB) % RPP == 0 && TA % RPP == 0, "converter passes");
+        const int ct = threadIdx.x - (64 + 32 * EW);
+        const int wd = ct & 7;
+        uint32_t offP[NPASS], offG[NPASS], offM[NPASS];
+#pragma unroll
+        for (int i = 0; i < NPASS; i++) {
+            const int rr = (ct >> 3) + RPP * i;        // record slot: A 0..63, B 64..191
+            const int r = i < APASS ? rr : rr - TA;
+            offP[i] = (uint32_t)(rr * 32 + wd * 4);
+            offG[i] = sw128_off(2 * r, wd);
+            offM[i] = sw128_off(2 * r + 1, wd);
+        }
+        int os = 0, ps = 0;
+        uint32_t oph = 0, pph = 0;
+        bool ok = true;
+        for (int64_t t = blockIdx.x; t < n_tiles && ok; t += gridDim.x) {
+            for (int kb = 0; kb < num_kb; kb++) {
+                // every lane waits (TMA data visible to each reader); the warp agrees on the outcome
+                const bool got = mbar_wait(&pfull[ps], pph, WAIT_LIMIT_NS) &&
+                                 mbar_wait(&empty[os], oph ^ 1, WAIT_LIMIT_NS);
+                if (!__all_sync(0xFFFFFFFFu, got)) {
+                    if (lane == 0) atomicOr(ep.err, 8u);
+                    ok = false;
+                    break;
+                }
+                const uint8_t* pk = sP + ps * P_BYTES;
+                uint8_t* oa = sA + os * A_BYTES;
+                uint8_t* ob = sB + os * B_BYTES;
+                uint32_t w[NPASS];
+#pragma unroll
+                for (int i = 0; i < NPASS; i++) w[i] = *reinterpret_cast<const uint32_t*>(pk + offP[i]);
+                const uint64_t i0 = (uint64_t)kb * 128 + (uint64_t)wd * 16;
+                if (i0 + 16 > n_indiv) {
+                    // individuals past N (and the zero fill past the row) read as missing
+                    const uint32_t valid = n_indiv > i0 ? (uint32_t)(n_indiv - i0) : 0u;
+                    const uint32_t keepm = (1u << (2 * valid)) - 1u;   // valid < 16 here
+#pragma unroll
+                    for (int i = 0; i < NPASS; i++) w[i] = (w[i] & keepm) | (0x55555555u & ~keepm);
+                }
+#pragma unroll
+                for (int i = 0; i < NPASS; i++) {
+                    uint4 g, mk;
+                    expand_chunk(w[i], g, mk);
+                    uint8_t* base = i < APASS ? oa : ob;
+                    *reinterpret_cast<uint4*>(base + offG[i]) = g;
+                    *reinterpret_cast<uint4*>(base + offM[i]) = mk;
+                }
+                // the generic-proxy stores must be visible to the tensor core's async proxy
+                fence_proxy_async_smem();
+                __syncwarp();
+                if (lane == 0) {
+                    mbar_arrive(&full[os]);
+                    mbar_arrive(&pempty[ps]);
+                }
+                if (++os == STAGES) {
+                    os = 0;
+                    oph ^= 1;
+                }
+                if (++ps == P_STAGES) {
+                    ps = 0;
+                    pph ^= 1;
+                }
             }
         }
     } else {
@@ -314,7 +452,11 @@ __global__ void __launch_bounds__(gram_threads(EW), 1)
                         cv += __shfl_xor_sync(0xFFFFFFFFu, cv, 16);
                         if (lane < 2) cpart[cslot * TB + c * 32 + p + lane] = cv;
                     } else {
-                        Rs[(row >> 1) * RLD + c * 32 + p + (grow ? 0 : 1)] = (float)r2u;
+                        // K > 1: the masked r2u value goes to the tile's f64 slot in
+                        // global memory (record k's row of TB values) for the banded
+                        // annotation contraction (contract.cu); lane pairs write
+                        // adjacent values
+                        ep.rtiles[(size_t)t * TA * TB + (size_t)(row >> 1) * TB + c * 32 + p + (grow ? 0 : 1)] = r2u;
                     }
                 }
             }
@@ -329,15 +471,7 @@ __global__ void __launch_bounds__(gram_threads(EW), 1)
                 }
                 named_bar_sync(1, EPI_T);
             } else {
-                // K > 1: the masked r2u tile goes to global memory for the
-                // banded annotation contraction (contract.cu)
-                named_bar_sync(1, EPI_T);
-                float4* dst = reinterpret_cast<float4*>(ep.rtiles + (size_t)t * TA * TB);
-                for (int q = et; q < TA * TB / 4; q += EPI_T) {
-                    const int e = q * 4, rr = e / TB, cc = e % TB;
-                    dst[q] = make_float4(Rs[rr * RLD + cc], Rs[rr * RLD + cc + 1], Rs[rr * RLD + cc + 2],
-                                         Rs[rr * RLD + cc + 3]);
-                }
+                // every thread has read this tile's wait decision before the next one is written
                 named_bar_sync(1, EPI_T);
             }
             if (++acc == 2) {
@@ -354,6 +488,8 @@ __global__ void __launch_bounds__(gram_threads(EW), 1)
 }
 
 }  // namespace
+
+static uint64_t round_up_128(uint64_t x) { return (x + 127) / 128 * 128; }
 
 using PFN_encodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
                                      const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
@@ -386,17 +522,20 @@ static bool make_map(CUtensorMap* map, const void* base, CUtensorMapDataType dt,
     return r == CUDA_SUCCESS;
 }
 
-template <int STAGES, int MODE, int EW>
+template <int STAGES, int MODE, int EW, int CW = 0>
 static cudaError_t run_tc(const CUtensorMap& tmA, const CUtensorMap& tmB, int num_kb, const Tile* tiles,
                           int64_t n_tiles, const EpilogueArgs& ep, int32_t* dbg, size_t smem, int64_t grid,
-                          cudaStream_t stream) {
-    cudaError_t e = cudaFuncSetAttribute(k_gram_tc<STAGES, MODE, EW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+                          cudaStream_t stream, uint64_t n_indiv = 0) {
+    cudaError_t e = cudaFuncSetAttribute(k_gram_tc<STAGES, MODE, EW, CW>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k_gram_tc<STAGES, MODE, EW><<<(unsigned)grid, gram_threads(EW), smem, stream>>>(tmA, tmB, num_kb, tiles,
-                                                                                   dbg ? 1 : n_tiles, ep, dbg);
+    k_gram_tc<STAGES, MODE, EW, CW><<<(unsigned)grid, gram_threads(EW, CW), smem, stream>>>(
+        tmA, tmB, num_kb, tiles, dbg ? 1 : n_tiles, ep, dbg, n_indiv);
     return cudaGetLastError();
 }
+
+// barriers (operand ring, packed ring, accumulators, drain) + TMEM slot words
+static constexpr size_t ctrl_bytes(int stages) { return 8 * (2 * stages + 2 * P_STAGES + 2 + 2 + 1 + 1); }
 
 template <int MODE>
 static cudaError_t launch_tc(const void* ops, CUtensorMapDataType dt, uint64_t elem_bytes, uint64_t ld_elems,
@@ -411,29 +550,20 @@ static cudaError_t launch_tc(const void* ops, CUtensorMapDataType dt, uint64_t e
         !make_map(&tmB, ops, dt, ld_elems, elem_bytes, rows, 2 * TB))
         return cudaErrorInvalidValue;
     const int num_kb = (int)(ld_elems * elem_bytes / 128);
-    const size_t ctrl = 8 * (2 * 4 + 2 + 2 + 1 + 1);  // barriers + tmem slot (upper bound)
+    const size_t ctrl = ctrl_bytes(4);  // upper bound over the stage counts used
     const size_t cbytes = sizeof(double) * 4 * TB;
     int64_t grid = n_tiles < sms ? n_tiles : sms;
     if (dbg) grid = 1;
     // more epilogue warps where the epilogue outweighs the MMAs: sixteen for
-    // the sketch forms with one annotation column (the f64 quadratic
-    // correction per pair), eight for INT8 rows under 32,768 individuals
+    // the sketch forms (the f64 quadratic correction per pair), eight for
+    // INT8 rows under 32,768 individuals
     const bool wide = MODE != 0 || ld_elems * elem_bytes < 32768;
-    if (ep.K == 1) {
-        const size_t smem = 1024 + 4 * (size_t)(A_BYTES + B_BYTES) + ctrl + cbytes;
-        if constexpr (MODE != 0) {
-            return run_tc<4, MODE, 16>(tmA, tmB, num_kb, tiles, n_tiles, ep, dbg, smem, grid, stream);
-        } else {
-            if (wide) return run_tc<4, MODE, 8>(tmA, tmB, num_kb, tiles, n_tiles, ep, dbg, smem, grid, stream);
-            return run_tc<4, MODE, 4>(tmA, tmB, num_kb, tiles, n_tiles, ep, dbg, smem, grid, stream);
-        }
-    }
-    const size_t smem = 1024 + 3 * (size_t)(A_BYTES + B_BYTES) + ctrl + cbytes + sizeof(float) * TA * RLD;
+    const size_t smem = 1024 + 4 * (size_t)(A_BYTES + B_BYTES) + ctrl + cbytes;
     if constexpr (MODE != 0) {
-        return run_tc<3, MODE, 8>(tmA, tmB, num_kb, tiles, n_tiles, ep, dbg, smem, grid, stream);
+        return run_tc<4, MODE, 16>(tmA, tmB, num_kb, tiles, n_tiles, ep, dbg, smem, grid, stream);
     } else {
-        if (wide) return run_tc<3, MODE, 8>(tmA, tmB, num_kb, tiles, n_tiles, ep, dbg, smem, grid, stream);
-        return run_tc<3, MODE, 4>(tmA, tmB, num_kb, tiles, n_tiles, ep, dbg, smem, grid, stream);
+        if (wide) return run_tc<4, MODE, 8>(tmA, tmB, num_kb, tiles, n_tiles, ep, dbg, smem, grid, stream);
+        return run_tc<4, MODE, 4>(tmA, tmB, num_kb, tiles, n_tiles, ep, dbg, smem, grid, stream);
     }
 }
 
@@ -442,11 +572,59 @@ cudaError_t launch_gram_i8(const uint8_t* ops, uint64_t ld, int64_t m, const Til
     return launch_tc<0>(ops, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, ld, m, tiles, n_tiles, ep, dbg, sms, stream);
 }
 
+// Map of the packed BED rows (record r at rows + r * pitch): boxes of 32 bytes
+// (128 individuals) x box_rows records, no swizzle (the converters read it
+// with plain shared loads).  Bytes past the pitch read as zero.
+static bool make_packed_map(CUtensorMap* map, const uint8_t* rows, uint64_t pitch, uint64_t m, uint32_t box_rows) {
+    PFN_encodeTiled enc = get_encode();
+    if (!enc) return false;
+    cuuint64_t dims[2] = {pitch, m};
+    cuuint64_t strides[1] = {pitch};
+    cuuint32_t box[2] = {32, box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<uint8_t*>(rows), dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+cudaError_t launch_gram_i8_packed(const uint8_t* rows, uint64_t pitch, uint64_t n_indiv, int64_t m, const Tile* tiles,
+                                  int64_t n_tiles, const EpilogueArgs& ep, int32_t* dbg, int sms,
+                                  cudaStream_t stream) {
+    if (n_tiles <= 0) return cudaSuccess;
+    if (pitch % 16 != 0 || pitch < (n_indiv + 3) / 4 || n_indiv == 0 ||
+        (reinterpret_cast<uintptr_t>(rows) & 15) != 0)
+        return cudaErrorInvalidValue;
+    CUtensorMap tmA, tmB;
+    if (!make_packed_map(&tmA, rows, pitch, (uint64_t)m, TA) || !make_packed_map(&tmB, rows, pitch, (uint64_t)m, TB))
+        return cudaErrorInvalidValue;
+    const int num_kb = (int)((n_indiv + 127) / 128);
+    const size_t cbytes = sizeof(double) * 4 * TB;
+    const size_t pbytes = (size_t)P_STAGES * P_BYTES;
+    int64_t grid = n_tiles < sms ? n_tiles : sms;
+    if (dbg) grid = 1;
+    const bool wide = round_up_128(n_indiv) < 32768;
+    const size_t smem = 1024 + 4 * (size_t)(A_BYTES + B_BYTES) + pbytes + ctrl_bytes(4) + cbytes;
+    if (wide)
+        return run_tc<4, 0, 8, CONV_WARPS>(tmA, tmB, num_kb, tiles, n_tiles, ep, dbg, smem, grid, stream, n_indiv);
+    return run_tc<4, 0, 4, CONV_WARPS>(tmA, tmB, num_kb, tiles, n_tiles, ep, dbg, smem, grid, stream, n_indiv);
+}
+
 cudaError_t launch_gram_tf32(const float* ops, uint64_t ld, int64_t m, const Tile* tiles, int64_t n_tiles,
                              const EpilogueArgs& ep, int maf_aware, int32_t* dbg, int sms, cudaStream_t stream) {
     if (maf_aware)
         return launch_tc<2>(ops, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, ld, m, tiles, n_tiles, ep, dbg, sms, stream);
     return launch_tc<1>(ops, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, ld, m, tiles, n_tiles, ep, dbg, sms, stream);
+}
+
+cudaError_t preload_gram_tc() {
+    cudaError_t e = preload_kernel(k_gram_tc<4, 0, 4, 0>);
+    if (e == cudaSuccess) e = preload_kernel(k_gram_tc<4, 0, 8, 0>);
+    if (e == cudaSuccess) e = preload_kernel(k_gram_tc<4, 1, 16, 0>);
+    if (e == cudaSuccess) e = preload_kernel(k_gram_tc<4, 2, 16, 0>);
+    if (e == cudaSuccess) e = preload_kernel(k_gram_tc<4, 0, 4, CONV_WARPS>);
+    if (e == cudaSuccess) e = preload_kernel(k_gram_tc<4, 0, 8, CONV_WARPS>);
+    return e;
 }
 
 }  // namespace ldsc

@@ -139,7 +139,7 @@ extern "C" int ldsc_l2_int8_noalloc(const uint8_t* d_rows, uint64_t pitch, uint6
     uint8_t* ops = base + o_ops;
     if ((rc = ck(launch_decode_i8(pv, nullptr, (int64_t)m, sel, ops, ld, st, 0, s), "decode"))) return rc;
     if ((rc = ck(launch_finalize_stats((int64_t)m, n_indiv, st, nullptr, 1, 0, 0.0,
-                                       reinterpret_cast<double*>(base + o_aeff), nullptr, d_l2, s),
+                                       reinterpret_cast<double*>(base + o_aeff), d_l2, s),
                  "finalize")))
         return rc;
     EpilogueArgs ep{};

@@ -17,6 +17,7 @@
 
 #include <cmath>
 
+#include "engine.h"
 #include "regress.h"
 
 namespace ldsc {
@@ -458,6 +459,17 @@ cudaError_t launch_partitioned(const PartJob* jobs, PartState* st, const double*
     k_p_solve<<<dim3(nb + 1, njobs), NT, solve_smem, s>>>(gram, tot, nb, q, sol);
     k_p_finish<<<njobs, NT, (size_t)p * sizeof(double), s>>>(jobs, st, sol, m_vec, nb, k, p, res);
     return cudaGetLastError();
+}
+
+cudaError_t preload_partitioned() {
+    cudaError_t e = preload_kernel(k_p_xtot);
+    if (e == cudaSuccess) e = preload_kernel(k_p_sums);
+    if (e == cudaSuccess) e = preload_kernel(k_p_aggregate);
+    if (e == cudaSuccess) e = preload_kernel(k_p_gram);
+    if (e == cudaSuccess) e = preload_kernel(k_p_total);
+    if (e == cudaSuccess) e = preload_kernel(k_p_solve);
+    if (e == cudaSuccess) e = preload_kernel(k_p_finish);
+    return e;
 }
 
 }  // namespace ldsc

@@ -16,6 +16,7 @@
 
 #include <cmath>
 
+#include "engine.h"
 #include "regress.h"
 
 namespace ldsc {
@@ -539,6 +540,20 @@ cudaError_t launch_select(const RegJob* jobs, uint64_t n, uint64_t rank, double*
     if (njobs <= 0 || n == 0) return cudaSuccess;
     k_select<<<njobs, NT, 0, s>>>(jobs, n, rank, out);
     return cudaGetLastError();
+}
+
+cudaError_t preload_regress() {
+    cudaError_t e = preload_kernel(k_reg_sums<0>);
+    if (e == cudaSuccess) e = preload_kernel(k_reg_sums<1>);
+    if (e == cudaSuccess) e = preload_kernel(k_reg_update<0>);
+    if (e == cudaSuccess) e = preload_kernel(k_reg_update<1>);
+    if (e == cudaSuccess) e = preload_kernel(k_reg_jackknife);
+    if (e == cudaSuccess) e = preload_kernel(k_rg_finish);
+    if (e == cudaSuccess) e = preload_kernel(k_select);
+    if (e == cudaSuccess) e = preload_kernel(k_ts_count);
+    if (e == cudaSuccess) e = preload_kernel(k_ts_seps);
+    if (e == cudaSuccess) e = preload_kernel(k_ts_combine);
+    return e;
 }
 
 }  // namespace ldsc

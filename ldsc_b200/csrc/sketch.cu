@@ -590,4 +590,13 @@ cudaError_t launch_sketch_segt(const int32_t* seg_off, uint64_t n_used, uint32_t
     return cudaGetLastError();
 }
 
+cudaError_t preload_sketch() {
+    cudaError_t e = preload_kernel(k_sketch_permute);
+    if (e == cudaSuccess) e = preload_kernel(k_sketch_seg);
+    if (e == cudaSuccess) e = preload_kernel(k_sketch_seg6);
+    if (e == cudaSuccess) e = preload_kernel(k_sketch_segt<SNT, true>);
+    if (e == cudaSuccess) e = preload_kernel(k_sketch_segt<S6T, false>);
+    return e;
+}
+
 }  // namespace ldsc

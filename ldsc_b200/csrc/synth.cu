@@ -110,4 +110,10 @@ cudaError_t launch_synth(uint8_t* rows, uint64_t pitch, uint64_t n_indiv, uint64
     return cudaGetLastError();
 }
 
+cudaError_t preload_synth() {
+    cudaError_t e = preload_kernel(k_founders);
+    if (e == cudaSuccess) e = preload_kernel(k_synth);
+    return e;
+}
+
 }  // namespace ldsc

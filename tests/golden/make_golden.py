@@ -54,7 +54,12 @@ MODES = {
     "cm1_perallele": ("cm", 1.0, 50, True, True, False, 0, False, 1.0),
     "cm1_f32": ("cm", 1.0, 50, False, True, True, 0, False, None),
     "cm1_sketch50": ("cm", 1.0, 50, True, True, True, 50, False, None),
+    "cm1_sketch200": ("cm", 1.0, 50, True, True, True, 200, False, None),
+    "cm1_sketch50_maf": ("cm", 1.0, 50, True, True, True, 50, False, None),
+    "cm1_sketch200_maf": ("cm", 1.0, 50, True, True, True, 200, False, None),
 }
+# sketch modes run with --sketch-maf-aware (the kurtosis-shifted correction)
+MAF_AWARE = {"cm1_sketch50_maf", "cm1_sketch200_maf"}
 
 
 def annot3(m, seed=5):
@@ -68,7 +73,8 @@ def oracle_args(name, body, n, chr_, cm, bp):
     return OracleL2Args(bed_body=body, n_file_indiv=n, chr=chr_, cm=cm, bp=bp, mode=mode,
                         wind=wind if mode != "snp" else 0.0, wind_snp=int(wind) if mode == "snp" else 0,
                         chunk_c=chunk, masking=masking, per_chr=per_chr, use_f32=f32, sketch_d=sk,
-                        annot=annot3(len(chr_)) if has_annot else None, pq_exp=pq)
+                        annot=annot3(len(chr_)) if has_annot else None, pq_exp=pq,
+                        sketch_maf_aware=name in MAF_AWARE)
 
 
 def main():

@@ -2,10 +2,9 @@
 panel, and the CLI's sliced path against its resident path.
 
 Tolerance: each slice sums the same pair contributions into l2 in its own
-tile order.  With one annotation column the sums are f64 and agree to 1e-12
-of the column's largest value; with K > 1 the r2u tiles are contracted in f32
-(tile grids start at each call's first record), so 2e-6.  The written files
-are identical.
+tile order (tile grids start at each call's first record).  The sums are f64
+for one annotation column and for K > 1 alike, and agree to 1e-12 of the
+column's largest value.  The written files are identical.
 """
 import gzip
 import os
@@ -56,7 +55,7 @@ def test_sliced_equals_resident(ctx, precision, masking, global_pass, sketch, k)
     got, maf_g, slices, perfs = run_l2_sliced(ctx, snps, body, spec.n_indiv, mode, 200, max_call_records=1800, **kw)
     assert len(slices) >= 4 and all(s.call_hi - s.call_lo <= 1800 for s in slices)
     scale = np.abs(want).max(axis=0, keepdims=True)
-    np.testing.assert_allclose(got / scale, want / scale, rtol=0, atol=1e-12 if k == 1 else 2e-6)
+    np.testing.assert_allclose(got / scale, want / scale, rtol=0, atol=1e-12)
     np.testing.assert_array_equal(maf_g, maf_w)
 
 
