@@ -9,9 +9,11 @@ INT8-vs-FP64 ratio.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-With --gpus N (launched by torchrun) each rank computes its own chromosome
-(an independent 100,000-SNP panel, seed + rank): weak scaling, no collective
-on the data path; the time is the max over ranks.  The reference arm
+With --gpus N (launched by torchrun) the ranks split the one panel into
+record cores balanced by pair count; each rank computes its core plus the
+halo records its windows need on its own GPU, and one all-gather of the core
+rows assembles the l2 (strong scaling; the time is the max over ranks).
+With --weak each rank computes its own panel (seed + rank) instead.  The reference arm
 (--impl reference) times the C restatement of the reference's CPU l2 path
 (the reference is Rust and cannot be compiled in this image) on all host
 cores, on a bounded SNP sample of the same workload.
@@ -124,18 +126,78 @@ def committed_traffic(kernel: str):
     return None
 
 
-def cpu_baseline(body_rows, spec, chr_, cm, bp, n_threads=0):
+def cpu_baseline(body_rows, spec, chr_, cm, bp, n_threads=0, masking=True, want_l2=False):
     """The C restatement of the reference's l2 (OpenMP, all host threads) on
     the first CPU_SAMPLE_SNPS SNPs of the panel, same flags."""
     sys.path.insert(0, ROOT)
     from oracle import OracleL2Args, max_threads, oracle_l2
     m = body_rows.shape[0]
     a = OracleL2Args(bed_body=body_rows, n_file_indiv=spec.n_indiv, chr=chr_[:m], cm=cm[:m], bp=bp[:m],
-                     mode="cm", wind=1.0, chunk_c=200, masking=True, per_chr=True, n_threads=n_threads)
+                     mode="cm", wind=1.0, chunk_c=200, masking=masking, per_chr=True, n_threads=n_threads)
+    work = {}
     t0 = time.perf_counter()
-    _, _, pairs, _ = oracle_l2(a)
+    l2, _, pairs, _ = oracle_l2(a, work)
     dt = time.perf_counter() - t0
-    return pairs / dt, pairs, dt, (n_threads or max_threads())
+    cores = n_threads or max_threads()
+    # the restatement's chunk Grams: dot products actually computed (w x c + c x c
+    # per chunk, 2 N flops each) over their wall time, per host thread
+    work["gemm_gflops_per_core"] = 2.0 * spec.n_indiv * work["n_dots"] / work["gemm_secs"] / 1e9 / cores
+    work["gemm_share_of_time"] = work["gemm_secs"] / dt
+    work["useful_gflops_per_core"] = 2.0 * spec.n_indiv * pairs / dt / 1e9 / cores
+    if want_l2:
+        return pairs / dt, pairs, dt, cores, l2[:, 0], work
+    return pairs / dt, pairs, dt, cores, work
+
+
+def cpu_gemm_fields(work):
+    return {"gemm_gflops_per_core": work["gemm_gflops_per_core"],
+            "gemm_share_of_time": work["gemm_share_of_time"],
+            "useful_gflops_per_core": work["useful_gflops_per_core"],
+            "gemm_note": "cache-blocked 3 x 4 AVX2 dot-product kernel of the C restatement (no packing); "
+                         "gemm = dot products the chunk Grams computed, useful = 2 N per counted pair"}
+
+
+def max_rel_per_l2j(got, ref):
+    """max_j |got_j - ref_j| / |ref_j| (every l2_j of these panels is well away from 0)."""
+    return float(np.max(np.abs(got - ref) / np.abs(ref)))
+
+
+def oracle_parity(ctx, panel, spec, snps, chr_, cm, bp, l2_full_masked, masked_sample_l2):
+    """Per-l2_j parity of the GPU forms against the oracle at the benchmark's
+    own N, on the SNP sample the CPU baseline times (records
+    [0, CPU_SAMPLE_SNPS) of the panel, both window modes):
+      * sample: the INT8 and FP64 forms run on exactly the oracle's inputs;
+      * full panel: l2 of the full-size INT8 run for every SNP whose pairs all
+        lie inside the sample (j < left[CPU_SAMPLE_SNPS] of the full run, as
+        left is non-decreasing), against the same oracle values."""
+    from ldsc_b200.api import WindowMode, left_limits, run_l2
+    from ldsc_b200.plink import BimTable
+    m = CPU_SAMPLE_SNPS
+    wm = WindowMode.Cm(1.0)
+    sample = BimTable(chr_[:m], [f"rs{i}" for i in range(m)], cm[:m], bp[:m], np.arange(m, dtype=np.int64))
+    rows = panel.download(0, m)
+    out = {"sample": f"records [0, {m}) of the panel, N={spec.n_indiv}, 1 cM, chunk 200",
+           "metric": "max_j |l2_j - oracle_j| / |oracle_j|"}
+    per_mode = {}
+    for name, masking in (("masked", True), ("chunk200", False)):
+        if masking:
+            ref = masked_sample_l2
+        else:
+            ref = cpu_baseline(rows, spec, chr_, cm, bp, masking=False, want_l2=True)[4]
+        got8 = run_l2(ctx, sample, panel, wm, 200, snp_level_masking=masking, precision="int8", yes_really=True)[0]
+        got64 = run_l2(ctx, sample, panel, wm, 200, snp_level_masking=masking, precision="fp64", yes_really=True)[0]
+        full = l2_full_masked if masking else run_l2(ctx, snps, panel, wm, 200, snp_level_masking=False,
+                                                     precision="int8", yes_really=True)[0][:, 0]
+        inside = int(left_limits(snps, wm, 200, snp_level_masking=masking)[m])
+        per_mode[name] = {"int8": max_rel_per_l2j(got8[:, 0], ref), "fp64": max_rel_per_l2j(got64[:, 0], ref),
+                          "full_panel_int8": max_rel_per_l2j(full[:inside], ref[:inside]),
+                          "full_panel_snps_compared": inside, "min_abs_oracle_l2": float(np.min(np.abs(ref)))}
+    out["int8_vs_oracle_max_rel_per_l2j"] = {k: v["int8"] for k, v in per_mode.items()}
+    out["fp64_vs_oracle_max_rel_per_l2j"] = {k: v["fp64"] for k, v in per_mode.items()}
+    out["full_panel_int8_vs_oracle_max_rel_per_l2j"] = {k: v["full_panel_int8"] for k, v in per_mode.items()}
+    out["detail"] = per_mode
+    out["bar"] = 1e-6
+    return out
 
 
 def run_reference(args):
@@ -147,9 +209,9 @@ def run_reference(args):
     for _ in range(args.warmup):
         cpu_baseline(rows[:200], spec, chr_, cm, bp)
     vals, tot_pairs, tot_t = [], 0, 0.0
-    cores = None
+    cores, work = None, None
     for _ in range(args.steps):
-        v, pairs, dt, cores = cpu_baseline(rows, spec, chr_, cm, bp)
+        v, pairs, dt, cores, work = cpu_baseline(rows, spec, chr_, cm, bp)
         vals.append(v)
         tot_pairs += pairs
         tot_t += dt
@@ -161,7 +223,7 @@ def run_reference(args):
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
            "data": "synthetic (seeded founder-mosaic panel)", "config": config_dict(spec),
            "cpu_baseline": {"value": value, "unit": "r2 pairs/s", "cores": cores, "kind": "port",
-                            "sample": sample},
+                            "sample": sample, **cpu_gemm_fields(work)},
            "e2e": {"value": value, "unit": "r2 pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
            "note": "reference is Rust (no cargo/rustc in this image); timed arm is the C restatement "
                    "oracle/ldsc_oracle.c of its CPU l2 path"}
@@ -208,6 +270,10 @@ def run_sketch_workload(args, ctx, stream):
     hbm, bf16, src = measured_peaks()
     tf32_peak = bf16 / 2.0
     for d in [int(x) for x in args.sketch_d.split(",")]:
+        # the first call with this d builds the CountSketch layout (hash, bucket-major
+        # order, panel rewritten in it): its one-time cost, then the timed passes
+        layout_s = run_l2(ctx, snps, panel, wm, 200, snp_level_masking=True, sketch=d,
+                          yes_really=True)[2].layout_secs
         t, outs = _timed_passes(ctx, stream, lambda: run_l2(ctx, snps, panel, wm, 200, snp_level_masking=True,
                                                             sketch=d, yes_really=True), args.warmup, args.steps)
         sk = outs[-1][0][:, 0]
@@ -222,6 +288,7 @@ def run_sketch_workload(args, ctx, stream):
                "metric": "r2 pairs/sec (sketch form)", "value": npairs * args.steps / t, "unit": "r2 pairs/s",
                "ms_per_step": 1e3 * t / args.steps, "n_pairs": npairs,
                "exact_int8_pairs_per_s": npairs / t_ex,
+               "layout_build_ms": 1e3 * layout_s,
                "sketch_kernel_ms": 1e3 * sk_s, "sketch_gram_ms": 1e3 * gram_s, "decode_ms": 1e3 * perf.norm_secs,
                "device_ms_per_call": float(np.mean([o[2].device_ms for o in outs])),
                "sketch_roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
@@ -573,6 +640,8 @@ def main():
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--weak", action="store_true",
+                    help="N > 1: every rank runs its own panel (seed + rank) instead of a shard of one panel")
     ap.add_argument("--workload", default="biobank",
                     choices=["biobank", "profile", "sketch", "partitioned", "partitioned-h2", "serving"])
     ap.add_argument("--h2p-snps", type=int, default=500_000, help="partitioned-h2: regression SNPs")
@@ -631,16 +700,35 @@ def main():
         print(json.dumps(run_serving_workload(args, ctx, args.serve_seconds, args.serve_rate)), flush=True)
         return
 
-    spec = workload_spec(seed_offset=rank, workload=args.workload)
+    # N > 1: the ranks split one panel into cores balanced by pair count, each
+    # computing its core plus halos, then one all-gather of the core rows
+    # (strong scaling); with --weak every rank runs its own panel (seed + rank)
+    sharded = world > 1 and not args.weak
+    spec = workload_spec(seed_offset=0 if sharded else rank, workload=args.workload)
     chr_, cm, bp = synth.positions(spec)
     m = spec.m
     snps = BimTable(chr_, [f"rs{i}" for i in range(m)], cm, bp, np.arange(m, dtype=np.int64))
     panel = ctx.synth(spec.n_indiv, m, spec.founders, spec.switch_p, spec.miss, spec.seed)
     wm = WindowMode.Cm(1.0)
     npairs = pair_count(snps, wm, 200, snp_level_masking=True)
+    if sharded:
+        from ldsc_b200.parallel import gather_l2, plan_shards, shard_records
+        plan = plan_shards(snps, wm, world, 200, snp_level_masking=True)
+        sh = plan[rank]
+        rec = shard_records(snps, sh)
+        n_call = sh.call_hi - sh.call_lo
+        d_l2 = torch.empty((1, n_call), dtype=torch.float64, device="cuda")
+        d_maf = torch.empty(n_call, dtype=torch.float64, device="cuda")
+        core = slice(sh.core_lo - sh.call_lo, sh.core_hi - sh.call_lo)
 
     def step(precision):
-        return run_l2(ctx, snps, panel, wm, 200, snp_level_masking=True, precision=precision, yes_really=True)
+        if not sharded:
+            return run_l2(ctx, snps, panel, wm, 200, snp_level_masking=True, precision=precision, yes_really=True)
+        # this rank's call on the resident panel, l2 left on the device, then
+        # the gather of every rank's core rows (the full l2 on rank 0's host)
+        _, _, perf = run_l2(ctx, rec, panel, wm, 200, snp_level_masking=True, precision=precision,
+                            yes_really=True, out_device=(d_l2, d_maf))
+        return gather_l2(d_l2[0, core].reshape(-1, 1), plan, rank, dst=0), None, perf
 
     # ---- INT8 form, inputs resident in HBM ----
     for _ in range(args.warmup):
@@ -654,7 +742,7 @@ def main():
     ev0.record(stream)
     gram_s, dec_s, dev_ms = [], [], []
     for _ in range(args.steps):
-        _, _, perf = step("int8")
+        l2_last, _, perf = step("int8")
         gram_s.append(perf.ab_dot_secs)
         dec_s.append(perf.norm_secs)
         dev_ms.append(perf.device_ms)
@@ -665,12 +753,14 @@ def main():
     launches = ctx.kernel_count - k0
     t_local = ev0.elapsed_time(ev1) / 1e3
     t_max, pairs_all = t_local, npairs
+    rank_pairs = perf.n_pairs   # pairs this rank's call computed (core plus halos when sharded)
     if world > 1:
         tt = torch.tensor([t_local], device="cuda", dtype=torch.float64)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         pp = torch.tensor([npairs], device="cuda", dtype=torch.float64)
         dist.all_reduce(pp, op=dist.ReduceOp.SUM)
-        t_max, pairs_all = float(tt.item()), float(pp.item())
+        # sharded: the panel's own pairs once; weak: every rank's panel
+        t_max, pairs_all = float(tt.item()), (npairs if sharded else float(pp.item()))
     value = pairs_all * args.steps / t_max
     gram_avg = float(np.mean(gram_s))
 
@@ -680,7 +770,8 @@ def main():
         l2_64 = step("fp64")[0]
         l2_i8 = step("int8")[0]
         # l2 of the INT8 form against the FP64 form on the same panel: max |a - b| / max(|b|, 1)
-        int8_err = float(np.max(np.abs(l2_i8 - l2_64) / np.maximum(np.abs(l2_64), 1.0)))
+        if l2_64 is not None:
+            int8_err = float(np.max(np.abs(l2_i8 - l2_64) / np.maximum(np.abs(l2_64), 1.0)))
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -691,26 +782,42 @@ def main():
         e1.record(stream)
         torch.cuda.synchronize()
         t64 = e0.elapsed_time(e1) / 1e3
-        fp64_value = npairs * args.fp64_steps / t64
+        if world > 1:
+            tt = torch.tensor([t64], device="cuda", dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t64 = float(tt.item())
+        fp64_value = pairs_all * args.fp64_steps / t64 / (1 if sharded else world)
 
     # ---- end to end through the whole-file C ABI entry point, host buffers ----
     e2e = None
     if not args.no_e2e:
-        rows = panel.download()
+        # the BED image this rank reads: the whole panel, or its call's rows when sharded
+        r0, r1 = (sh.call_lo, sh.call_hi) if sharded else (0, m)
+        e2e_snps = snps
+        if sharded:
+            e2e_snps = rec.subset(np.arange(n_call))
+            e2e_snps.bed_idx = np.arange(n_call, dtype=np.int64)
+        rows = panel.download(r0, r1)
         bed = torch.empty(3 + rows.size, dtype=torch.uint8, pin_memory=True)
         bnp = bed.numpy()
         bnp[:3] = [0x6C, 0x1B, 0x01]
         bnp[3:] = rows.reshape(-1)
         del rows
-        for _ in range(1):
-            l2_from_bed_bytes(ctx, bnp, spec.n_indiv, snps, wm, 200, precision="int8", snp_level_masking=True)
+
+        def e2e_step():
+            l2h, _, p = l2_from_bed_bytes(ctx, bnp, spec.n_indiv, e2e_snps, wm, 200, precision="int8",
+                                          snp_level_masking=True)
+            if sharded:
+                gather_l2(l2h[core], plan, rank, dst=0)
+            return p
+
+        e2e_step()
         barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         e2e_perf = []
         for _ in range(args.steps):
-            e2e_perf.append(l2_from_bed_bytes(ctx, bnp, spec.n_indiv, snps, wm, 200, precision="int8",
-                                              snp_level_masking=True)[2])
+            e2e_perf.append(e2e_step())
         torch.cuda.synchronize()
         te = time.perf_counter() - t0
         if world > 1:
@@ -727,7 +834,7 @@ def main():
     # ---- roofline of the dominant kernel (INT8 band Gram) ----
     hbm, bf16, src = measured_peaks()
     int8_peak = 2.0 * bf16   # dense int8 tensor rate is 2x bf16 on sm_100
-    ops = 8.0 * spec.n_indiv * npairs   # 4 integer products x 2 ops x N per in-band pair
+    ops = 8.0 * spec.n_indiv * rank_pairs   # 4 integer products x 2 ops x N per in-band pair
     achieved = ops / gram_avg / 1e12
     roofline = {"bound": "tensor", "achieved": achieved, "peak": int8_peak, "unit": "TFLOP/s",
                 "frac": achieved / int8_peak, "traffic": committed_traffic("k_gram_tc"),
@@ -737,12 +844,15 @@ def main():
                            "fallback bf16 dense burst 1590 TFLOP/s (MEASURED_PEAKS.json absent)")
                         + ", nominal int8 dense 4500"}
 
-    cpu = None
+    cpu, parity = None, None
     if rank == 0 and world == 1 and not args.no_cpu:
         rows = panel.download(0, CPU_SAMPLE_SNPS)
-        v, pairs_s, dt, cores = cpu_baseline(rows, spec, chr_, cm, bp)
+        v, pairs_s, dt, cores, ref_masked, work = cpu_baseline(rows, spec, chr_, cm, bp, want_l2=True)
         cpu = {"value": v, "unit": "r2 pairs/s", "cores": cores, "kind": "port",
-               "sample": f"first {CPU_SAMPLE_SNPS} SNPs of the panel ({pairs_s} pairs, {dt:.1f} s), same flags, f64"}
+               "sample": f"first {CPU_SAMPLE_SNPS} SNPs of the panel ({pairs_s} pairs, {dt:.1f} s), same flags, f64",
+               **cpu_gemm_fields(work)}
+        if args.workload == "biobank":
+            parity = oracle_parity(ctx, panel, spec, snps, chr_, cm, bp, l2_last[:, 0], ref_masked)
 
     # ---- serving latency at a stated rate (the metric's second half), 1 GPU ----
     serving = None
@@ -759,16 +869,19 @@ def main():
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": "r2 pairs/s", "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
-               "scaling": "weak", "vs_baseline": None, "dtype": "int8 (int32 accumulate, f64 epilogue)",
+               "scaling": "strong" if sharded else "weak", "vs_baseline": None,
+               "dtype": "int8 (int32 accumulate, f64 epilogue)",
                "data": "synthetic (seeded founder-mosaic panel generated on the device)",
                "config": config_dict(spec), "e2e": e2e, "gpu_launches": int(launches),
                "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks, "serving": serving,
+               "int8_vs_oracle_max_rel_per_l2j": parity["int8_vs_oracle_max_rel_per_l2j"] if parity else None,
+               "parity": parity,
                "forms": {"int8_pairs_per_s": value / world, "fp64_pairs_per_s": fp64_value,
                          "int8_over_fp64": (value / world) / fp64_value if fp64_value else None,
                          "int8_gram_ms": 1e3 * gram_avg, "fp64_gram_ms": 1e3 * float(np.mean(fp64_gram)),
                          "int8_decode_ms": 1e3 * float(np.mean(dec_s)),
                          "int8_device_ms_per_pass": float(np.mean(dev_ms)),
-                         "n_pairs_per_rank": npairs,
+                         "n_pairs_per_rank": int(rank_pairs),
                          "int8_vs_fp64_l2_max_rel_err": int8_err}}
         print(json.dumps(out))
     panel.close()
