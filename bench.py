@@ -453,15 +453,16 @@ def _partitioned_h2(ctx, stream, d_l2, annot, args, n_traits=8, n_blocks=200):
                     "annotations); the Gram rate is a lower bound (call time includes the solves)"}
 
 
-def run_serving_workload(args, ctx, duration_s: float, rate: float, seed: int = 7):
+def run_serving_workload(args, ctx, duration_s: float, rates, seed: int = 7):
     """Serving mix on a resident N=20,000 x M=1,200,000 panel (22
-    chromosomes, 3,500 cM).  Poisson arrivals at `rate` requests/s for
+    chromosomes, 3,500 cM).  Poisson arrivals at each rate (requests/s) for
     `duration_s` seconds: 70% LD-score requests (region M log-uniform in
     [2,000, 200,000], K in {1, 10, 97} from resident annotations, exact INT8
     or sketch d=1000, 1 cM, per-SNP masking), 20% h2 over 1,000 traits and 10%
     rg over 200 trait pairs, both against the resident LD scores of every 6th
     SNP (200,000 regression SNPs, 200-block jackknife).  Returns the latency
-    and throughput summary."""
+    and throughput summary, one per rate of `rates` (the same server and
+    resident data serve the rates one after another)."""
     import threading
     import queue as pyqueue
     import torch
@@ -515,21 +516,23 @@ def run_serving_workload(args, ctx, duration_s: float, rate: float, seed: int = 
     del annot
     torch.cuda.synchronize()
 
-    rng = np.random.default_rng(seed)
-    n_req = max(1, int(rate * duration_s))
-    arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
-    reqs = []
-    for _ in range(n_req):
-        u = rng.random()
-        if u < 0.7:
-            mreg = int(np.exp(rng.uniform(np.log(2000), np.log(200000))))
-            b = int(rng.integers(0, M - mreg))
-            reqs.append(("l2", dict(b=b, e=b + mreg, K=int(rng.choice([1, 10, 97])),
-                                    sketch=None if rng.random() < 0.5 else 1000)))
-        elif u < 0.9:
-            reqs.append(("h2", {}))
-        else:
-            reqs.append(("rg", dict(p0=int(rng.integers(0, Pn - 200)))))
+    def make_requests(rate):
+        rng = np.random.default_rng(seed)
+        n_req = max(1, int(rate * duration_s))
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
+        reqs = []
+        for _ in range(n_req):
+            u = rng.random()
+            if u < 0.7:
+                mreg = int(np.exp(rng.uniform(np.log(2000), np.log(200000))))
+                b = int(rng.integers(0, M - mreg))
+                reqs.append(("l2", dict(b=b, e=b + mreg, K=int(rng.choice([1, 10, 97])),
+                                        sketch=None if rng.random() < 0.5 else 1000)))
+            elif u < 0.9:
+                reqs.append(("h2", {}))
+            else:
+                reqs.append(("rg", dict(p0=int(rng.integers(0, Pn - 200)))))
+        return reqs, arrivals
 
     def region(b, e):
         return BimTable(chr_[b:e], names[b:e], cm[b:e], bp[b:e], np.arange(b, e, dtype=np.int64))
@@ -557,78 +560,85 @@ def run_serving_workload(args, ctx, duration_s: float, rate: float, seed: int = 
             srv.wait(t)
     setup_s = time.perf_counter() - t_setup
 
-    done = []
-    q = pyqueue.Queue()
+    def one_rate(rate):
+        reqs, arrivals = make_requests(rate)
+        n_req = len(reqs)
+        done = []
+        q = pyqueue.Queue()
 
-    def waiter():
-        while True:
-            item = q.get()
-            if item is None:
-                return
-            kind, p, t = item
-            try:
-                res, timing = srv.wait(t)
-                pairs = res[2].n_pairs if kind == "l2" else 0
-                done.append((kind, p, timing, pairs, None))
-            except Exception as e:  # noqa: BLE001
-                done.append((kind, p, None, 0, str(e)))
+        def waiter():
+            while True:
+                item = q.get()
+                if item is None:
+                    return
+                kind, p, t = item
+                try:
+                    res, timing = srv.wait(t)
+                    pairs = res[2].n_pairs if kind == "l2" else 0
+                    done.append((kind, p, timing, pairs, None))
+                except Exception as e:  # noqa: BLE001
+                    done.append((kind, p, None, 0, str(e)))
 
-    waiters = [threading.Thread(target=waiter) for _ in range(n_slots + 2)]
-    for w in waiters:
-        w.start()
-    st0 = srv.stats()
-    t0 = time.perf_counter()
-    late = []
-    for (kind, p), ta in zip(reqs, arrivals):
-        now = time.perf_counter() - t0
-        if ta > now:
-            time.sleep(ta - now)
-        else:
-            late.append(now - ta)
-        q.put((kind, p, submit(srv, kind, p)))
-    for _ in waiters:
-        q.put(None)
-    for w in waiters:
-        w.join()
-    wall = time.perf_counter() - t0
-    st1 = srv.stats()
-    srv.close()
-    panel.close()
+        waiters = [threading.Thread(target=waiter) for _ in range(n_slots + 2)]
+        for w in waiters:
+            w.start()
+        st0 = srv.stats()
+        t0 = time.perf_counter()
+        late = []
+        for (kind, p), ta in zip(reqs, arrivals):
+            now = time.perf_counter() - t0
+            if ta > now:
+                time.sleep(ta - now)
+            else:
+                late.append(now - ta)
+            q.put((kind, p, submit(srv, kind, p)))
+        for _ in waiters:
+            q.put(None)
+        for w in waiters:
+            w.join()
+        wall = time.perf_counter() - t0
+        st1 = srv.stats()
 
-    ok = [d for d in done if d[4] is None]
-    lat = np.array([d[2].latency_ms for d in ok])
-    que = np.array([d[2].queue_ms for d in ok])
-    run = np.array([d[2].run_ms for d in ok])
+        ok = [d for d in done if d[4] is None]
+        lat = np.array([d[2].latency_ms for d in ok])
+        que = np.array([d[2].queue_ms for d in ok])
+        run = np.array([d[2].run_ms for d in ok])
 
-    def pct(a):
-        return {"p50": float(np.percentile(a, 50)), "p99": float(np.percentile(a, 99)), "mean": float(np.mean(a)),
-                "max": float(np.max(a)), "n": int(len(a))} if len(a) else None
+        def pct(a):
+            return {"p50": float(np.percentile(a, 50)), "p99": float(np.percentile(a, 99)),
+                    "mean": float(np.mean(a)), "max": float(np.max(a)), "n": int(len(a))} if len(a) else None
 
-    def label(kind, p):
-        if kind != "l2":
-            return kind
-        return f"l2_{'sketch1000' if p['sketch'] else 'int8'}_K{p['K']}"
+        def label(kind, p):
+            if kind != "l2":
+                return kind
+            return f"l2_{'sketch1000' if p['sketch'] else 'int8'}_K{p['K']}"
 
-    by = {}
-    for d in ok:
-        by.setdefault(label(d[0], d[1]), []).append(d[2].latency_ms)
-    pairs = float(sum(d[3] for d in ok))
-    return {"workload": "serving", "metric": "request latency (ms) and throughput at a stated Poisson rate",
-            "rate_req_s": rate, "duration_s": duration_s, "requests": n_req, "completed": len(ok),
-            "failed": len(done) - len(ok), "errors": sorted({d[4] for d in done if d[4]})[:3],
-            "wall_s": wall, "throughput_req_s": len(ok) / wall, "l2_pairs_per_s": pairs / wall,
-            "latency_ms": pct(lat), "queue_ms": pct(que), "run_ms": pct(run),
-            "by_kind_latency_ms": {k: pct(np.array(v)) for k, v in sorted(by.items())},
-            "arrival_lag_ms_p99": float(np.percentile(late, 99) * 1e3) if late else 0.0,
-            "slots": n_slots, "graph_launches": st1["graph_launches"] - st0["graph_launches"],
-            "gpu_launches": st1["kernels"] - st0["kernels"], "setup_s": setup_s,
-            "config": {"panel": "N=20,000 x M=1,200,000, 22 chromosomes, 3,500 cM, 1% missing",
-                       "l2": "70%: region M log-uniform [2k, 200k], K in {1,10,97} (resident annotations), "
-                             "INT8 exact or sketch d=1000, 1 cM, per-SNP masking",
-                       "h2": "20%: 1,000 traits x 200,000 regression SNPs, 200 blocks",
-                       "rg": "10%: 200 trait pairs x 200,000 regression SNPs, 200 blocks",
-                       "traits": "z = sqrt(N h2 l2 / M) b + e, h2 ~ U(0.05, 0.5), N log-uniform [1e4, 5e5], "
-                                 "chi2 = z^2; rg ~ U(-0.8, 0.8)"}}
+        by = {}
+        for d in ok:
+            by.setdefault(label(d[0], d[1]), []).append(d[2].latency_ms)
+        pairs = float(sum(d[3] for d in ok))
+        return {"workload": "serving", "metric": "request latency (ms) and throughput at a stated Poisson rate",
+                "rate_req_s": rate, "duration_s": duration_s, "requests": n_req, "completed": len(ok),
+                "failed": len(done) - len(ok), "errors": sorted({d[4] for d in done if d[4]})[:3],
+                "wall_s": wall, "throughput_req_s": len(ok) / wall, "l2_pairs_per_s": pairs / wall,
+                "latency_ms": pct(lat), "queue_ms": pct(que), "run_ms": pct(run),
+                "by_kind_latency_ms": {k: pct(np.array(v)) for k, v in sorted(by.items())},
+                "arrival_lag_ms_p99": float(np.percentile(late, 99) * 1e3) if late else 0.0,
+                "slots": n_slots, "graph_launches": st1["graph_launches"] - st0["graph_launches"],
+                "gpu_launches": st1["kernels"] - st0["kernels"], "setup_s": setup_s,
+                "config": {"panel": "N=20,000 x M=1,200,000, 22 chromosomes, 3,500 cM, 1% missing",
+                           "l2": "70%: region M log-uniform [2k, 200k], K in {1,10,97} (resident annotations), "
+                                 "INT8 exact or sketch d=1000, 1 cM, per-SNP masking",
+                           "h2": "20%: 1,000 traits x 200,000 regression SNPs, 200 blocks",
+                           "rg": "10%: 200 trait pairs x 200,000 regression SNPs, 200 blocks",
+                           "traits": "z = sqrt(N h2 l2 / M) b + e, h2 ~ U(0.05, 0.5), N log-uniform [1e4, 5e5], "
+                                     "chi2 = z^2; rg ~ U(-0.8, 0.8)"}}
+
+    try:
+        return [one_rate(r) for r in rates]
+    finally:
+        srv.close()
+        panel.close()
 
 
 def main():
@@ -648,6 +658,7 @@ def main():
     ap.add_argument("--h2p-annot", type=int, default=97, help="partitioned-h2: LD-score columns K")
     ap.add_argument("--h2p-traits", type=int, default=8, help="partitioned-h2: traits per call")
     ap.add_argument("--serve-rate", type=float, default=40.0, help="serving: Poisson arrivals per second")
+    ap.add_argument("--serve-rates", default="", help="serving workload: comma-separated rates, one line each")
     ap.add_argument("--serve-seconds", type=float, default=30.0, help="serving: length of the arrival window")
     ap.add_argument("--serve-slots", type=int, default=6, help="serving: concurrent job slots")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving summary of the default run")
@@ -697,7 +708,9 @@ def main():
         run_partitioned_h2_workload(args, ctx, stream)
         return
     if args.workload == "serving":
-        print(json.dumps(run_serving_workload(args, ctx, args.serve_seconds, args.serve_rate)), flush=True)
+        rates = [float(x) for x in args.serve_rates.split(",")] if args.serve_rates else [args.serve_rate]
+        for line in run_serving_workload(args, ctx, args.serve_seconds, rates):
+            print(json.dumps(line), flush=True)
         return
 
     # N > 1: the ranks split one panel into cores balanced by pair count, each
@@ -858,7 +871,7 @@ def main():
     serving = None
     if world == 1 and args.serve_seconds > 0 and not args.no_serving:
         try:
-            sv = run_serving_workload(args, ctx, min(args.serve_seconds, 10.0), args.serve_rate)
+            sv = run_serving_workload(args, ctx, min(args.serve_seconds, 10.0), [args.serve_rate])[0]
             serving = {k: sv[k] for k in ("rate_req_s", "duration_s", "requests", "completed", "failed",
                                           "throughput_req_s", "l2_pairs_per_s", "latency_ms", "queue_ms",
                                           "by_kind_latency_ms", "slots", "graph_launches")}
