@@ -37,6 +37,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "r2 pairs/sec (INT8 exact vs FP64 plain, same GPU); p50/p99 request latency"
 CPU_SAMPLE_SNPS = 3000
+SKETCH_ORACLE_SNPS = 2000
 
 
 def workload_spec(seed_offset=0, workload="biobank"):
@@ -249,8 +250,11 @@ def _timed_passes(ctx, stream, fn, warmup, steps):
 def run_sketch_workload(args, ctx, stream):
     """Fused CountSketch l2: N=100,000 x M=200,000 (1% missing, 150 cM),
     --sketch d --snp-level-masking, 1 cM.  Prints one JSON line per d with
-    the sketch pass rate, the scatter kernel's HBM roofline, and the error of
-    the sketched l2 against exact l2 (INT8 form) on the same panel."""
+    the sketch pass rate, the scatter kernel's HBM roofline, the error of the
+    sketched l2 against exact l2 (INT8 form) on the same panel, and -- on the
+    first SKETCH_ORACLE_SNPS records -- the GPU sketch against the oracle's
+    f32 --sketch path (seed-42 stream) and both sketches' Pearson r against
+    the oracle's exact l2 on that sample."""
     from ldsc_b200 import synth
     from ldsc_b200.api import WindowMode, pair_count, run_l2
     from ldsc_b200.plink import BimTable
@@ -269,6 +273,14 @@ def run_sketch_workload(args, ctx, stream):
     exact = outs[0][0][:, 0]
     hbm, bf16, src = measured_peaks()
     tf32_peak = bf16 / 2.0
+    # oracle sample: records [0, ms) of the same panel
+    from oracle import OracleL2Args, oracle_l2
+    ms = min(SKETCH_ORACLE_SNPS, m)
+    sample = BimTable(chr_[:ms], [f"rs{i}" for i in range(ms)], cm[:ms], bp[:ms], np.arange(ms, dtype=np.int64))
+    srows = panel.download(0, ms)
+    sarg = dict(bed_body=srows, n_file_indiv=spec.n_indiv, chr=chr_[:ms], cm=cm[:ms], bp=bp[:ms], chunk_c=200,
+                masking=True)
+    exact_o = oracle_l2(OracleL2Args(**sarg))[0][:, 0]
     for d in [int(x) for x in args.sketch_d.split(",")]:
         # the first call with this d builds the CountSketch layout (hash, bucket-major
         # order, panel rewritten in it): its one-time cost, then the timed passes
@@ -277,6 +289,13 @@ def run_sketch_workload(args, ctx, stream):
         t, outs = _timed_passes(ctx, stream, lambda: run_l2(ctx, snps, panel, wm, 200, snp_level_masking=True,
                                                             sketch=d, yes_really=True), args.warmup, args.steps)
         sk = outs[-1][0][:, 0]
+        sk_o = oracle_l2(OracleL2Args(**sarg, use_f32=True, sketch_d=d))[0][:, 0]
+        sk_g = run_l2(ctx, sample, panel, wm, 200, snp_level_masking=True, sketch=d, yes_really=True)[0][:, 0]
+        vs_oracle = {"snps": ms, "max_abs_diff": float(np.max(np.abs(sk_g - sk_o))),
+                     "max_rel_per_l2j": float(np.max(np.abs(sk_g - sk_o) / np.abs(sk_o))),
+                     "pearson_gpu_sketch_vs_exact": float(np.corrcoef(sk_g, exact_o)[0, 1]),
+                     "pearson_oracle_sketch_vs_exact": float(np.corrcoef(sk_o, exact_o)[0, 1]),
+                     "mean_exact_l2": float(np.mean(exact_o))}
         perf = outs[-1][2]
         sk_s = float(np.mean([o[2].sketch_secs for o in outs]))
         gram_s = float(np.mean([o[2].ab_dot_secs for o in outs]))
@@ -307,7 +326,8 @@ def run_sketch_workload(args, ctx, stream):
                "vs_exact": {"pearson_r": float(np.corrcoef(sk, exact)[0, 1]),
                             "max_abs_err": float(np.max(np.abs(sk - exact))),
                             "mean_abs_err": float(np.mean(np.abs(sk - exact))),
-                            "mean_exact_l2": float(np.mean(exact))}}
+                            "mean_exact_l2": float(np.mean(exact))},
+               "vs_oracle_sketch": vs_oracle}
         print(json.dumps(out), flush=True)
     panel.close()
 
