@@ -127,6 +127,7 @@ struct ldsc_ctx {
     GraphCache graphs;            // regression pipelines
     uint64_t graph_launches = 0;  // replays of cached graphs
     DevBuf rtiles, cptr_r, cidx_r, cptr_l, cidx_l;  // K > 1 contraction: r2u tiles and CSR tile lists
+    DevBuf prow, pcol;                              // K = 1: per-tile row / column sums
     DevBuf rg_jobs, rg_states, rg_outs, rg_part, rg_tdel, rg_y, rg_y2, rg_n, rg_ld, rg_wld, rg_sel, rg_pairs, rg_res;
     DevBuf ts_seps, ts_n1, ts_cnt, ts_dv, ts_outs;  // --two-step
     // partitioned h2
@@ -135,6 +136,7 @@ struct ldsc_ctx {
     // the host plan of the last l2 call, kept so the next one reuses its pages
     LeftLimits plan_left;
     std::vector<Tile> plan_tiles;
+    std::vector<int32_t> plan_ptr_r, plan_idx_r, plan_ptr_l, plan_idx_l;  // CSR tile lists
     // whole-file entry: staged file rows, the pitched panel, per-chunk events
     DevBuf bed_stage, bed_rows;
     std::vector<cudaEvent_t> feed_ev;
@@ -146,7 +148,7 @@ struct ldsc_ctx {
                       &pq, &err, &st_n, &st_s, &st_q, &st_q3,
                       &st_q4, &st_mean, &st_inv, &st_qinv, &st_kappa,
                       &packed, &tsum, &dbg,
-                      &rtiles, &cptr_r, &cidx_r, &cptr_l, &cidx_l,
+                      &rtiles, &cptr_r, &cidx_r, &cptr_l, &cidx_l, &prow, &pcol,
                       &rg_jobs, &rg_states, &rg_outs, &rg_part, &rg_tdel,
                       &rg_y, &rg_y2, &rg_n, &rg_ld, &rg_wld, &rg_sel,
                       &rg_pairs, &rg_res, &bed_stage, &bed_rows, &ts_seps, &ts_n1, &ts_cnt, &ts_dv, &ts_outs,
@@ -443,7 +445,9 @@ int ldsc_l2_workspace_bytes(const ldsc_l2_args* a, uint64_t n_indiv, uint64_t* b
     const uint64_t ntiles = band_tiles(L.left, ta, tb).size();
     uint64_t b = m * (12 + 32 + 16 * K) + 8 * m + 8 * (ntiles + 1) + 64;  // stats, l2/aeff, left, tiles
     if (d && a->sketch_maf_aware) b += 16 * m;
-    if (K > 1) b += (uint64_t)8 * ta * tb * ntiles + 8 * ntiles + 4 * (m / 64 + m / 128 + 4);  // f64 r2u tiles, lists
+    // f64 r2u tiles (K > 1) or per-tile row / column sums (K = 1), CSR tile lists
+    b += (K > 1 ? (uint64_t)8 * ta * tb * ntiles : (uint64_t)8 * (ta + tb) * ntiles) + 8 * ntiles +
+         4 * (m / 64 + m / 128 + 4);
     if (a->annot && !a->annot_on_device) b += 8 * m * K;
     if (a->bed_idx) b += 8 * m;
     if (a->keep_iids) b += 8 * a->n_keep;
@@ -841,9 +845,17 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
         CK(cudaMemcpyAsync(ctx->left.p, L.left.data(), 8 * nmom, cudaMemcpyHostToDevice, up));
         if (!tiles.empty())
             CK(cudaMemcpyAsync(ctx->tiles.p, tiles.data(), sizeof(Tile) * tiles.size(), cudaMemcpyHostToDevice, up));
-        // K > 1: CSR lists of tiles per right block and per left block for the contraction
-        if (K > 1 && !tiles.empty()) {
-            std::vector<int32_t> ptr_r(n_right + 1, 0), ptr_l(n_left + 1, 0), idx_r(tiles.size()), idx_l(tiles.size());
+        // CSR lists of tiles per right block and per left block: the K > 1
+        // contraction passes and the K = 1 reduction of per-tile sums.  The
+        // host lists live in the context until the next call (the copies
+        // read them asynchronously).
+        if (!tiles.empty()) {
+            std::vector<int32_t>&ptr_r = ctx->plan_ptr_r, &ptr_l = ctx->plan_ptr_l, &idx_r = ctx->plan_idx_r,
+                                  &idx_l = ctx->plan_idx_l;
+            ptr_r.assign(n_right + 1, 0);
+            ptr_l.assign(n_left + 1, 0);
+            idx_r.resize(tiles.size());
+            idx_l.resize(tiles.size());
             for (const Tile& t : tiles) {
                 ptr_r[t.b_blk + 1]++;
                 ptr_l[t.a_blk + 1]++;
@@ -855,7 +867,12 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
                 idx_r[fr[tiles[t].b_blk]++] = t;
                 idx_l[fl[tiles[t].a_blk]++] = t;
             }
-            CK(ctx->rtiles.ensure(sizeof(double) * (size_t)ta * tb * tiles.size()));
+            if (K > 1) {
+                CK(ctx->rtiles.ensure(sizeof(double) * (size_t)ta * tb * tiles.size()));
+            } else {
+                CK(ctx->prow.ensure(sizeof(double) * (size_t)ta * tiles.size()));
+                CK(ctx->pcol.ensure(sizeof(double) * (size_t)tb * tiles.size()));
+            }
             CK(ctx->cptr_r.ensure(4 * ptr_r.size()));
             CK(ctx->cidx_r.ensure(4 * idx_r.size()));
             CK(ctx->cptr_l.ensure(4 * ptr_l.size()));
@@ -864,8 +881,6 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
             CK(cudaMemcpyAsync(ctx->cidx_r.p, idx_r.data(), 4 * idx_r.size(), cudaMemcpyHostToDevice, up));
             CK(cudaMemcpyAsync(ctx->cptr_l.p, ptr_l.data(), 4 * ptr_l.size(), cudaMemcpyHostToDevice, up));
             CK(cudaMemcpyAsync(ctx->cidx_l.p, idx_l.data(), 4 * idx_l.size(), cudaMemcpyHostToDevice, up));
-            // the host vectors are read by the copies above before they go out of scope
-            CK(cudaStreamSynchronize(up));
         }
         return join_up();
     };
@@ -902,6 +917,8 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
         if (rc != LDSC_OK) return rc;
         ep.left = ctx->left.as<int64_t>();
         ep.rtiles = nullptr;
+        ep.prow = tiles.empty() ? nullptr : ctx->prow.as<double>();
+        ep.pcol = tiles.empty() ? nullptr : ctx->pcol.as<double>();
     }
     if (chunked) {
         int rc = feed->start(s);
@@ -953,12 +970,16 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
                     size_t t1 = t0;
                     while (t1 < tiles.size() && (r1 == m || (int64_t)(tiles[t1].b_blk + 1) * tb <= r1)) t1++;
                     if (t1 > t0) {
+                        // this launch's tiles write their sums at their own tile indices
+                        EpilogueArgs ec = ep;
+                        ec.prow += t0 * ta;
+                        ec.pcol += t0 * tb;
                         if (fused_i8)
                             CK(launch_gram_i8_packed(pv.rows, pv.pitch, n_used, m, ctx->tiles.as<Tile>() + t0,
-                                                     (int64_t)(t1 - t0), ep, nullptr, ctx->sms, s));
+                                                     (int64_t)(t1 - t0), ec, nullptr, ctx->sms, s));
                         else
                             CK(launch_gram_i8(ctx->ops.as<uint8_t>(), ld_i8, m, ctx->tiles.as<Tile>() + t0,
-                                              (int64_t)(t1 - t0), ep, nullptr, ctx->sms, s));
+                                              (int64_t)(t1 - t0), ec, nullptr, ctx->sms, s));
                         ctx->kernels++;
                     }
                     t0 = t1;
@@ -998,6 +1019,8 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
         if (rc != LDSC_OK) return rc;
         ep.left = ctx->left.as<int64_t>();
         ep.rtiles = (K > 1 && !tiles.empty()) ? ctx->rtiles.as<double>() : nullptr;
+        ep.prow = (K == 1 && !tiles.empty()) ? ctx->prow.as<double>() : nullptr;
+        ep.pcol = (K == 1 && !tiles.empty()) ? ctx->pcol.as<double>() : nullptr;
     }
     // ---- band Gram + epilogue ----
     const int e2 = ev.mark();
@@ -1025,6 +1048,13 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
                                ctx->cidx_l.as<int32_t>(), n_left, false, ep, s));
             ctx->kernels += 2;
         }
+    }
+    if (K == 1 && !tiles.empty()) {
+        // the per-tile sums into l2, in a fixed order
+        CK(launch_l2_reduce(m, ta, tb, ctx->cptr_r.as<int32_t>(), ctx->cidx_r.as<int32_t>(), ctx->cptr_l.as<int32_t>(),
+                            ctx->cidx_l.as<int32_t>(), ctx->prow.as<double>(), ctx->pcol.as<double>(),
+                            ctx->l2.as<double>(), s));
+        ctx->kernels++;
     }
     const int e3 = ev.mark();
     const cudaMemcpyKind okind = a->out_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;

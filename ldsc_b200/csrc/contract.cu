@@ -108,7 +108,32 @@ __global__ void __launch_bounds__(NT) k_contract(const double* __restrict__ rtil
     }
 }
 
+// K = 1: one thread per record, the record's column sums over the tiles of its
+// right block, then its row sums over the tiles of its left block, in list
+// order (coalesced: consecutive records read consecutive partials of a tile).
+__global__ void __launch_bounds__(NT) k_l2_reduce(int64_t m, int ta, int tb, const int32_t* __restrict__ ptr_r,
+                                                  const int32_t* __restrict__ idx_r, const int32_t* __restrict__ ptr_l,
+                                                  const int32_t* __restrict__ idx_l, const double* __restrict__ prow,
+                                                  const double* __restrict__ pcol, double* __restrict__ l2) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= m) return;
+    double acc = l2[j];
+    const int64_t rb = j / tb, lb = j / ta;
+    for (int32_t i = ptr_r[rb]; i < ptr_r[rb + 1]; i++) acc += pcol[(size_t)idx_r[i] * tb + (j - rb * tb)];
+    for (int32_t i = ptr_l[lb]; i < ptr_l[lb + 1]; i++) acc += prow[(size_t)idx_l[i] * ta + (j - lb * ta)];
+    l2[j] = acc;
+}
+
 }  // namespace
+
+cudaError_t launch_l2_reduce(int64_t m, int ta, int tb, const int32_t* ptr_r, const int32_t* idx_r,
+                             const int32_t* ptr_l, const int32_t* idx_l, const double* prow, const double* pcol,
+                             double* l2, cudaStream_t stream) {
+    if (m <= 0) return cudaSuccess;
+    k_l2_reduce<<<(unsigned)((m + NT - 1) / NT), NT, 0, stream>>>(m, ta, tb, ptr_r, idx_r, ptr_l, idx_l, prow, pcol,
+                                                                  l2);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_contract(const double* rtiles, int ta, int tb, const Tile* tiles, const int32_t* ptr,
                             const int32_t* idx, int32_t nblocks, bool by_right, const EpilogueArgs& ep,
@@ -136,6 +161,7 @@ cudaError_t preload_contract() {
     if (e == cudaSuccess) e = preload_kernel(k_contract<64, 128, false>);
     if (e == cudaSuccess) e = preload_kernel(k_contract<128, 128, true>);
     if (e == cudaSuccess) e = preload_kernel(k_contract<128, 128, false>);
+    if (e == cudaSuccess) e = preload_kernel(k_l2_reduce);
     return e;
 }
 

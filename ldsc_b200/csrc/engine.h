@@ -63,6 +63,11 @@ struct EpilogueArgs {
     double sketch_d;          // d as double   (sketch form)
     unsigned int* err;        // device error word (non-zero = a bounded wait gave up)
     double* rtiles;           // K > 1: tile t's masked r2u values, ta rows (k) x tb (j) f64 at t * ta * tb
+    // K = 1: tile t's row sums (ta values at prow + t * ta: sum_j r2u a_j for
+    // each left record k) and column sums (tb values at pcol + t * tb), added
+    // to l2 in a fixed order by launch_l2_reduce; null = atomics into l2
+    double* prow;
+    double* pcol;
 };
 
 // ---- kernels (launchers return cudaError_t of the launch) ----
@@ -175,6 +180,13 @@ cudaError_t preload_contract();
 cudaError_t preload_synth();
 cudaError_t preload_regress();
 cudaError_t preload_partitioned();
+
+// K = 1: l2[j] += the column sums of the tiles of j's right block, then the
+// row sums of the tiles of j's left block, in list order (deterministic).
+// ptr/idx: the CSR tile lists of launch_contract.
+cudaError_t launch_l2_reduce(int64_t m, int ta, int tb, const int32_t* ptr_r, const int32_t* idx_r,
+                             const int32_t* ptr_l, const int32_t* idx_l, const double* prow, const double* pcol,
+                             double* l2, cudaStream_t stream);
 
 // Synthetic panel generator (founder mosaic, counter-based RNG).
 cudaError_t launch_synth(uint8_t* rows, uint64_t pitch, uint64_t n_indiv, uint64_t n_snp,

@@ -139,7 +139,11 @@ __global__ void __launch_bounds__(NT, 1)
                 v += __shfl_xor_sync(0xFFFFFFFFu, v, 2);
                 v += __shfl_xor_sync(0xFFFFFFFFu, v, 1);
                 const int64_t k = k0 + ty + 16 * i;
-                if (tx == 0 && k < m && v != 0.0) atomicAdd(ep.l2 + k, v);
+                if (ep.prow) {
+                    if (tx == 0) ep.prow[(size_t)t * TA + ty + 16 * i] = v;   // summed by launch_l2_reduce
+                } else if (tx == 0 && k < m && v != 0.0) {
+                    atomicAdd(ep.l2 + k, v);
+                }
             }
             double* cpart = reinterpret_cast<double*>(smem_raw);  // [16][TB], fits the operand area
 #pragma unroll
@@ -150,7 +154,10 @@ __global__ void __launch_bounds__(NT, 1)
 #pragma unroll
                 for (int r = 0; r < 16; r++) v += cpart[r * TB + tid];
                 const int64_t j = j0 + tid;
-                if (j < m && v != 0.0) atomicAdd(ep.l2 + j, v);
+                if (ep.pcol)
+                    ep.pcol[(size_t)t * TB + tid] = v;
+                else if (j < m && v != 0.0)
+                    atomicAdd(ep.l2 + j, v);
             }
             __syncthreads();
         } else {

@@ -147,6 +147,7 @@ __global__ void __launch_bounds__(gram_threads(EW, CW), 1)
     uint64_t* drain = tempty + 2;       // [1]
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
     double* cpart = reinterpret_cast<double*>(drain + 2);  // [4][TB]
+    double* rpart = cpart + 4 * TB;                         // [4][TA]: row sums per column group
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
@@ -462,12 +463,27 @@ __global__ void __launch_bounds__(gram_threads(EW, CW), 1)
             }
             if (ep.K == 1) {
                 rsum += __shfl_xor_sync(0xFFFFFFFFu, rsum, 1);
-                if (grow && kval && rsum != 0.0) atomicAdd(ep.l2 + k, rsum);
-                named_bar_sync(1, EPI_T);
-                if (et < TB) {
-                    const int64_t j = j0 + et;
-                    const double cs = cpart[et] + cpart[TB + et] + cpart[2 * TB + et] + cpart[3 * TB + et];
-                    if (j < m && cs != 0.0) atomicAdd(ep.l2 + j, cs);
+                if (ep.prow) {
+                    // per-tile sums in fixed order; launch_l2_reduce adds them to l2
+                    constexpr int G = EPI_T / 128;   // warps per TMEM lane quarter (column groups)
+                    if (grow) rpart[(ew >> 2) * TA + (row >> 1)] = rsum;
+                    named_bar_sync(1, EPI_T);
+                    if (et < TA) {
+                        double rs = 0.0;
+#pragma unroll
+                        for (int g = 0; g < G; g++) rs += rpart[g * TA + et];
+                        ep.prow[(size_t)t * TA + et] = rs;
+                    }
+                    if (et < TB)
+                        ep.pcol[(size_t)t * TB + et] = cpart[et] + cpart[TB + et] + cpart[2 * TB + et] + cpart[3 * TB + et];
+                } else {
+                    if (grow && kval && rsum != 0.0) atomicAdd(ep.l2 + k, rsum);
+                    named_bar_sync(1, EPI_T);
+                    if (et < TB) {
+                        const int64_t j = j0 + et;
+                        const double cs = cpart[et] + cpart[TB + et] + cpart[2 * TB + et] + cpart[3 * TB + et];
+                        if (j < m && cs != 0.0) atomicAdd(ep.l2 + j, cs);
+                    }
                 }
                 named_bar_sync(1, EPI_T);
             } else {
@@ -551,7 +567,7 @@ static cudaError_t launch_tc(const void* ops, CUtensorMapDataType dt, uint64_t e
         return cudaErrorInvalidValue;
     const int num_kb = (int)(ld_elems * elem_bytes / 128);
     const size_t ctrl = ctrl_bytes(4);  // upper bound over the stage counts used
-    const size_t cbytes = sizeof(double) * 4 * TB;
+    const size_t cbytes = sizeof(double) * 4 * (TB + TA);   // column and row partials
     int64_t grid = n_tiles < sms ? n_tiles : sms;
     if (dbg) grid = 1;
     // more epilogue warps where the epilogue outweighs the MMAs: sixteen for
@@ -599,7 +615,7 @@ cudaError_t launch_gram_i8_packed(const uint8_t* rows, uint64_t pitch, uint64_t 
     if (!make_packed_map(&tmA, rows, pitch, (uint64_t)m, TA) || !make_packed_map(&tmB, rows, pitch, (uint64_t)m, TB))
         return cudaErrorInvalidValue;
     const int num_kb = (int)((n_indiv + 127) / 128);
-    const size_t cbytes = sizeof(double) * 4 * TB;
+    const size_t cbytes = sizeof(double) * 4 * (TB + TA);   // column and row partials
     const size_t pbytes = (size_t)P_STAGES * P_BYTES;
     int64_t grid = n_tiles < sms ? n_tiles : sms;
     if (dbg) grid = 1;
