@@ -211,3 +211,75 @@ def test_scatter_subsample_matches_all_iids_on_full_keep():
         b = scatter_column_f32(row, n, bucket, sign, mean, inv, float(n), d,
                                iid_idx=np.arange(n, dtype=np.int64))
         assert np.array_equal(a, b)
+
+
+def _numpy_sketch_l2(body, n, chr_, cm, bp, d, maf_aware):
+    """Independent restatement of the --sketch d --snp-level-masking path on
+    the CPU: per SNP the f32 LUT values (normalize_col_f32_with_stats,
+    src/l2/normalize.rs:115-154) scattered into d buckets in individual order
+    (src/wasm_simd.rs:1617-1784) and renormalised with an f64 norm; the
+    per-pair quadratic bias inversion with the kurtosis shift when MAF-aware
+    (quadratic_sketch_correction[_maf_aware], src/l2/compute.rs:947-998;
+    per_snp_kappa, :525-538); l2_j = 1 + the corrected r^2 over the SNP's own
+    window."""
+    from ldsc_b200.plink import decode_genotypes
+    from oracle import block_lefts, countsketch_hash
+    G = decode_genotypes(body, n)                      # M x N, NaN missing
+    m = G.shape[0]
+    bucket, sign = countsketch_hash(n, d, 42)
+    S = np.zeros((m, d), dtype=np.float32)
+    kappa = np.zeros(m)
+    for j in range(m):
+        g = G[j]
+        pres = ~np.isnan(g)
+        cnt = pres.sum()
+        gv = np.where(pres, g, 0.0)
+        mean = gv.sum() / cnt if cnt else 0.0
+        css = (gv * gv).sum() - cnt * mean * mean
+        sd = np.sqrt(css / n)
+        inv = np.float32(1.0 / sd) if sd > 0 else np.float32(0.0)
+        m32 = np.float32(mean)
+        lut = {2.0: (np.float32(2.0) - m32) * inv, 1.0: (np.float32(1.0) - m32) * inv, 0.0: (-m32) * inv}
+        vals = np.array([lut[x] if p else np.float32(0.0) for x, p in zip(gv, pres)], dtype=np.float32)
+        out = np.zeros(d, dtype=np.float32)
+        np.add.at(out, bucket, (sign * vals).astype(np.float32))
+        nrm = float(np.sum(out.astype(np.float64) ** 2))
+        if nrm > 0:
+            out = out * np.float32(np.sqrt(n / nrm))
+        S[j] = out
+        if cnt and css > 0:
+            dv = gv[pres] - mean
+            kappa[j] = float((dv ** 4).sum()) / css ** 2
+    bl, _ = block_lefts(chr_, cm, bp, "cm", 1.0)
+    denom = n - 2.0
+    l2 = np.ones(m)
+    for j in range(m):
+        for k in range(bl[j], j):
+            val = float(np.dot(S[j].astype(np.float64), S[k].astype(np.float64)))
+            kap = (kappa[j] + kappa[k]) if maf_aware else 0.0
+            tilde = val * val / (n * n)
+            dm3 = d - 3.0 - 2.0 * kap
+            disc = dm3 * dm3 + 8.0 * (d * tilde - 1.0)
+            r2 = (-dm3 + np.sqrt(disc)) / 4.0 if disc >= 0 else 0.0
+            r2u = r2 * (1 + 1 / denom) - 1 / denom
+            l2[j] += r2u
+            l2[k] += r2u
+    return l2
+
+
+@pytest.mark.parametrize("name", ["cm1_sketch50", "cm1_sketch200", "cm1_sketch50_maf", "cm1_sketch200_maf"])
+def test_oracle_sketch_matches_numpy_restatement(name):
+    """The oracle's sketch path, plain and MAF-aware, against the restatement
+    above on the golden panel (the dot products here are f64 over the f32
+    sketched values, the oracle's are f32: agreement to f32 rounding)."""
+    z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "small_panel.npz"))
+    from golden.make_golden import MODES
+    d = MODES[name][6]
+    got = _numpy_sketch_l2(z["body"], int(z["n_indiv"]), z["chr"], z["cm"], z["bp"], d, name.endswith("_maf"))
+    ref = z[f"l2_{name}"][:, 0]
+    # measured ~5e-7 (the f32 dot products' rounding)
+    assert np.max(np.abs(got - ref)) < 1e-5
+    if name.endswith("_maf"):
+        # the kurtosis shift is visible: the plain correction differs by far more
+        plain = z[f"l2_{name[:-4]}"][:, 0]
+        assert np.max(np.abs(plain - ref)) > 1000 * np.max(np.abs(got - ref))
