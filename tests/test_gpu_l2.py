@@ -14,6 +14,10 @@ GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 EXACT_TOL = 1e-9
 # K > 1: r2u tiles contracted with the annotations in f64, relative per l2_jC
 ANNOT_TOL = 1e-9
+# --sketch: absolute on l2.  Summing each bucket exactly instead of in f32
+# individual order moves l2 by ~2.4e-6 at d = 50 on the golden panel (CPU
+# restatement of both), the f32 dot products by ~5e-7.
+SKETCH_TOL = 2e-5
 
 
 def table(chr_, cm, bp):
@@ -44,15 +48,15 @@ def small_panel(ctx, small):
 
 
 def run_mode(ctx, small, panel, name, precision):
-    from golden.make_golden import MODES, annot3
+    from golden.make_golden import MAF_AWARE, MODES, annot3
     from ldsc_b200.api import WindowMode, run_l2
     mode, wind, chunk, masking, per_chr, f32, sk, has_annot, pq = MODES[name]
     wm = {"cm": WindowMode.Cm, "kb": WindowMode.Kb, "snp": WindowMode.Snp}[mode](wind)
     snps = table(small["chr"], small["cm"], small["bp"])
     A = annot3(len(snps)) if has_annot else None
     return run_l2(ctx, snps, panel, wm, chunk, annot=A, pq_exp=pq, use_f32=f32, sketch=sk or None,
-                  snp_level_masking=masking, global_pass=not per_chr, precision=precision,
-                  yes_really=True)
+                  sketch_maf_aware=name in MAF_AWARE, snp_level_masking=masking, global_pass=not per_chr,
+                  precision=precision, yes_really=True)
 
 
 def test_micro_known_answer_from_bytes(ctx):
@@ -104,13 +108,32 @@ def test_fast_f32_flag_within_reference_tolerance(ctx, small, small_panel):
     assert relerr(l2, small["l2_cm1_chunk50"]) < EXACT_TOL
 
 
-def test_sketch_matches_oracle(ctx, small, small_panel):
-    """CountSketch d = 50, seed-42 stream.  The sketched columns differ from
-    the reference's f32 scatter only by its accumulation rounding."""
-    l2, maf, _ = run_mode(ctx, small, small_panel, "cm1_sketch50", "fp64")
-    ref = small["l2_cm1_sketch50"]
-    assert np.max(np.abs(l2 - ref)) < 1e-3 * max(1.0, np.abs(ref).max())
-    np.testing.assert_allclose(maf, small["maf_cm1_sketch50"], atol=1e-15)
+SKETCH_MODES = ["cm1_sketch50", "cm1_sketch200", "cm1_sketch50_maf", "cm1_sketch200_maf"]
+
+
+@pytest.mark.parametrize("name", SKETCH_MODES)
+def test_sketch_matches_oracle(ctx, small, small_panel, name):
+    """CountSketch d = 50 and 200, seed-42 stream, plain and MAF-aware
+    correction, against the oracle's f32 --sketch path.  The sketched values
+    differ only by rounding (here each bucket is summed exactly and rounded to
+    f32 once; the reference accumulates f32 in individual order), and the dot
+    products are f32-accurate on both sides."""
+    l2, maf, _ = run_mode(ctx, small, small_panel, name, "fp64")
+    ref = small[f"l2_{name}"]
+    assert np.max(np.abs(l2 - ref)) < SKETCH_TOL
+    np.testing.assert_allclose(maf, small[f"maf_{name}"], atol=1e-15)
+
+
+@pytest.mark.parametrize("d", [50, 200])
+def test_sketch_maf_aware_correction_runs(ctx, small, small_panel, d):
+    """--sketch-maf-aware is the kurtosis-shifted inversion, not the plain one:
+    the two differ by far more than the parity tolerance, as in the oracle."""
+    aware = run_mode(ctx, small, small_panel, f"cm1_sketch{d}_maf", "fp64")[0]
+    plain = run_mode(ctx, small, small_panel, f"cm1_sketch{d}", "fp64")[0]
+    gap = np.max(np.abs(aware - plain))
+    want = np.max(np.abs(small[f"l2_cm1_sketch{d}_maf"] - small[f"l2_cm1_sketch{d}"]))
+    assert gap > 100 * SKETCH_TOL
+    assert abs(gap - want) < 2 * SKETCH_TOL
 
 
 def test_keep_subset_matches_oracle(ctx, small, small_panel):
