@@ -668,8 +668,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--fp64-steps", type=int, default=2)
-    ap.add_argument("--two-pass-steps", type=int, default=5,
-                    help="passes of the two-pass INT8 form (staged operand rows) timed for comparison")
+    ap.add_argument("--fused-steps", type=int, default=5,
+                    help="passes of the fused INT8 form (no operand buffer) timed for comparison")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--weak", action="store_true",
@@ -823,10 +823,10 @@ def main():
             t64 = float(tt.item())
         fp64_value = pairs_all * args.fp64_steps / t64 / (1 if sharded else world)
 
-    # ---- the two-pass INT8 form (operand rows decoded into HBM, then the Gram) ----
-    two_pass = None
-    if not sharded and args.two_pass_steps > 0:
-        ctx2 = Context(local, staged_operands=True)
+    # ---- the fused INT8 form (packed rows expanded in shared memory, no operand buffer) ----
+    fused = None
+    if not sharded and args.fused_steps > 0:
+        ctx2 = Context(local, fused_operands=True)
         ctx2.set_stream(stream.cuda_stream)
         for _ in range(2):
             run_l2(ctx2, snps, panel, wm, 200, snp_level_masking=True, precision="int8", yes_really=True)
@@ -834,16 +834,16 @@ def main():
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         tp = []
-        for _ in range(args.two_pass_steps):
+        for _ in range(args.fused_steps):
             tp.append(run_l2(ctx2, snps, panel, wm, 200, snp_level_masking=True, precision="int8",
                              yes_really=True)[2])
         e1.record(stream)
         torch.cuda.synchronize()
         t2 = e0.elapsed_time(e1) / 1e3
-        two_pass = {"pairs_per_s": npairs * args.two_pass_steps / t2, "ms_per_pass": 1e3 * t2 / args.two_pass_steps,
-                    "gram_ms": 1e3 * float(np.mean([q.ab_dot_secs for q in tp])),
-                    "decode_ms": 1e3 * float(np.mean([q.norm_secs for q in tp])),
-                    "operand_bytes": 2 * m * ((spec.n_indiv + 127) // 128 * 128)}
+        fused = {"pairs_per_s": npairs * args.fused_steps / t2, "ms_per_pass": 1e3 * t2 / args.fused_steps,
+                 "gram_ms": 1e3 * float(np.mean([q.ab_dot_secs for q in tp])),
+                 "decode_ms": 1e3 * float(np.mean([q.norm_secs for q in tp])),
+                 "operand_bytes_saved": 2 * m * ((spec.n_indiv + 127) // 128 * 128)}
         ctx2.close()
 
     # ---- end to end through the whole-file C ABI entry point, host buffers ----
@@ -941,7 +941,7 @@ def main():
                          "int8_device_ms_per_pass": float(np.mean(dev_ms)),
                          "n_pairs_per_rank": int(rank_pairs),
                          "int8_vs_fp64_l2_max_rel_err": int8_err,
-                         "int8_two_pass": two_pass}}
+                         "int8_fused_operands": fused}}
         print(json.dumps(out))
     panel.close()
     ctx.close()

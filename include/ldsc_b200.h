@@ -143,17 +143,20 @@ int ldsc_abi_version(void);
 
 /* Create a context on CUDA device `device` (the reference creates one
  * GpuContext per run and shares it across chromosomes: src/l2/mod.rs:410-436).
- * flags: 0, or LDSC_CTX_STAGED_OPERANDS. */
+ * flags: 0, or LDSC_CTX_FUSED_OPERANDS. */
 int ldsc_ctx_create(int device, uint32_t flags, ldsc_ctx **out);
 
-/* Context flag: run the INT8-exact form as two passes -- decode the panel
- * into INT8 genotype / mask operand rows in device memory (2 bytes per
- * individual per SNP), then the band Gram over them -- instead of the default
- * fused Gram, which stages the packed 2-bit rows and expands them in shared
- * memory.  Results agree to rounding (the same integer sums); the fused form
- * needs no operand buffer.  Runs with --keep, or whose records are not
- * consecutive panel rows, always take the two-pass form. */
-#define LDSC_CTX_STAGED_OPERANDS 1u
+/* Context flag: run the INT8-exact form as one fused Gram that stages the
+ * packed 2-bit BED rows and expands them into operand tiles in shared memory,
+ * instead of the default two passes (decode the panel into INT8 genotype /
+ * mask operand rows in device memory, 2 bytes per individual per SNP, then the
+ * band Gram over them).  Results are bit-identical; the fused form needs no
+ * operand buffer (10 GB for 50,000 individuals x 100,000 SNPs) but its Gram
+ * is slower (shared-memory bandwidth: the expansion writes the same operand
+ * bytes the two-pass form's TMA copies write, on top of the packed rows).
+ * Runs with --keep, or whose records are not consecutive panel rows, always
+ * take the two-pass form. */
+#define LDSC_CTX_FUSED_OPERANDS 1u
 int ldsc_ctx_destroy(ldsc_ctx *ctx);
 
 /* Launch this context's work on an existing cudaStream_t (NULL = the

@@ -31,7 +31,7 @@ STATUS_NAMES = {
 
 WINDOW_CM, WINDOW_KB, WINDOW_SNP = 0, 1, 2
 PRECISION_FP64, PRECISION_INT8 = 0, 1
-CTX_STAGED_OPERANDS = 1   # context flag: INT8 form through materialised operand rows
+CTX_FUSED_OPERANDS = 1   # context flag: fused INT8 Gram over the packed rows (no operand buffer)
 
 
 class Progress(C.Structure):

@@ -193,7 +193,7 @@ extern "C" {
 int ldsc_abi_version(void) { return LDSC_B200_ABI_VERSION; }
 
 int ldsc_ctx_create(int device, uint32_t flags, ldsc_ctx** out) {
-    if (!out || (flags & ~LDSC_CTX_STAGED_OPERANDS)) return LDSC_E_INVALID;
+    if (!out || (flags & ~LDSC_CTX_FUSED_OPERANDS)) return LDSC_E_INVALID;
     *out = nullptr;
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
@@ -451,10 +451,9 @@ int ldsc_l2_workspace_bytes(const ldsc_l2_args* a, uint64_t n_indiv, uint64_t* b
     if (a->annot && !a->annot_on_device) b += 8 * m * K;
     if (a->bed_idx) b += 8 * m;
     if (a->keep_iids) b += 8 * a->n_keep;
-    // INT8 operand rows only when the Gram cannot read the packed rows in place
-    if (exact_i8 && (a->bed_idx || a->keep_iids)) b += 2 * m * round_up(n_used, 128);
+    // INT8 operand rows (the default two-pass form; an upper bound for the fused one)
+    if (exact_i8) b += 2 * m * round_up(n_used, 128);
     else if (d) b += 8 * m * round_up(d, 32);
-    else if (exact_i8) b += 0;
     else b += 8 * m * round_up(n_used, 128);
     *bytes = b;
     return LDSC_OK;
@@ -681,9 +680,10 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
     }
 
     const bool exact_i8 = !d && a->precision == LDSC_PRECISION_INT8;
-    // the INT8 Gram reads the packed rows in place when the records are the
-    // panel rows in order and every individual is used
-    const bool fused_i8 = exact_i8 && !a->bed_idx && !a->keep_iids && !(ctx->flags & LDSC_CTX_STAGED_OPERANDS);
+    // with LDSC_CTX_FUSED_OPERANDS the INT8 Gram reads the packed rows in
+    // place when the records are the panel rows in order and every individual
+    // is used
+    const bool fused_i8 = exact_i8 && !a->bed_idx && !a->keep_iids && (ctx->flags & LDSC_CTX_FUSED_OPERANDS);
     const int ta = (exact_i8 || d) ? 64 : 128, tb = 128;  // tcgen05 tiles: 64 x 128 records
     pf.gram_kind = d ? 2u : (exact_i8 ? 1u : 0u);
 
@@ -1269,7 +1269,7 @@ int ldsc_debug_gram_i8_tile(ldsc_ctx* ctx, const ldsc_panel* panel, uint64_t k0,
     const uint64_t ld = round_up(n, 128);
     cudaStream_t s = ctx->stream;
     CK(cudaSetDevice(ctx->device));
-    const bool fused = !(ctx->flags & LDSC_CTX_STAGED_OPERANDS);
+    const bool fused = (ctx->flags & LDSC_CTX_FUSED_OPERANDS) != 0;
     if (!fused) CK(ctx->ops.ensure((size_t)2 * m * ld));
     CK(ctx->st_n.ensure(4 * (size_t)m));
     CK(ctx->st_s.ensure(4 * (size_t)m));

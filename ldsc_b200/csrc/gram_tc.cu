@@ -304,6 +304,15 @@ __global__ void __launch_bounds__(gram_threads(EW, CW), 1)
         uint32_t oph = 0, pph = 0;
         bool ok = true;
         for (int64_t t = blockIdx.x; t < n_tiles && ok; t += gridDim.x) {
+            // records past the last one read as missing (the map's zero fill would read as genotype 2)
+            const Tile tl = tiles[t];
+            uint32_t live = 0;
+#pragma unroll
+            for (int i = 0; i < NPASS; i++) {
+                const int rr = (ct >> 3) + RPP * i;
+                const int64_t rec = i < APASS ? (int64_t)tl.a_blk * TA + rr : (int64_t)tl.b_blk * TB + (rr - TA);
+                live |= (rec < ep.m ? 1u : 0u) << i;
+            }
             for (int kb = 0; kb < num_kb; kb++) {
                 // every lane waits (TMA data visible to each reader); the warp agrees on the outcome
                 const bool got = mbar_wait(&pfull[ps], pph, WAIT_LIMIT_NS) &&
@@ -318,7 +327,8 @@ __global__ void __launch_bounds__(gram_threads(EW, CW), 1)
                 uint8_t* ob = sB + os * B_BYTES;
                 uint32_t w[NPASS];
 #pragma unroll
-                for (int i = 0; i < NPASS; i++) w[i] = *reinterpret_cast<const uint32_t*>(pk + offP[i]);
+                for (int i = 0; i < NPASS; i++)
+                    w[i] = (live >> i) & 1u ? *reinterpret_cast<const uint32_t*>(pk + offP[i]) : 0x55555555u;
                 const uint64_t i0 = (uint64_t)kb * 128 + (uint64_t)wd * 16;
                 if (i0 + 16 > n_indiv) {
                     // individuals past N (and the zero fill past the row) read as missing
