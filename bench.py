@@ -896,7 +896,7 @@ def main():
     achieved = ops / gram_avg / 1e12
     roofline = {"bound": "tensor", "achieved": achieved, "peak": int8_peak, "unit": "TFLOP/s",
                 "frac": achieved / int8_peak, "traffic": committed_traffic("k_gram_tc"),
-                "kernel": "k_gram_tc<4,0> (tcgen05.mma kind::i8)",
+                "kernel": "k_gram_tc<4,0,4,0> (tcgen05.mma kind::i8, TMA-staged operand rows)",
                 "note": "int8 ops counted like flops (2 per MAC, 4 products per pair); peak = 2 x "
                         + ("measured bf16 dense burst (MEASURED_PEAKS.json)" if src == "measured" else
                            "fallback bf16 dense burst 1590 TFLOP/s (MEASURED_PEAKS.json absent)")

@@ -20,16 +20,19 @@ namespace ldsc {
 namespace {
 
 constexpr int NT = 256;
-constexpr int CC = 32;  // annotation columns per CTA (4 per warp)
+constexpr int CW = 8;              // annotation columns per warp
+constexpr int CC = CW * NT / 32;   // annotation columns per CTA
+constexpr int ALD = CC + 2;        // staged annotation row stride (even: 16-byte reads; staging stores 2-way)
 
 // Grid: (output block, 32-column chunk), chunk fastest so the CTAs of one
 // output block run together and share its r2u tiles through L2.  Per tile the
 // r2u tile (padded row stride TB + 1: the 16 lanes of a half-warp that read
 // one column hit distinct bank pairs) and the CC annotation columns of the
 // summed side are staged in shared memory; thread (og, cg) owns output rows
-// og + 32 i (i < RJ) and columns 4 cg .. 4 cg + 3, in f64 registers across
-// all tiles of the block.  Warps whose four columns lie past K skip the
-// products.
+// og + 32 i (i < RJ) and columns CW cg .. CW cg + CW - 1, in f64 registers
+// across all tiles of the block.  Per summed index a warp reads its CW
+// annotation values as broadcasts and RJ r2u values, for RJ x CW fused
+// multiply-adds.  Warps whose columns lie past K skip the products.
 //   BY_RIGHT: out rows j of the right block, out[j][c] += sum_k R[k][j] A[k][c]  (RJ = TB / 32)
 //   BY_LEFT:  out rows k of the left block,  out[k][c] += sum_j R[k][j] A[j][c]  (RJ = TA / 32)
 template <int TA, int TB, bool BY_RIGHT>
@@ -42,7 +45,7 @@ __global__ void __launch_bounds__(NT) k_contract(const double* __restrict__ rtil
     constexpr int RLD = TB + 1;
     extern __shared__ double smd[];
     double* Rs = smd;                            // [TA][RLD]
-    double* As = smd + TA * RLD;                 // [NS][CC]
+    double* As = smd + TA * RLD;                 // [NS][ALD]
     const int tid = threadIdx.x;
     const int og = tid & 31, cg = tid >> 5;
     const int K = ep.K;
@@ -53,12 +56,12 @@ __global__ void __launch_bounds__(NT) k_contract(const double* __restrict__ rtil
         const int c0 = (int)(w % nchunks) * CC;
         const int32_t t0 = ptr[blk], t1 = ptr[blk + 1];
         if (t0 == t1) continue;
-        const bool active = c0 + 4 * cg < K;     // warp-uniform
-        double acc[RJ][4];
+        const bool active = c0 + CW * cg < K;    // warp-uniform
+        double acc[RJ][CW];
 #pragma unroll
         for (int i = 0; i < RJ; i++)
 #pragma unroll
-            for (int u = 0; u < 4; u++) acc[i][u] = 0.0;
+            for (int u = 0; u < CW; u++) acc[i][u] = 0.0;
         for (int32_t ti = t0; ti < t1; ti++) {
             const int32_t t = idx[ti];
             const Tile tl = tiles[t];
@@ -76,21 +79,24 @@ __global__ void __launch_bounds__(NT) k_contract(const double* __restrict__ rtil
             for (int q = tid; q < NS * CC; q += NT) {
                 const int r = q % NS, c = q / NS;
                 const int64_t srow = s0 + r;
-                As[r * CC + c] = (srow < m && c0 + c < K) ? __ldg(ep.aeff + srow + (int64_t)(c0 + c) * m) : 0.0;
+                As[r * ALD + c] = (srow < m && c0 + c < K) ? __ldg(ep.aeff + srow + (int64_t)(c0 + c) * m) : 0.0;
             }
             __syncthreads();
             if (!active) continue;
-#pragma unroll 4
+#pragma unroll 2
             for (int sidx = 0; sidx < NS; sidx++) {
-                const double2 a01 = *reinterpret_cast<const double2*>(As + sidx * CC + 4 * cg);
-                const double2 a23 = *reinterpret_cast<const double2*>(As + sidx * CC + 4 * cg + 2);
+                double a[CW];
+#pragma unroll
+                for (int u = 0; u < CW; u += 2) {
+                    const double2 v = *reinterpret_cast<const double2*>(As + sidx * ALD + CW * cg + u);
+                    a[u] = v.x;
+                    a[u + 1] = v.y;
+                }
 #pragma unroll
                 for (int i = 0; i < RJ; i++) {
                     const double r = BY_RIGHT ? Rs[sidx * RLD + og + 32 * i] : Rs[(og + 32 * i) * RLD + sidx];
-                    acc[i][0] = fma(r, a01.x, acc[i][0]);
-                    acc[i][1] = fma(r, a01.y, acc[i][1]);
-                    acc[i][2] = fma(r, a23.x, acc[i][2]);
-                    acc[i][3] = fma(r, a23.y, acc[i][3]);
+#pragma unroll
+                    for (int u = 0; u < CW; u++) acc[i][u] = fma(r, a[u], acc[i][u]);
                 }
             }
         }
@@ -100,8 +106,8 @@ __global__ void __launch_bounds__(NT) k_contract(const double* __restrict__ rtil
             const int64_t row = (int64_t)blk * OB + og + 32 * i;
             if (row >= m) continue;
 #pragma unroll
-            for (int u = 0; u < 4; u++) {
-                const int c = c0 + 4 * cg + u;
+            for (int u = 0; u < CW; u++) {
+                const int c = c0 + CW * cg + u;
                 if (c < K) ep.l2[row + (int64_t)c * m] += acc[i][u];
             }
         }
@@ -143,7 +149,7 @@ cudaError_t launch_contract(const double* rtiles, int ta, int tb, const Tile* ti
     const int64_t work = (int64_t)nblocks * nchunks;
     const unsigned grid = (unsigned)(work < 148 * 8 ? work : 148 * 8);
     auto go = [&](auto kern, int ns) {
-        const size_t smem = sizeof(double) * ((size_t)ta * (tb + 1) + (size_t)ns * CC);
+        const size_t smem = sizeof(double) * ((size_t)ta * (tb + 1) + (size_t)ns * ALD);
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         kern<<<grid, NT, smem, stream>>>(rtiles, tiles, ptr, idx, nblocks, ep);
