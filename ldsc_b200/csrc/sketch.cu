@@ -43,14 +43,19 @@ __device__ __forceinline__ T warp_sum(T v) {
 // Rewrite panel rows in bucket-major individual order, as bit-plane quads
 // (sketch_quad.cuh).  perm[p] = FAM index of the individual at permuted
 // position p (p < n_used); positions past n_used read as missing.  One CTA per
-// row, the row staged in shared memory when it fits (smem_row != 0); each
-// thread forms one 32-position half: its low-plane and high-plane words.
+// row, the row staged in shared memory when it fits (smem_row != 0).  A warp
+// forms 32 halves (32 positions each) per step: for half h lane l reads the
+// code at position 32 h + l (coalesced perm loads, eight halves' loads in
+// flight), two ballots give the half's low-plane and high-plane words, and
+// lane t keeps half t's pair, so the step ends in one coalesced 256-byte store.
 __global__ void __launch_bounds__(NT) k_sketch_permute(PanelView p, const int32_t* __restrict__ perm,
                                                        uint64_t n_used, uint32_t* __restrict__ out,
                                                        uint64_t out_pitch_words, int smem_row) {
     extern __shared__ uint32_t srow32[];
     const uint8_t* srow = reinterpret_cast<const uint8_t*>(srow32);
     const uint64_t halves = out_pitch_words / 2;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int NW = NT / 32;
     for (uint64_t r = blockIdx.x; r < p.n_snp; r += gridDim.x) {
         const uint8_t* row = p.rows + r * p.pitch;
         if (smem_row) {
@@ -61,20 +66,26 @@ __global__ void __launch_bounds__(NT) k_sketch_permute(PanelView p, const int32_
         }
         const uint8_t* from = smem_row ? srow : row;
         uint2* orow = reinterpret_cast<uint2*>(out + r * out_pitch_words);
-        for (uint64_t h = threadIdx.x; h < halves; h += NT) {
-            uint32_t lo = 0, hi = 0;
-#pragma unroll 4
+        for (uint64_t g0 = (uint64_t)warp * 32; g0 < halves; g0 += NW * 32) {
+            uint32_t my_lo = 0, my_hi = 0;
+#pragma unroll 8
             for (int t = 0; t < 32; t++) {
-                const uint64_t pos = h * 32 + t;
+                const uint64_t h = g0 + t;  // the same in every lane
+                if (h >= halves) break;
+                const uint64_t pos = h * 32 + lane;
                 uint32_t code = 1u;  // missing
                 if (pos < n_used) {
                     const int32_t iid = __ldg(perm + pos);
                     code = (from[iid >> 2] >> ((iid & 3) * 2)) & 3u;
                 }
-                lo |= (code & 1u) << t;
-                hi |= (code >> 1) << t;
+                const uint32_t lo = __ballot_sync(0xFFFFFFFFu, code & 1u);
+                const uint32_t hi = __ballot_sync(0xFFFFFFFFu, code >> 1);
+                if (lane == t) {
+                    my_lo = lo;
+                    my_hi = hi;
+                }
             }
-            orow[h] = make_uint2(lo, hi);
+            if (g0 + lane < halves) orow[g0 + lane] = make_uint2(my_lo, my_hi);
         }
         __syncthreads();
     }
