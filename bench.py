@@ -670,8 +670,6 @@ def main():
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--fused-steps", type=int, default=5,
                     help="passes of the fused INT8 form (no operand buffer) timed for comparison")
-    ap.add_argument("--pair-steps", type=int, default=5,
-                    help="passes of the two-pass INT8 form with its Gram on SM pairs, timed for comparison")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--weak", action="store_true",
@@ -848,35 +846,6 @@ def main():
                  "operand_bytes_saved": 2 * m * ((spec.n_indiv + 127) // 128 * 128)}
         ctx2.close()
 
-    # ---- the SM-pair Grams (tcgen05 cta_group::2 over 128 x 128 record tiles),
-    # over staged operand rows and over the packed rows ----
-    pair_forms = {}
-    if not sharded and args.pair_steps > 0:
-        ref_l2 = run_l2(ctx, snps, panel, wm, 200, snp_level_masking=True, precision="int8", yes_really=True)[0]
-        for key, kw in (("int8_sm_pairs", {"sm_pairs": True}),
-                        ("int8_fused_sm_pairs", {"sm_pairs": True, "fused_operands": True})):
-            ctx3 = Context(local, **kw)
-            ctx3.set_stream(stream.cuda_stream)
-            for _ in range(2):
-                got = run_l2(ctx3, snps, panel, wm, 200, snp_level_masking=True, precision="int8",
-                             yes_really=True)[0]
-            torch.cuda.synchronize()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            tp = []
-            for _ in range(args.pair_steps):
-                tp.append(run_l2(ctx3, snps, panel, wm, 200, snp_level_masking=True, precision="int8",
-                                 yes_really=True)[2])
-            e1.record(stream)
-            torch.cuda.synchronize()
-            t3 = e0.elapsed_time(e1) / 1e3
-            pair_forms[key] = {"pairs_per_s": npairs * args.pair_steps / t3,
-                               "ms_per_pass": 1e3 * t3 / args.pair_steps,
-                               "gram_ms": 1e3 * float(np.mean([q.ab_dot_secs for q in tp])),
-                               "decode_ms": 1e3 * float(np.mean([q.norm_secs for q in tp])),
-                               "l2_bit_identical_to_single_sm": bool(np.array_equal(got, ref_l2))}
-            ctx3.close()
-
     # ---- end to end through the whole-file C ABI entry point, host buffers ----
     e2e = None
     if not args.no_e2e:
@@ -972,7 +941,7 @@ def main():
                          "int8_device_ms_per_pass": float(np.mean(dev_ms)),
                          "n_pairs_per_rank": int(rank_pairs),
                          "int8_vs_fp64_l2_max_rel_err": int8_err,
-                         "int8_fused_operands": fused, **pair_forms}}
+                         "int8_fused_operands": fused}}
         print(json.dumps(out))
     panel.close()
     ctx.close()

@@ -143,7 +143,7 @@ int ldsc_abi_version(void);
 
 /* Create a context on CUDA device `device` (the reference creates one
  * GpuContext per run and shares it across chromosomes: src/l2/mod.rs:410-436).
- * flags: 0, or an OR of LDSC_CTX_FUSED_OPERANDS and LDSC_CTX_SM_PAIRS. */
+ * flags: 0, or LDSC_CTX_FUSED_OPERANDS. */
 int ldsc_ctx_create(int device, uint32_t flags, ldsc_ctx **out);
 
 /* Context flag: run the INT8-exact form as one fused Gram that stages the
@@ -157,12 +157,6 @@ int ldsc_ctx_create(int device, uint32_t flags, ldsc_ctx **out);
  * Runs with --keep, or whose records are not consecutive panel rows, always
  * take the two-pass form. */
 #define LDSC_CTX_FUSED_OPERANDS 1u
-/* Context flag: run the INT8-exact form's band Gram on SM pairs (clusters of
- * two CTAs sharing one tensor-core instruction over 128 x 128 record tiles:
- * each SM stages half of both operand tiles).  With LDSC_CTX_FUSED_OPERANDS
- * too, each SM expands only its own 64 + 64 packed rows per stage instead of
- * 64 + 128.  Results are bit-identical to the single-SM Gram. */
-#define LDSC_CTX_SM_PAIRS 2u
 int ldsc_ctx_destroy(ldsc_ctx *ctx);
 
 /* Launch this context's work on an existing cudaStream_t (NULL = the

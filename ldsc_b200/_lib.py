@@ -32,7 +32,6 @@ STATUS_NAMES = {
 WINDOW_CM, WINDOW_KB, WINDOW_SNP = 0, 1, 2
 PRECISION_FP64, PRECISION_INT8 = 0, 1
 CTX_FUSED_OPERANDS = 1   # context flag: fused INT8 Gram over the packed rows (no operand buffer)
-CTX_SM_PAIRS = 2         # context flag: two-pass INT8 Gram on SM pairs (tcgen05 cta_group::2)
 
 
 class Progress(C.Structure):

@@ -79,15 +79,13 @@ def _perf(p: L.Perf) -> L2Perf:
 class Context:
     """One engine context on a CUDA device (GpuContext, src/gpu.rs:92-130)."""
 
-    def __init__(self, device: int = 0, fused_operands: bool = False, sm_pairs: bool = False):
+    def __init__(self, device: int = 0, fused_operands: bool = False):
         """fused_operands: run the INT8 form as the fused packed-row Gram
         (LDSC_CTX_FUSED_OPERANDS, no operand buffer) instead of decoding the
-        operand rows into device memory first.  sm_pairs: run the two-pass
-        INT8 form's Gram on SM pairs (LDSC_CTX_SM_PAIRS, 128 x 128 record
-        tiles, one tensor-core instruction across two SMs)."""
+        operand rows into device memory first."""
         self.lib = L.load()
         h = C.c_void_p()
-        flags = (L.CTX_FUSED_OPERANDS if fused_operands else 0) | (L.CTX_SM_PAIRS if sm_pairs else 0)
+        flags = L.CTX_FUSED_OPERANDS if fused_operands else 0
         rc = self.lib.ldsc_ctx_create(int(device), flags, C.byref(h))
         if rc != L.LDSC_OK:
             raise LdscError(rc, f"could not create a context on CUDA device {device}")

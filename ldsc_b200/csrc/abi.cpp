@@ -128,7 +128,6 @@ struct ldsc_ctx {
     uint64_t graph_launches = 0;  // replays of cached graphs
     DevBuf rtiles, cptr_r, cidx_r, cptr_l, cidx_l;  // K > 1 contraction: r2u tiles and CSR tile lists
     DevBuf prow, pcol;                              // K = 1: per-tile row / column sums
-    DevBuf ptiles;                                  // SM-pair form: 128 x 128 pair tiles
     DevBuf rg_jobs, rg_states, rg_outs, rg_part, rg_tdel, rg_y, rg_y2, rg_n, rg_ld, rg_wld, rg_sel, rg_pairs, rg_res;
     DevBuf ts_seps, ts_n1, ts_cnt, ts_dv, ts_outs;  // --two-step
     // partitioned h2
@@ -137,7 +136,6 @@ struct ldsc_ctx {
     // the host plan of the last l2 call, kept so the next one reuses its pages
     LeftLimits plan_left;
     std::vector<Tile> plan_tiles;
-    std::vector<Tile> plan_band, plan_pairs;  // SM-pair form: band tiles, pair tiles
     std::vector<int32_t> plan_ptr_r, plan_idx_r, plan_ptr_l, plan_idx_l;  // CSR tile lists
     // whole-file entry: staged file rows, the pitched panel, per-chunk events
     DevBuf bed_stage, bed_rows;
@@ -150,7 +148,7 @@ struct ldsc_ctx {
                       &pq, &err, &st_n, &st_s, &st_q, &st_q3,
                       &st_q4, &st_mean, &st_inv, &st_qinv, &st_kappa,
                       &packed, &tsum, &dbg,
-                      &rtiles, &cptr_r, &cidx_r, &cptr_l, &cidx_l, &prow, &pcol, &ptiles,
+                      &rtiles, &cptr_r, &cidx_r, &cptr_l, &cidx_l, &prow, &pcol,
                       &rg_jobs, &rg_states, &rg_outs, &rg_part, &rg_tdel,
                       &rg_y, &rg_y2, &rg_n, &rg_ld, &rg_wld, &rg_sel,
                       &rg_pairs, &rg_res, &bed_stage, &bed_rows, &ts_seps, &ts_n1, &ts_cnt, &ts_dv, &ts_outs,
@@ -195,7 +193,7 @@ extern "C" {
 int ldsc_abi_version(void) { return LDSC_B200_ABI_VERSION; }
 
 int ldsc_ctx_create(int device, uint32_t flags, ldsc_ctx** out) {
-    if (!out || (flags & ~(LDSC_CTX_FUSED_OPERANDS | LDSC_CTX_SM_PAIRS))) return LDSC_E_INVALID;
+    if (!out || (flags & ~LDSC_CTX_FUSED_OPERANDS)) return LDSC_E_INVALID;
     *out = nullptr;
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
@@ -215,7 +213,7 @@ int ldsc_ctx_create(int device, uint32_t flags, ldsc_ctx** out) {
         static std::vector<int> preloaded;
         std::lock_guard<std::mutex> g(preload_mu);
         if (std::find(preloaded.begin(), preloaded.end(), device) == preloaded.end()) {
-            for (cudaError_t (*f)() : {preload_gram_tc, preload_gram_pair, preload_gram_simt, preload_decode, preload_sketch,
+            for (cudaError_t (*f)() : {preload_gram_tc, preload_gram_simt, preload_decode, preload_sketch,
                                        preload_contract, preload_synth, preload_regress, preload_partitioned})
                 if (f() != cudaSuccess) {
                     cudaGetLastError();
@@ -444,11 +442,8 @@ int ldsc_l2_workspace_bytes(const ldsc_l2_args* a, uint64_t n_indiv, uint64_t* b
     const uint32_t d = a->sketch_d;
     const bool exact_i8 = !d && a->precision == LDSC_PRECISION_INT8;
     const int ta = (exact_i8 || d) ? 64 : 128, tb = 128;
-    // the SM-pair form's 64 x 128 sub-tiles include the band tiles: an upper bound for INT8
-    std::vector<Tile> band = band_tiles(L.left, ta, tb), pairs, subs;
-    if (exact_i8) pair_tiles(band, &pairs, &subs);
-    const uint64_t ntiles = exact_i8 ? subs.size() : band.size();
-    uint64_t b = m * (12 + 32 + 16 * K) + 8 * m + 12 * (ntiles + 1) + 64;  // stats, l2/aeff, left, tiles
+    const uint64_t ntiles = band_tiles(L.left, ta, tb).size();
+    uint64_t b = m * (12 + 32 + 16 * K) + 8 * m + 8 * (ntiles + 1) + 64;  // stats, l2/aeff, left, tiles
     if (d && a->sketch_maf_aware) b += 16 * m;
     // f64 r2u tiles (K > 1) or per-tile row / column sums (K = 1), CSR tile lists
     b += (K > 1 ? (uint64_t)8 * ta * tb * ntiles : (uint64_t)8 * (ta + tb) * ntiles) + 8 * ntiles +
@@ -689,9 +684,6 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
     // place when the records are the panel rows in order and every individual
     // is used
     const bool fused_i8 = exact_i8 && !a->bed_idx && !a->keep_iids && (ctx->flags & LDSC_CTX_FUSED_OPERANDS);
-    // INT8 form with LDSC_CTX_SM_PAIRS: the Gram (two-pass or fused) runs on SM
-    // pairs over 128 x 128 pair tiles; every other pass sees their 64 x 128 sub-tiles
-    const bool pair_i8 = exact_i8 && (ctx->flags & LDSC_CTX_SM_PAIRS);
     const int ta = (exact_i8 || d) ? 64 : 128, tb = 128;  // tcgen05 tiles: 64 x 128 records
     pf.gram_kind = d ? 2u : (exact_i8 ? 1u : 0u);
 
@@ -846,23 +838,13 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
         if (L.any_full && !a->yes_really)
             std::printf("WARNING: LD window spans the entire chromosome. Use --yes-really to silence this warning.\n");
         pf.n_pairs = L.n_pairs;
-        if (pair_i8) {
-            band_tiles(L.left, ta, tb, &ctx->plan_band);
-            pair_tiles(ctx->plan_band, &ctx->plan_pairs, &tiles);
-        } else {
-            band_tiles(L.left, ta, tb, &tiles);
-        }
+        band_tiles(L.left, ta, tb, &tiles);
         pf.n_tiles = tiles.size();
         CK(ctx->left.ensure(sizeof(int64_t) * nmom));
         CK(ctx->tiles.ensure(sizeof(Tile) * (tiles.size() + 1)));
         CK(cudaMemcpyAsync(ctx->left.p, L.left.data(), 8 * nmom, cudaMemcpyHostToDevice, up));
         if (!tiles.empty())
             CK(cudaMemcpyAsync(ctx->tiles.p, tiles.data(), sizeof(Tile) * tiles.size(), cudaMemcpyHostToDevice, up));
-        if (pair_i8 && !ctx->plan_pairs.empty()) {
-            const std::vector<Tile>& pt = ctx->plan_pairs;
-            CK(ctx->ptiles.ensure(sizeof(Tile) * pt.size()));
-            CK(cudaMemcpyAsync(ctx->ptiles.p, pt.data(), sizeof(Tile) * pt.size(), cudaMemcpyHostToDevice, up));
-        }
         // CSR lists of tiles per right block and per left block: the K > 1
         // contraction passes and the K = 1 reduction of per-tile sums.  The
         // host lists live in the context until the next call (the copies
@@ -872,20 +854,16 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
                                   &idx_l = ctx->plan_idx_l;
             ptr_r.assign(n_right + 1, 0);
             ptr_l.assign(n_left + 1, 0);
-            // (a pair's second sub-tile can start past the last record: it holds
-            // no pair and is left out of both lists)
+            idx_r.resize(tiles.size());
+            idx_l.resize(tiles.size());
             for (const Tile& t : tiles) {
-                if ((int32_t)t.a_blk >= n_left) continue;
                 ptr_r[t.b_blk + 1]++;
                 ptr_l[t.a_blk + 1]++;
             }
             for (int32_t i = 0; i < n_right; i++) ptr_r[i + 1] += ptr_r[i];
             for (int32_t i = 0; i < n_left; i++) ptr_l[i + 1] += ptr_l[i];
-            idx_r.resize(ptr_r[n_right]);
-            idx_l.resize(ptr_l[n_left]);
             std::vector<int32_t> fr(ptr_r.begin(), ptr_r.end() - 1), fl(ptr_l.begin(), ptr_l.end() - 1);
             for (int32_t t = 0; t < (int32_t)tiles.size(); t++) {
-                if ((int32_t)tiles[t].a_blk >= n_left) continue;
                 idx_r[fr[tiles[t].b_blk]++] = t;
                 idx_l[fl[tiles[t].a_blk]++] = t;
             }
@@ -988,24 +966,15 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
                                              a->has_pq_exp, a->pq_exp, ctx->aeff.as<double>() + r0,
                                              ctx->l2.as<double>() + r0, s, annot_ld_dev));
                     ctx->kernels++;
-                    // tiles are ordered by right block; take those whose right block is
-                    // complete (pair tiles in the SM-pair form)
-                    const std::vector<Tile>& lt = pair_i8 ? ctx->plan_pairs : tiles;
-                    const size_t per = pair_i8 ? 2 : 1;  // sub-tiles per launched tile
+                    // tiles are ordered by right block; take those whose right block is complete
                     size_t t1 = t0;
-                    while (t1 < lt.size() && (r1 == m || (int64_t)(lt[t1].b_blk + 1) * tb <= r1)) t1++;
+                    while (t1 < tiles.size() && (r1 == m || (int64_t)(tiles[t1].b_blk + 1) * tb <= r1)) t1++;
                     if (t1 > t0) {
                         // this launch's tiles write their sums at their own tile indices
                         EpilogueArgs ec = ep;
-                        ec.prow += t0 * per * ta;
-                        ec.pcol += t0 * per * tb;
-                        if (pair_i8 && fused_i8)
-                            CK(launch_gram_i8_pair_packed(pv.rows, pv.pitch, n_used, m, ctx->ptiles.as<Tile>() + t0,
-                                                          (int64_t)(t1 - t0), ec, nullptr, ctx->sms, s));
-                        else if (pair_i8)
-                            CK(launch_gram_i8_pair(ctx->ops.as<uint8_t>(), ld_i8, m, ctx->ptiles.as<Tile>() + t0,
-                                                   (int64_t)(t1 - t0), ec, nullptr, ctx->sms, s));
-                        else if (fused_i8)
+                        ec.prow += t0 * ta;
+                        ec.pcol += t0 * tb;
+                        if (fused_i8)
                             CK(launch_gram_i8_packed(pv.rows, pv.pitch, n_used, m, ctx->tiles.as<Tile>() + t0,
                                                      (int64_t)(t1 - t0), ec, nullptr, ctx->sms, s));
                         else
@@ -1060,12 +1029,6 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
         if (d) {
             CK(launch_gram_tf32(ctx->xsk.as<float>(), ld_sk, m, ctx->tiles.as<Tile>(), (int64_t)tiles.size(), ep,
                                 maf_aware ? 1 : 0, nullptr, ctx->sms, s));
-        } else if (pair_i8 && fused_i8) {
-            CK(launch_gram_i8_pair_packed(pv.rows, pv.pitch, n_used, m, ctx->ptiles.as<Tile>(),
-                                          (int64_t)ctx->plan_pairs.size(), ep, nullptr, ctx->sms, s));
-        } else if (pair_i8) {
-            CK(launch_gram_i8_pair(ctx->ops.as<uint8_t>(), ld_i8, m, ctx->ptiles.as<Tile>(),
-                                   (int64_t)ctx->plan_pairs.size(), ep, nullptr, ctx->sms, s));
         } else if (fused_i8) {
             CK(launch_gram_i8_packed(pv.rows, pv.pitch, n_used, m, ctx->tiles.as<Tile>(), (int64_t)tiles.size(), ep,
                                      nullptr, ctx->sms, s));
@@ -1320,8 +1283,7 @@ int ldsc_debug_gram_i8_tile(ldsc_ctx* ctx, const ldsc_panel* panel, uint64_t k0,
     CK(ctx->l2.ensure(8 * (size_t)m));
     CK(ctx->tiles.ensure(sizeof(Tile)));
     CK(ctx->err.ensure(16));
-    const bool pair = (ctx->flags & LDSC_CTX_SM_PAIRS) != 0;
-    CK(ctx->dbg.ensure((pair ? 2 : 1) * 4 * 128 * 256));
+    CK(ctx->dbg.ensure(4 * 128 * 256));
     PanelView pv{panel->rows, panel->n_snp, panel->n_indiv, panel->bpr, panel->pitch};
     IndivSel sel{nullptr, n};
     RecStats st{};
@@ -1336,9 +1298,7 @@ int ldsc_debug_gram_i8_tile(ldsc_ctx* ctx, const ldsc_panel* panel, uint64_t k0,
     CK(launch_finalize_stats(m, n, st, nullptr, 1, 0, 0.0, ctx->aeff.as<double>(), ctx->l2.as<double>(), s));
     CK(cudaMemsetAsync(ctx->left.p, 0, 8 * (size_t)m, s));
     CK(cudaMemsetAsync(ctx->err.p, 0, 16, s));
-    // the SM-pair form runs the 128 x 128 pair tile holding k0; its left half
-    // (k0 / 64) % 2 is this tile
-    Tile t{(uint32_t)(pair ? k0 / 128 : k0 / 64), (uint32_t)(j0 / 128)};
+    Tile t{(uint32_t)(k0 / 64), (uint32_t)(j0 / 128)};
     CK(cudaMemcpyAsync(ctx->tiles.p, &t, sizeof(Tile), cudaMemcpyHostToDevice, s));
     EpilogueArgs ep{};
     ep.left = ctx->left.as<int64_t>();
@@ -1352,22 +1312,15 @@ int ldsc_debug_gram_i8_tile(ldsc_ctx* ctx, const ldsc_panel* panel, uint64_t k0,
     ep.r2u_a = 1.0;
     ep.r2u_b = 0.0;
     ep.err = ctx->err.as<unsigned int>();
-    if (fused && pair)
-        CK(launch_gram_i8_pair_packed(panel->rows, panel->pitch, n, m, ctx->tiles.as<Tile>(), 1, ep,
-                                      ctx->dbg.as<int32_t>(), ctx->sms, s));
-    else if (fused)
+    if (fused)
         CK(launch_gram_i8_packed(panel->rows, panel->pitch, n, m, ctx->tiles.as<Tile>(), 1, ep,
                                  ctx->dbg.as<int32_t>(), ctx->sms, s));
-    else if (pair)
-        CK(launch_gram_i8_pair(ctx->ops.as<uint8_t>(), ld, m, ctx->tiles.as<Tile>(), 1, ep, ctx->dbg.as<int32_t>(),
-                               ctx->sms, s));
     else
         CK(launch_gram_i8(ctx->ops.as<uint8_t>(), ld, m, ctx->tiles.as<Tile>(), 1, ep, ctx->dbg.as<int32_t>(),
                           ctx->sms, s));
     ctx->kernels += 3;
     unsigned int herr[4];
-    const size_t half = pair ? (size_t)((k0 / 64) % 2) * 128 * 256 : 0;
-    CK(cudaMemcpyAsync(out, ctx->dbg.as<int32_t>() + half, 4 * 128 * 256, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(out, ctx->dbg.p, 4 * 128 * 256, cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(herr, ctx->err.p, 16, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     if (herr[0]) return fail(ctx, LDSC_E_TIMEOUT, "Gram kernel wait timed out");

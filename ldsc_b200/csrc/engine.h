@@ -106,20 +106,6 @@ cudaError_t launch_gram_i8(const uint8_t* ops, uint64_t ld, int64_t m, const Til
                            int64_t n_tiles, const EpilogueArgs& ep, int32_t* dbg, int sms,
                            cudaStream_t stream);
 
-// INT8 band Gram on SM pairs (tcgen05 cta_group::2, clusters of two CTAs):
-// tiles are 128 x 128 records (a_blk in units of 128 left records); pair tile
-// t's epilogue writes 64 x 128 sub-tile 2t + r for the left half r, exactly as
-// launch_gram_i8 writes a tile (rtiles / prow / pcol indexed by sub-tile).
-// dbg (optional) receives both halves' raw accumulators of the first tile
-// (2 x 128 x 256 int32, left half r at r * 128 * 256).
-cudaError_t launch_gram_i8_pair(const uint8_t* ops, uint64_t ld, int64_t m, const Tile* tiles, int64_t n_tiles,
-                                const EpilogueArgs& ep, int32_t* dbg, int sms, cudaStream_t stream);
-// The same over the packed BED rows (the fused form of launch_gram_i8_packed):
-// each CTA stages its own 64 + 64 packed rows and expands them in place.
-cudaError_t launch_gram_i8_pair_packed(const uint8_t* rows, uint64_t pitch, uint64_t n_indiv, int64_t m,
-                                       const Tile* tiles, int64_t n_tiles, const EpilogueArgs& ep, int32_t* dbg,
-                                       int sms, cudaStream_t stream);
-
 // Fused INT8 band Gram over the packed BED rows themselves (record r at
 // rows + r * pitch, all n_indiv individuals): the kernel stages 2-bit rows by
 // TMA and expands them into the G / M operand tiles in shared memory, so no
@@ -187,7 +173,6 @@ cudaError_t preload_kernel(F* kernel) {
     return cudaFuncGetAttributes(&a, reinterpret_cast<const void*>(kernel));
 }
 cudaError_t preload_gram_tc();
-cudaError_t preload_gram_pair();
 cudaError_t preload_gram_simt();
 cudaError_t preload_decode();
 cudaError_t preload_sketch();

@@ -184,18 +184,6 @@ void band_tiles(const std::vector<int64_t>& left, int ta, int tb, std::vector<Ti
     }
 }
 
-void pair_tiles(const std::vector<Tile>& band, std::vector<Tile>* pairs, std::vector<Tile>* subs) {
-    pairs->clear();
-    subs->clear();
-    for (const Tile& t : band) {
-        const Tile p{t.a_blk / 2, t.b_blk};
-        if (!pairs->empty() && pairs->back().a_blk == p.a_blk && pairs->back().b_blk == p.b_blk) continue;
-        pairs->push_back(p);
-        subs->push_back(Tile{2 * p.a_blk, p.b_blk});
-        subs->push_back(Tile{2 * p.a_blk + 1, p.b_blk});
-    }
-}
-
 // ---- fastrand 2.3.0 WyRand (independent restatement of the published
 // algorithm; the crate is not vendored with the reference) ----
 namespace {

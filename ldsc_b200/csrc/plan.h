@@ -40,13 +40,6 @@ bool left_limits(int64_t m, const uint8_t* chr, const double* cm, const uint32_t
 std::vector<Tile> band_tiles(const std::vector<int64_t>& left, int ta, int tb);
 void band_tiles(const std::vector<int64_t>& left, int ta, int tb, std::vector<Tile>* out);
 
-// SM-pair tiles from band tiles of 64 x tb records (ordered by right block,
-// then left block): *pairs gets each (a / 2, b) once, in the same order, and
-// *subs the 64 x tb sub-tiles (2 p.a, b), (2 p.a + 1, b) of pair p at 2p and
-// 2p + 1 -- a superset of the band tiles whose extra entries hold no in-band
-// pair.
-void pair_tiles(const std::vector<Tile>& band, std::vector<Tile>* pairs, std::vector<Tile>* subs);
-
 // fastrand 2.3.0 WyRand stream as used by CountSketchProj::new
 // (src/l2/compute.rs:179-184): n bucket draws u32(..d), then n bool draws.
 void countsketch_hash(uint64_t n, uint32_t d, uint64_t seed, uint32_t* bucket, float* sign);

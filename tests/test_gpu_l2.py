@@ -177,30 +177,14 @@ def fused_ctx():
     c.close()
 
 
-@pytest.fixture(scope="module")
-def pair_ctx():
-    """Contexts that run the INT8 Gram on SM pairs: over staged operand rows
-    ("pair") and over the packed rows ("fused_pair")."""
-    from ldsc_b200.api import Context
-    c = {"pair": Context(0, sm_pairs=True), "fused_pair": Context(0, fused_operands=True, sm_pairs=True)}
-    yield c
-    for x in c.values():
-        x.close()
-
-
-def pick(form, ctx, fused_ctx, pair_ctx):
-    return {"fused": fused_ctx, **pair_ctx}.get(form, ctx)
-
-
-@pytest.mark.parametrize("form", ["fused", "staged", "pair", "fused_pair"])
-def test_int8_gram_tile_is_bit_exact(ctx, fused_ctx, pair_ctx, form):
+@pytest.mark.parametrize("form", ["fused", "staged"])
+def test_int8_gram_tile_is_bit_exact(ctx, fused_ctx, form):
     """Raw INT32 accumulators of one tcgen05 tile vs an integer recompute, for
     the fused Gram (packed rows expanded in shared memory; N = 777 leaves a
-    partial last stage), for the Gram over staged operand rows, and for the
-    SM-pair forms of both (the 64 x 128 half of a 128 x 128 pair tile)."""
+    partial last stage) and for the Gram over staged operand rows."""
     from ldsc_b200.api import debug_gram_i8_tile
     from ldsc_b200.plink import decode_genotypes
-    ctx = pick(form, ctx, fused_ctx, pair_ctx)
+    ctx = fused_ctx if form == "fused" else ctx
     spec = synth.PanelSpec(n_indiv=777, chrom_sizes=[300], chrom_cm=[3.0], founders=9, miss=0.05, seed=5)
     body = synth.bed_body(spec)
     panel = ctx.upload(body, spec.n_indiv)
@@ -221,12 +205,10 @@ def test_int8_gram_tile_is_bit_exact(ctx, fused_ctx, pair_ctx, form):
 
 
 @pytest.mark.parametrize("name", EXACT_MODES + ["cm1_annot3"])
-@pytest.mark.parametrize("form", ["fused", "pair", "fused_pair"])
-def test_int8_forms_agree_with_two_pass(ctx, fused_ctx, pair_ctx, small, small_panel, name, form):
-    """The fused INT8 Gram and the SM-pair Grams give l2 bit-identical to the
-    single-SM two-pass form: the same integer sums, the same per-tile sums,
-    and l2 summed in a fixed order in all of them."""
-    a, ma, pa = run_mode(pick(form, ctx, fused_ctx, pair_ctx), small, small_panel, name, "int8")
+def test_fused_and_staged_int8_forms_agree(ctx, fused_ctx, small, small_panel, name):
+    """The fused INT8 Gram and the two-pass form give bit-identical l2: the
+    same integer sums, and l2 summed in a fixed order in both."""
+    a, ma, pa = run_mode(fused_ctx, small, small_panel, name, "int8")
     b, mb, pb = run_mode(ctx, small, small_panel, name, "int8")
     assert np.array_equal(a, b)
     assert np.array_equal(ma, mb)
@@ -234,15 +216,15 @@ def test_int8_forms_agree_with_two_pass(ctx, fused_ctx, pair_ctx, small, small_p
 
 
 @pytest.mark.parametrize("n_indiv", [40, 128, 129, 1000])
-@pytest.mark.parametrize("form", ["fused", "staged", "pair", "fused_pair"])
-def test_int8_form_at_small_and_ragged_n(ctx, fused_ctx, pair_ctx, n_indiv, form):
+@pytest.mark.parametrize("form", ["fused", "staged"])
+def test_int8_form_at_small_and_ragged_n(ctx, fused_ctx, n_indiv, form):
     """Individual counts around the 128-individual stage: a packed row
     narrower than one stage (N = 40, 16-byte rows), exactly one stage, one
     individual into the next, and a ragged tail; against the brute-force
     definition."""
     from conftest import brute_force_l2
     from ldsc_b200.api import WindowMode, left_limits, run_l2
-    ctx = pick(form, ctx, fused_ctx, pair_ctx)
+    ctx = fused_ctx if form == "fused" else ctx
     spec = synth.PanelSpec(n_indiv=n_indiv, chrom_sizes=[260, 140], chrom_cm=[2.0, 1.0], founders=7, miss=0.03,
                            seed=n_indiv)
     body = synth.bed_body(spec)
@@ -396,13 +378,10 @@ def streamed():
     return spec, cm, bp
 
 
-@pytest.mark.parametrize("case", ["all_int8", "all_fp64", "every_other_int8", "unordered_int8", "sketch",
-                                  "all_int8_pair", "all_int8_fused_pair"])
-def test_whole_file_entry_matches_resident_panel(ctx, pair_ctx, streamed, case):
+@pytest.mark.parametrize("case", ["all_int8", "all_fp64", "every_other_int8", "unordered_int8", "sketch"])
+def test_whole_file_entry_matches_resident_panel(ctx, streamed, case):
     """ldsc_l2_from_bed streams the file through the copy stream and decodes
-    chunk by chunk; its results equal a run on the same rows uploaded first
-    (bit for bit when the streamed run's Gram is an SM-pair form, whose
-    launches follow the chunks in pair tiles)."""
+    chunk by chunk; its results equal a run on the same rows uploaded first."""
     from ldsc_b200.api import WindowMode, l2_from_bed_bytes, run_l2
     spec, cm, bp = streamed
     panel = ctx.synth(spec.n_indiv, spec.m, spec.founders, spec.switch_p, spec.miss, spec.seed)
@@ -424,11 +403,8 @@ def test_whole_file_entry_matches_resident_panel(ctx, pair_ctx, streamed, case):
     sk = 200 if case == "sketch" else None
     ref, ref_maf, _ = run_l2(ctx, snps, panel, WindowMode.Cm(1.0), 200, precision=prec, sketch=sk,
                              snp_level_masking=True, yes_really=True)
-    form = case[len("all_int8_"):] if case.endswith("pair") else None
-    got, maf, perf = l2_from_bed_bytes(pair_ctx[form] if form else ctx, bed, spec.n_indiv, snps,
-                                       WindowMode.Cm(1.0), 200, precision=prec, sketch=sk, snp_level_masking=True)
+    got, maf, perf = l2_from_bed_bytes(ctx, bed, spec.n_indiv, snps, WindowMode.Cm(1.0), 200, precision=prec,
+                                       sketch=sk, snp_level_masking=True)
     np.testing.assert_array_equal(maf, ref_maf)
     assert relerr(got, ref) < 1e-12
-    if form:
-        np.testing.assert_array_equal(got, ref)
     assert perf.bed_read_secs > 0
