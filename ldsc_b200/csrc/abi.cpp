@@ -114,6 +114,9 @@ struct ldsc_ctx {
     cudaStream_t own = nullptr;
     cudaStream_t stream = nullptr;
     cudaStream_t copy = nullptr;  // host-to-device BED stream of ldsc_l2_from_bed
+    cudaStream_t side = nullptr;  // low-priority stream of the decode that overlaps the Gram
+    std::vector<cudaEvent_t> ovl_ev;  // per decoded record chunk
+    cudaEvent_t ovl_go = nullptr;
     std::mutex mu;
     std::string last_error;
     uint64_t kernels = 0;
@@ -252,13 +255,16 @@ int ldsc_ctx_destroy(ldsc_ctx* ctx) {
     cudaStreamSynchronize(ctx->stream);
     std::vector<DevBuf*> bufs = ctx->workspace();
     cudaStreamSynchronize(ctx->copy);
+    if (ctx->side) cudaStreamSynchronize(ctx->side);
     for (DevBuf* b : bufs) b->release();
     ctx->sk.release();
     ctx->graphs.clear();
     cudaStreamSynchronize(ctx->stream);
     for (cudaEvent_t e : ctx->feed_ev) cudaEventDestroy(e);
-    for (cudaEvent_t e : {ctx->feed_t0, ctx->feed_t1, ctx->feed_go, ctx->up_ev})
+    for (cudaEvent_t e : ctx->ovl_ev) cudaEventDestroy(e);
+    for (cudaEvent_t e : {ctx->feed_t0, ctx->feed_t1, ctx->feed_go, ctx->up_ev, ctx->ovl_go})
         if (e) cudaEventDestroy(e);
+    if (ctx->side) cudaStreamDestroy(ctx->side);
     if (ctx->copy) cudaStreamDestroy(ctx->copy);
     if (ctx->own) cudaStreamDestroy(ctx->own);
     delete ctx;
@@ -486,9 +492,10 @@ struct Events {
     ~Events() {
         for (int i = 0; i < n; i++) cudaEventDestroy(ev[i]);
     }
-    int mark() {
+    int mark() { return mark_on(s); }
+    int mark_on(cudaStream_t on) {
         cudaEventCreate(&ev[n]);
-        cudaEventRecord(ev[n], s);
+        cudaEventRecord(ev[n], on);
         return n++;
     }
     double ms(int a, int b) const {
@@ -610,6 +617,32 @@ struct RowFeed {
         return t / 1e3;
     }
 };
+
+// The decode-overlap side stream (lowest priority, so the Gram's CTAs are
+// placed first when both wait for an SM) and n per-chunk events, created on
+// first use.
+int ensure_overlap(ldsc_ctx* ctx, int n) {
+    if (!ctx->side) {
+        int least = 0, greatest = 0;
+        CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        CK(cudaStreamCreateWithPriority(&ctx->side, cudaStreamNonBlocking, least));
+    }
+    if (!ctx->ovl_go) CK(cudaEventCreateWithFlags(&ctx->ovl_go, cudaEventDisableTiming));
+    while ((int)ctx->ovl_ev.size() < n) {
+        cudaEvent_t e;
+        CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        ctx->ovl_ev.push_back(e);
+    }
+    return LDSC_OK;
+}
+
+// Record chunks of the overlapped decode (each a multiple of the 128-record
+// right block), and the smallest run that overlaps.  On B200 at 50,000
+// individuals x 100,000 records, 4 and 8 chunks both cut a pass from 15.9 to
+// 15.4 ms; 16 chunks, or a decode confined to fewer blocks, slow the Gram
+// beside it more than they save.
+constexpr int64_t OVERLAP_CHUNKS = 4;
+constexpr int64_t OVERLAP_MIN_RECORDS = 16384;
 
 int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double* l2_out, double* maf_out,
            ldsc_perf* perf, double upload_secs, RowFeed* feed = nullptr) {
@@ -908,6 +941,14 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
     // with the upload too: after chunk k is decoded and finalised, the tiles
     // whose records all lie in chunks [0, k] run while later chunks copy.
     const bool stream_gram = chunked && exact_i8 && K == 1;
+    // Resident panels (two-pass INT8 form, one annotation column) overlap the
+    // decode of record chunk k + 1, on the side stream, with the band Gram of
+    // the tiles whose records all lie in chunks [0, k]: the decode is
+    // HBM-bound, the Gram tensor-bound, and decode blocks (40 registers x 256
+    // threads, no shared memory) fit on an SM beside a Gram CTA.
+    const bool overlap = !feed && exact_i8 && !fused_i8 && K == 1 && m >= OVERLAP_MIN_RECORDS;
+    const int64_t ov_per = overlap ? (int64_t)round_up((uint64_t)((m + OVERLAP_CHUNKS - 1) / OVERLAP_CHUNKS), 128) : 0;
+    const int ov_n = overlap ? (int)((m + ov_per - 1) / ov_per) : 0;
     if (stream_gram) {
         // the first chunk's copy runs while the host plans; the plan's uploads
         // queue behind that chunk only
@@ -931,7 +972,7 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
     // ---- decode ----
     const uint64_t ld_i8 = round_up(n_used, 128);
     const uint64_t ld_sk = round_up(d ? d : 1, 32);  // 128-byte operand rows for TMA
-    int e_sk = -1;
+    int e_sk = -1, e_side = -1;
     const bool staged_i8 = exact_i8 && !fused_i8;
     if (staged_i8) CK(ctx->ops.ensure((size_t)2 * nmom * ld_i8));
     if (chunked) {
@@ -988,6 +1029,35 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
             r0 = r1;
         }
         ctx->kernels--;  // counted once below
+    } else if (overlap) {
+        // decode and finalise chunk by chunk on the side stream, after the
+        // compute stream's work so far (uploads, the error-word reset)
+        int rc = ensure_overlap(ctx, ov_n);
+        if (rc != LDSC_OK) return rc;
+        CK(cudaEventRecord(ctx->ovl_go, s));
+        CK(cudaStreamWaitEvent(ctx->side, ctx->ovl_go, 0));
+        for (int k = 0; k < ov_n; k++) {
+            const int64_t r0 = k * ov_per, r1 = std::min<int64_t>(m, r0 + ov_per);
+            PanelView pc = pv;
+            if (!rr) pc.rows = pv.rows + (uint64_t)r0 * pv.pitch;
+            RecStats sc = st;
+            sc.n += r0;
+            sc.s += r0;
+            sc.q += r0;
+            sc.maf += r0;
+            sc.mean += r0;
+            sc.inv_std += r0;
+            sc.qinv += r0;
+            CK(launch_decode_i8(pc, rr ? rr + r0 : nullptr, r1 - r0, sel, ctx->ops.as<uint8_t>() + (size_t)2 * r0 * ld_i8,
+                                ld_i8, sc, 0, ctx->side));
+            CK(launch_finalize_stats(r1 - r0, n_used, sc, annot_dev ? annot_dev + r0 : nullptr, 1, a->has_pq_exp,
+                                     a->pq_exp, ctx->aeff.as<double>() + r0, ctx->l2.as<double>() + r0, ctx->side,
+                                     annot_ld_dev));
+            CK(cudaEventRecord(ctx->ovl_ev[k], ctx->side));
+            ctx->kernels += 2;
+        }
+        e_side = ev.mark_on(ctx->side);
+        ctx->kernels--;  // counted once below
     } else if (staged_i8) {
         CK(launch_decode_i8(pv, rr, m, sel, ctx->ops.as<uint8_t>(), ld_i8, st, 0, s));
     } else if (d) {
@@ -1000,7 +1070,7 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
         CK(launch_decode_i8(pv, rr, m, sel, nullptr, 0, st, 0, s));
     }
     ctx->kernels++;
-    if (!stream_gram) {
+    if (!stream_gram && !overlap) {
         CK(launch_finalize_stats(m, n_used, st, annot_dev, K, a->has_pq_exp, a->pq_exp, ctx->aeff.as<double>(),
                                  ctx->l2.as<double>(), s, annot_ld_dev));
         ctx->kernels++;
@@ -1023,9 +1093,31 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
         ep.pcol = (K == 1 && !tiles.empty()) ? ctx->pcol.as<double>() : nullptr;
     }
     // ---- band Gram + epilogue ----
+    if (overlap) CK(cudaStreamWaitEvent(s, ctx->ovl_ev[0], 0));  // the Gram's time starts at its first tiles
     const int e2 = ev.mark();
     int e_c = -1;
-    if (!tiles.empty() && !stream_gram) {
+    if (!tiles.empty() && overlap) {
+        // tiles are ordered by right block; chunk k's launch takes those whose
+        // right block is complete once chunks [0, k] are decoded
+        size_t t0 = 0;
+        for (int k = 0; k < ov_n; k++) {
+            const int64_t r1 = std::min<int64_t>(m, (k + 1) * ov_per);
+            size_t t1 = t0;
+            while (t1 < tiles.size() && (r1 == m || (int64_t)(tiles[t1].b_blk + 1) * tb <= r1)) t1++;
+            if (t1 == t0) continue;
+            CK(cudaStreamWaitEvent(s, ctx->ovl_ev[k], 0));
+            EpilogueArgs ec = ep;  // this launch's tiles write their sums at their own tile indices
+            ec.prow += t0 * ta;
+            ec.pcol += t0 * tb;
+            CK(launch_gram_i8(ctx->ops.as<uint8_t>(), ld_i8, m, ctx->tiles.as<Tile>() + t0, (int64_t)(t1 - t0), ec,
+                              nullptr, ctx->sms, s));
+            ctx->kernels++;
+            t0 = t1;
+        }
+    }
+    // every record's statistics are final before the reduction reads them
+    if (overlap) CK(cudaStreamWaitEvent(s, ctx->ovl_ev[ov_n - 1], 0));
+    if (!tiles.empty() && !stream_gram && !overlap) {
         if (d) {
             CK(launch_gram_tf32(ctx->xsk.as<float>(), ld_sk, m, ctx->tiles.as<Tile>(), (int64_t)tiles.size(), ep,
                                 maf_aware ? 1 : 0, nullptr, ctx->sms, s));
@@ -1067,7 +1159,7 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
     if (herr[0] != 0)
         return fail(ctx, LDSC_E_TIMEOUT, "a device wait in the Gram kernel exceeded its bound (error word " +
                                              std::to_string(herr[0]) + ")");
-    pf.norm_secs = ev.ms(d ? e_sk : e0, e1) / 1e3;
+    pf.norm_secs = ev.ms(d ? e_sk : e0, overlap ? e_side : e1) / 1e3;
     if (d) pf.sketch_secs = ev.ms(e0, e_sk) / 1e3;
     pf.ab_dot_secs = ev.ms(e2, e3) / 1e3;
     if (e_c >= 0 && K > 1) pf.contract_secs = ev.ms(e_c, e3) / 1e3;

@@ -215,6 +215,43 @@ def test_fused_and_staged_int8_forms_agree(ctx, fused_ctx, small, small_panel, n
     assert pa.n_pairs == pb.n_pairs
 
 
+@pytest.mark.parametrize("subset", ["all", "every_other"])
+def test_overlapped_decode_is_bit_identical(ctx, fused_ctx, subset):
+    """Resident panels of 16,384 records or more decode in record chunks on a
+    side stream while the Gram runs the tiles of chunks already decoded.  The
+    result equals, bit for bit, the fused form's (one Gram over packed rows,
+    no chunking) on the same records, including a record list (every other
+    row) whose chunks are not row ranges."""
+    from ldsc_b200.api import WindowMode, run_l2
+    spec = synth.PanelSpec(n_indiv=1500, chrom_sizes=[30000, 14000], chrom_cm=[40.0, 20.0], founders=30,
+                           miss=0.02, seed=77)
+    chr_, cm, bp = synth.positions(spec)
+    panel = ctx.synth(spec.n_indiv, spec.m, spec.founders, spec.switch_p, spec.miss, spec.seed)
+    try:
+        idx = np.arange(spec.m) if subset == "all" else np.arange(0, spec.m, 2)
+        if subset == "every_other":
+            assert len(idx) >= 16384   # still the overlapped form
+        snps = table(chr_[idx], cm[idx], bp[idx])
+        snps.bed_idx = idx.astype(np.int64)
+        got, maf, perf = run_l2(ctx, snps, panel, WindowMode.Cm(1.0), 200, snp_level_masking=True,
+                                precision="int8", yes_really=True)
+        # the same records as consecutive rows of their own panel, through the fused form
+        rows = panel.download()[idx]
+        sub = fused_ctx.upload(rows.reshape(-1), spec.n_indiv)
+        try:
+            snps2 = table(chr_[idx], cm[idx], bp[idx])
+            ref, ref_maf, rperf = run_l2(fused_ctx, snps2, sub, WindowMode.Cm(1.0), 200, snp_level_masking=True,
+                                         precision="int8", yes_really=True)
+        finally:
+            sub.close()
+        assert perf.n_pairs == rperf.n_pairs
+        np.testing.assert_array_equal(maf, ref_maf)
+        np.testing.assert_array_equal(got, ref)
+        assert perf.kernel_launches > rperf.kernel_launches   # chunked decode + Gram launches
+    finally:
+        panel.close()
+
+
 @pytest.mark.parametrize("n_indiv", [40, 128, 129, 1000])
 @pytest.mark.parametrize("form", ["fused", "staged"])
 def test_int8_form_at_small_and_ragged_n(ctx, fused_ctx, n_indiv, form):
