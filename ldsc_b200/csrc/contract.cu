@@ -14,129 +14,172 @@
 #include <cuda_runtime.h>
 
 #include "engine.h"
+#include "sm100.cuh"
 
 namespace ldsc {
 
 namespace {
 
-constexpr int NT = 256;
-constexpr int CW = 8;              // annotation columns per warp
-constexpr int CC = CW * NT / 32;   // annotation columns per CTA
-constexpr int ALD = CC + 2;        // staged annotation row stride (even: 16-byte reads; staging stores 2-way)
+constexpr int NT = 256;  // threads of k_l2_reduce
 
-// Grid: (output block, CC-column chunk), chunk fastest so the CTAs of one
-// output block run together and share its r2u tiles through L2.  Per tile,
-// in steps of JS summed records, the step's r2u values (padded row stride:
-// the lanes that read one column hit distinct bank pairs) and the CC
-// annotation columns of those records are staged in shared memory; thread
-// (og, cg) owns output rows og + 32 i (i < RJ) and columns CW cg .. CW cg +
-// CW - 1, in f64 registers across all tiles of the block.  Per summed record a
-// warp reads its CW annotation values as broadcasts and RJ r2u values, for
-// RJ x CW fused multiply-adds.  Warps whose columns lie past K skip the
-// products.  The left-block pass stages 64 of a tile's 128 right records at a
-// time, which keeps its shared memory at 67 KB (three CTAs per SM).
-//   BY_RIGHT: out rows j of the right block, out[j][c] += sum_k R[k][j] A[k][c]  (RJ = TB / 32)
-//   BY_LEFT:  out rows k of the left block,  out[k][c] += sum_j R[k][j] A[j][c]  (RJ = TA / 32)
+// The contraction on the FP64 tensor path (mma.sync m8n8k4 .f64):
+//   BY_RIGHT: out rows j of the right block, out[j][c] += sum_k R[k][j] A[k][c]
+//   BY_LEFT:  out rows k of the left block,  out[k][c] += sum_j R[k][j] A[j][c]
+// One CTA owns one output block and up to MK = 128 annotation columns (K > 128
+// runs column chunks).  The summed records of every tile of the block go by in
+// steps of JS_M = 32; a step's r2u values and the annotation values of its 32
+// records are staged by cp.async into one of two buffers while the MMAs run
+// on the other.  Warp (rg, cg) owns output rows 32 rg .. 32 rg + 31 and
+// columns 32 cg .. 32 cg + 31 of the chunk: 4 x 4 fragments of 8 x 8 f64
+// accumulators, eight k-steps of four records per staged step.  Fragment
+// layouts of m8n8k4 (row.col): A element (lane / 4, lane % 4), B element
+// (lane % 4, lane / 4), D elements (lane / 4, 2 (lane % 4) + {0, 1}).  Shared
+// rows are padded to a stride of 4 mod 16 doubles, so each half-warp's 16
+// 8-byte fragment loads hit 16 distinct bank pairs.
+constexpr int MK = 128;        // annotation columns per chunk
+constexpr int JS_M = 32;       // summed records per staged step
+constexpr int SLD = JS_M + 4;  // staged annotation stride (annotations are [column][record])
+
 template <int TA, int TB, bool BY_RIGHT>
-struct ContractShape {
+struct MmaShape {
     static constexpr int OB = BY_RIGHT ? TB : TA;          // output rows per block
     static constexpr int NS = BY_RIGHT ? TA : TB;          // summed records per tile
-    static constexpr int JS = BY_RIGHT ? NS : 64;          // summed records per staging step
-    static constexpr int RLD = BY_RIGHT ? TB + 1 : JS + 1; // staged r2u row stride (doubles)
-    static constexpr int RROWS = BY_RIGHT ? JS : TA;       // staged r2u rows
-    static constexpr size_t smem = sizeof(double) * ((size_t)RROWS * RLD + (size_t)JS * ALD);
+    static constexpr int SPT = NS / JS_M;                  // staged steps per tile
+    static constexpr int WARPS = (OB / 32) * (MK / 32);
+    static constexpr int THREADS = 32 * WARPS;
+    // r2u stage: BY_RIGHT [JS_M k][TB j], BY_LEFT [TA k][JS_M j]
+    static constexpr int RLD = BY_RIGHT ? TB + 4 : JS_M + 4;
+    static constexpr int RROWS = BY_RIGHT ? JS_M : TA;
+    static constexpr int R_ELEMS = RROWS * RLD;
+    static constexpr int A_ELEMS = MK * SLD;
+    static constexpr int STAGE = R_ELEMS + A_ELEMS;          // doubles per buffer
+    static constexpr size_t smem = sizeof(double) * 2 * (size_t)STAGE;
 };
 
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+
+// 8 bytes, or zeros (nothing read) when !valid
+__device__ __forceinline__ void cp_async8_zfill(void* dst, const void* src, bool valid) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(smem_u32(dst)), "l"(src),
+                 "r"(valid ? 8 : 0)
+                 : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
 template <int TA, int TB, bool BY_RIGHT>
-__global__ void __launch_bounds__(NT) k_contract(const double* __restrict__ rtiles, const Tile* __restrict__ tiles,
-                                                 const int32_t* __restrict__ ptr, const int32_t* __restrict__ idx,
-                                                 int32_t nblocks, EpilogueArgs ep) {
-    using S = ContractShape<TA, TB, BY_RIGHT>;
-    constexpr int OB = S::OB, NS = S::NS, JS = S::JS, RLD = S::RLD, RROWS = S::RROWS;
-    constexpr int RJ = OB / 32;                  // output rows per thread
-    extern __shared__ double smd[];
-    double* Rs = smd;                            // BY_RIGHT: [JS k][TB j]; BY_LEFT: [TA k][JS j]
-    double* As = smd + RROWS * RLD;              // [JS][ALD]
-    const int tid = threadIdx.x;
-    const int og = tid & 31, cg = tid >> 5;
+__global__ void __launch_bounds__(MmaShape<TA, TB, BY_RIGHT>::THREADS)
+    k_contract_mma(const double* __restrict__ rtiles, const Tile* __restrict__ tiles,
+                   const int32_t* __restrict__ ptr, const int32_t* __restrict__ idx, int32_t nblocks,
+                   EpilogueArgs ep) {
+    using S = MmaShape<TA, TB, BY_RIGHT>;
+    constexpr int NTH = S::THREADS, SPT = S::SPT, RLD = S::RLD, OB = S::OB;
+    extern __shared__ __align__(16) double smm[];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int rg = warp / (MK / 32), cg = warp % (MK / 32);
     const int K = ep.K;
     const int64_t m = ep.m;
-    const int nchunks = (K + CC - 1) / CC;
+    const int nchunks = (K + MK - 1) / MK;
+    const int fr = lane >> 2, fc = lane & 3;   // fragment row / column of this lane
+
     for (int64_t w = blockIdx.x; w < (int64_t)nblocks * nchunks; w += gridDim.x) {
         const int32_t blk = (int32_t)(w / nchunks);
-        const int c0 = (int)(w % nchunks) * CC;
+        const int c0 = (int)(w % nchunks) * MK;
         const int32_t t0 = ptr[blk], t1 = ptr[blk + 1];
-        if (t0 == t1) continue;
-        const bool active = c0 + CW * cg < K;    // warp-uniform
-        double acc[RJ][CW];
-#pragma unroll
-        for (int i = 0; i < RJ; i++)
-#pragma unroll
-            for (int u = 0; u < CW; u++) acc[i][u] = 0.0;
-        for (int32_t ti = t0; ti < t1; ti++) {
-            const int32_t t = idx[ti];
+        const int nsteps = (t1 - t0) * SPT;
+        if (nsteps == 0) continue;
+        const bool active = c0 + 32 * cg < K;  // warp-uniform: any of this warp's columns in range
+
+        // stage step st into buffer b
+        auto issue = [&](int st, int b) {
+            const int32_t t = idx[t0 + st / SPT];
+            const int js = (st % SPT) * JS_M;
             const Tile tl = tiles[t];
             const double* src = rtiles + (size_t)t * TA * TB;
-            // records of the summed side of this tile
-            const int64_t s0 = BY_RIGHT ? (int64_t)tl.a_blk * TA : (int64_t)tl.b_blk * TB;
-            for (int js = 0; js < NS; js += JS) {
-                __syncthreads();  // the previous step's stages are no longer read
-                if (BY_RIGHT) {
-                    // r2u rows k of the step, all TB columns
-#pragma unroll 4
-                    for (int q = tid; q < JS * TB / 2; q += NT) {
-                        const double2 v = __ldg(reinterpret_cast<const double2*>(src + (size_t)js * TB) + q);
-                        const int e = q * 2, r = e / TB, cc = e % TB;
-                        Rs[r * RLD + cc] = v.x;
-                        Rs[r * RLD + cc + 1] = v.y;
-                    }
-                } else {
-                    // all TA rows, columns js .. js + JS of the step
-#pragma unroll 4
-                    for (int q = tid; q < TA * JS / 2; q += NT) {
-                        const int e = q * 2, r = e / JS, cc = e % JS;
-                        const double2 v = __ldg(reinterpret_cast<const double2*>(src + (size_t)r * TB + js + cc));
-                        Rs[r * RLD + cc] = v.x;
-                        Rs[r * RLD + cc + 1] = v.y;
-                    }
+            double* Rs = smm + b * S::STAGE;
+            double* As = Rs + S::R_ELEMS;
+            if (BY_RIGHT) {
+                // rows k = js .. js + 31 of the tile, all TB values: 16-byte pieces
+#pragma unroll
+                for (int q = tid; q < JS_M * TB / 2; q += NTH) {
+                    const int r = q / (TB / 2), cc = 2 * (q % (TB / 2));
+                    cp_async16(Rs + r * RLD + cc, src + (size_t)(js + r) * TB + cc);
                 }
-                // annotation column c of record s0 + js + r at aeff[s0 + js + r + c * m]: consecutive r are coalesced
-#pragma unroll 4
-                for (int q = tid; q < JS * CC; q += NT) {
-                    const int r = q % JS, c = q / JS;
-                    const int64_t srow = s0 + js + r;
-                    As[r * ALD + c] = (srow < m && c0 + c < K) ? __ldg(ep.aeff + srow + (int64_t)(c0 + c) * m) : 0.0;
-                }
-                __syncthreads();
-                if (!active) continue;
-#pragma unroll 2
-                for (int sidx = 0; sidx < JS; sidx++) {
-                    double a[CW];
+            } else {
+                // all TA rows, values js .. js + 31
 #pragma unroll
-                    for (int u = 0; u < CW; u += 2) {
-                        const double2 v = *reinterpret_cast<const double2*>(As + sidx * ALD + CW * cg + u);
-                        a[u] = v.x;
-                        a[u + 1] = v.y;
-                    }
-#pragma unroll
-                    for (int i = 0; i < RJ; i++) {
-                        const double r = BY_RIGHT ? Rs[sidx * RLD + og + 32 * i] : Rs[(og + 32 * i) * RLD + sidx];
-#pragma unroll
-                        for (int u = 0; u < CW; u++) acc[i][u] = fma(r, a[u], acc[i][u]);
-                    }
+                for (int q = tid; q < TA * JS_M / 2; q += NTH) {
+                    const int r = q / (JS_M / 2), cc = 2 * (q % (JS_M / 2));
+                    cp_async16(Rs + r * RLD + cc, src + (size_t)r * TB + js + cc);
                 }
             }
+            // annotation column c0 + c of summed record s at aeff[s + (c0 + c) m]; consecutive threads
+            // take consecutive records (coalesced), zeros past m or K
+            const int64_t s0 = (BY_RIGHT ? (int64_t)tl.a_blk * TA : (int64_t)tl.b_blk * TB) + js;
+#pragma unroll
+            for (int e = tid; e < MK * JS_M; e += NTH) {
+                const int s = e & (JS_M - 1), c = e / JS_M;
+                const bool ok = s0 + s < m && c0 + c < K;
+                cp_async8_zfill(As + c * SLD + s, ok ? ep.aeff + (s0 + s) + (int64_t)(c0 + c) * m : ep.aeff, ok);
+            }
+        };
+
+        double acc[4][4][2];
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+        issue(0, 0);
+        cp_async_commit();
+        for (int st = 0; st < nsteps; st++) {
+            if (st + 1 < nsteps) issue(st + 1, (st + 1) & 1);
+            cp_async_commit();
+            cp_async_wait1();  // step st's copies (this thread's) have landed
+            __syncthreads();   // ... and every thread's
+            if (active) {
+                const double* Rs = smm + (st & 1) * S::STAGE;
+                const double* As = Rs + S::R_ELEMS;
+#pragma unroll
+                for (int kk = 0; kk < JS_M; kk += 4) {
+                    double a[4], b[4];
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        const int orow = 32 * rg + 8 * i + fr;  // output row of the fragment
+                        a[i] = BY_RIGHT ? Rs[(kk + fc) * RLD + orow] : Rs[orow * RLD + kk + fc];
+                    }
+#pragma unroll
+                    for (int j = 0; j < 4; j++) b[j] = As[(32 * cg + 8 * j + fr) * SLD + kk + fc];
+#pragma unroll
+                    for (int i = 0; i < 4; i++)
+#pragma unroll
+                        for (int j = 0; j < 4; j++) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+                }
+            }
+            __syncthreads();  // buffer st & 1 is refilled by the next iteration's issue
         }
         if (!active) continue;
 #pragma unroll
-        for (int i = 0; i < RJ; i++) {
-            const int64_t row = (int64_t)blk * OB + og + 32 * i;
+        for (int i = 0; i < 4; i++) {
+            const int64_t row = (int64_t)blk * OB + 32 * rg + 8 * i + fr;
             if (row >= m) continue;
 #pragma unroll
-            for (int u = 0; u < CW; u++) {
-                const int c = c0 + CW * cg + u;
-                if (c < K) ep.l2[row + (int64_t)c * m] += acc[i][u];
-            }
+            for (int j = 0; j < 4; j++)
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const int c = c0 + 32 * cg + 8 * j + 2 * fc + h;
+                    if (c < K) ep.l2[row + (int64_t)c * m] += acc[i][j][h];
+                }
         }
     }
 }
@@ -172,29 +215,28 @@ cudaError_t launch_contract(const double* rtiles, int ta, int tb, const Tile* ti
                             const int32_t* idx, int32_t nblocks, bool by_right, const EpilogueArgs& ep,
                             cudaStream_t stream) {
     if (nblocks <= 0) return cudaSuccess;
-    const int nchunks = (ep.K + CC - 1) / CC;
-    const int64_t work = (int64_t)nblocks * nchunks;
-    const unsigned grid = (unsigned)(work < 148 * 8 ? work : 148 * 8);
-    auto go = [&](auto kern, size_t smem) {
+    const int64_t work = (int64_t)nblocks * ((ep.K + MK - 1) / MK);
+    auto go = [&](auto kern, size_t smem, int threads) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        kern<<<grid, NT, smem, stream>>>(rtiles, tiles, ptr, idx, nblocks, ep);
+        // 512-thread CTAs (141 - 147 KB): one per SM; 256-thread CTAs (111 KB): two
+        const int64_t cap = (int64_t)148 * (threads <= 256 ? 2 : 1);
+        kern<<<(unsigned)(work < cap ? work : cap), threads, smem, stream>>>(rtiles, tiles, ptr, idx, nblocks, ep);
         return cudaGetLastError();
     };
-    if (ta == 64 && tb == 128)
-        return by_right ? go(k_contract<64, 128, true>, ContractShape<64, 128, true>::smem)
-                        : go(k_contract<64, 128, false>, ContractShape<64, 128, false>::smem);
-    if (ta == 128 && tb == 128)
-        return by_right ? go(k_contract<128, 128, true>, ContractShape<128, 128, true>::smem)
-                        : go(k_contract<128, 128, false>, ContractShape<128, 128, false>::smem);
+#define LDSC_CONTRACT(TA_, TB_, BR_) \
+    go(k_contract_mma<TA_, TB_, BR_>, MmaShape<TA_, TB_, BR_>::smem, MmaShape<TA_, TB_, BR_>::THREADS)
+    if (ta == 64 && tb == 128) return by_right ? LDSC_CONTRACT(64, 128, true) : LDSC_CONTRACT(64, 128, false);
+    if (ta == 128 && tb == 128) return by_right ? LDSC_CONTRACT(128, 128, true) : LDSC_CONTRACT(128, 128, false);
+#undef LDSC_CONTRACT
     return cudaErrorInvalidValue;
 }
 
 cudaError_t preload_contract() {
-    cudaError_t e = preload_kernel(k_contract<64, 128, true>);
-    if (e == cudaSuccess) e = preload_kernel(k_contract<64, 128, false>);
-    if (e == cudaSuccess) e = preload_kernel(k_contract<128, 128, true>);
-    if (e == cudaSuccess) e = preload_kernel(k_contract<128, 128, false>);
+    cudaError_t e = preload_kernel(k_contract_mma<64, 128, true>);
+    if (e == cudaSuccess) e = preload_kernel(k_contract_mma<64, 128, false>);
+    if (e == cudaSuccess) e = preload_kernel(k_contract_mma<128, 128, true>);
+    if (e == cudaSuccess) e = preload_kernel(k_contract_mma<128, 128, false>);
     if (e == cudaSuccess) e = preload_kernel(k_l2_reduce);
     return e;
 }
