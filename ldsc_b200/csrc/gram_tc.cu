@@ -94,6 +94,30 @@ __device__ __forceinline__ double sketch_r2u(float val, int64_t k, int64_t j, co
     return r2 * ep.r2u_a + ep.r2u_b;
 }
 
+// Sketch constants in f32 for sketch_r2u_f32.
+struct SketchF {
+    float n_inv_sq, d, r2u_a, r2u_b;
+};
+
+// sketch_r2u in f32, for d >= 8 (then dm3 > 2 - 2 kappa > 0 and the
+// discriminant is positive): the root (-dm3 + sqrt(disc)) / 4 is taken in the
+// cancellation-free form 2 q / (sqrt(disc) + dm3), q = d tilde - 1 (the same
+// value: disc - dm3^2 = 8 q).  Its absolute error is about ulp(d tilde) / dm3,
+// 3e-10 at d = 200, against the reference's f64 evaluation; l2 sums of a
+// thousand such terms move by ~1e-7 relative, far inside the sketch's own
+// f32 dot-product error.
+template <int MODE>
+__device__ __forceinline__ float sketch_r2u_f32(float val, int64_t k, int64_t j, const EpilogueArgs& ep,
+                                                const SketchF& cf) {
+    const float kap = MODE == 2 ? (float)(__ldg(ep.kappa + k) + __ldg(ep.kappa + j)) : 0.f;
+    const float tilde = val * val * cf.n_inv_sq;
+    const float dm3 = cf.d - 3.f - 2.f * kap;
+    const float q = fmaf(cf.d, tilde, -1.f);
+    const float disc = fmaf(dm3, dm3, 8.f * q);
+    const float r2 = disc >= 0.f ? 2.f * q / (sqrtf(disc) + dm3) : 0.f;
+    return fmaf(r2, cf.r2u_a, cf.r2u_b);
+}
+
 // CW = 0: A / B operand rows staged by TMA.  CW > 0 (INT8 only): packed 2-bit
 // rows staged by TMA (tmA / tmB map the BED rows, boxes of 32 bytes x 64 / 128
 // rows) and expanded by CW converter warps; n_indiv masks the last stage.
@@ -372,6 +396,8 @@ __global__ void __launch_bounds__(gram_threads(EW, CW), 1)
             }
             tc_fence_after();
             double rsum = 0.0;
+            const SketchF cf{(float)ep.n_inv_sq, (float)ep.sketch_d, (float)ep.r2u_a, (float)ep.r2u_b};
+            const bool f32_corr = MODE != 0 && ep.sketch_d >= 8.0;
             for (int c = c_lo; c < c_lo + CPW; c++) {
                 uint32_t v[64];
                 tmem_ld_32x32b_x64(tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)acc * 256u +
@@ -424,17 +450,29 @@ __global__ void __launch_bounds__(gram_threads(EW, CW), 1)
                         const float val = (grow ? pa : pb) + recv;
                         j = grow ? ja : jb;
                         valid = kval && pair_in_band(k, j, m, ep.left);
-                        if (valid) r2u = sketch_r2u<MODE>(val, k, j, ep);
+                        if (valid)
+                            r2u = f32_corr ? (double)sketch_r2u_f32<MODE>(val, k, j, ep, cf)
+                                           : sketch_r2u<MODE>(val, k, j, ep);
                     }
                     if (ep.K == 1) {
                         if (valid) rsum += r2u * __ldg(ep.aeff + j);
-                        // column j: sum over the 16 same-parity lanes of this warp
-                        double cv = r2u * ak;
-                        cv += __shfl_xor_sync(0xFFFFFFFFu, cv, 2);
-                        cv += __shfl_xor_sync(0xFFFFFFFFu, cv, 4);
-                        cv += __shfl_xor_sync(0xFFFFFFFFu, cv, 8);
-                        cv += __shfl_xor_sync(0xFFFFFFFFu, cv, 16);
-                        if (lane < 2) cpart[cslot * TB + c * 32 + p + lane] = cv;
+                        // column j: sum over the 16 same-parity lanes of this warp (in f32
+                        // for the sketch forms, whose terms carry f32 error already)
+                        if (MODE != 0) {
+                            float cv = (float)(r2u * ak);
+                            cv += __shfl_xor_sync(0xFFFFFFFFu, cv, 2);
+                            cv += __shfl_xor_sync(0xFFFFFFFFu, cv, 4);
+                            cv += __shfl_xor_sync(0xFFFFFFFFu, cv, 8);
+                            cv += __shfl_xor_sync(0xFFFFFFFFu, cv, 16);
+                            if (lane < 2) cpart[cslot * TB + c * 32 + p + lane] = (double)cv;
+                        } else {
+                            double cv = r2u * ak;
+                            cv += __shfl_xor_sync(0xFFFFFFFFu, cv, 2);
+                            cv += __shfl_xor_sync(0xFFFFFFFFu, cv, 4);
+                            cv += __shfl_xor_sync(0xFFFFFFFFu, cv, 8);
+                            cv += __shfl_xor_sync(0xFFFFFFFFu, cv, 16);
+                            if (lane < 2) cpart[cslot * TB + c * 32 + p + lane] = cv;
+                        }
                     } else {
                         // K > 1: the masked r2u value goes to the tile's f64 slot in
                         // global memory (record k's row of TB values) for the banded
