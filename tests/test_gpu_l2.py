@@ -215,8 +215,9 @@ def test_fused_and_staged_int8_forms_agree(ctx, fused_ctx, small, small_panel, n
     assert pa.n_pairs == pb.n_pairs
 
 
+@pytest.mark.parametrize("masking", [True, False], ids=["masked", "chunk200"])
 @pytest.mark.parametrize("subset", ["all", "every_other"])
-def test_overlapped_decode_is_bit_identical(ctx, fused_ctx, subset):
+def test_overlapped_decode_is_bit_identical(ctx, fused_ctx, subset, masking):
     """Resident panels of 16,384 records or more decode in record chunks on a
     side stream while the Gram runs the tiles of chunks already decoded.  The
     result equals, bit for bit, the fused form's (one Gram over packed rows,
@@ -233,15 +234,15 @@ def test_overlapped_decode_is_bit_identical(ctx, fused_ctx, subset):
             assert len(idx) >= 16384   # still the overlapped form
         snps = table(chr_[idx], cm[idx], bp[idx])
         snps.bed_idx = idx.astype(np.int64)
-        got, maf, perf = run_l2(ctx, snps, panel, WindowMode.Cm(1.0), 200, snp_level_masking=True,
+        got, maf, perf = run_l2(ctx, snps, panel, WindowMode.Cm(1.0), 200, snp_level_masking=masking,
                                 precision="int8", yes_really=True)
         # the same records as consecutive rows of their own panel, through the fused form
         rows = panel.download()[idx]
         sub = fused_ctx.upload(rows.reshape(-1), spec.n_indiv)
         try:
             snps2 = table(chr_[idx], cm[idx], bp[idx])
-            ref, ref_maf, rperf = run_l2(fused_ctx, snps2, sub, WindowMode.Cm(1.0), 200, snp_level_masking=True,
-                                         precision="int8", yes_really=True)
+            ref, ref_maf, rperf = run_l2(fused_ctx, snps2, sub, WindowMode.Cm(1.0), 200,
+                                         snp_level_masking=masking, precision="int8", yes_really=True)
         finally:
             sub.close()
         assert perf.n_pairs == rperf.n_pairs
