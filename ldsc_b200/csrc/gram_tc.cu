@@ -105,7 +105,9 @@ struct SketchF {
 // value: disc - dm3^2 = 8 q).  Its absolute error is about ulp(d tilde) / dm3,
 // 3e-10 at d = 200, against the reference's f64 evaluation; l2 sums of a
 // thousand such terms move by ~1e-7 relative, far inside the sketch's own
-// f32 dot-product error.
+// f32 dot-product error.  Each pair's value depends on that pair alone, so
+// runs over different tile grids (slices, shards) still agree to f64
+// rounding of the sums.
 template <int MODE>
 __device__ __forceinline__ float sketch_r2u_f32(float val, int64_t k, int64_t j, const EpilogueArgs& ep,
                                                 const SketchF& cf) {
@@ -456,23 +458,13 @@ __global__ void __launch_bounds__(gram_threads(EW, CW), 1)
                     }
                     if (ep.K == 1) {
                         if (valid) rsum += r2u * __ldg(ep.aeff + j);
-                        // column j: sum over the 16 same-parity lanes of this warp (in f32
-                        // for the sketch forms, whose terms carry f32 error already)
-                        if (MODE != 0) {
-                            float cv = (float)(r2u * ak);
-                            cv += __shfl_xor_sync(0xFFFFFFFFu, cv, 2);
-                            cv += __shfl_xor_sync(0xFFFFFFFFu, cv, 4);
-                            cv += __shfl_xor_sync(0xFFFFFFFFu, cv, 8);
-                            cv += __shfl_xor_sync(0xFFFFFFFFu, cv, 16);
-                            if (lane < 2) cpart[cslot * TB + c * 32 + p + lane] = (double)cv;
-                        } else {
-                            double cv = r2u * ak;
-                            cv += __shfl_xor_sync(0xFFFFFFFFu, cv, 2);
-                            cv += __shfl_xor_sync(0xFFFFFFFFu, cv, 4);
-                            cv += __shfl_xor_sync(0xFFFFFFFFu, cv, 8);
-                            cv += __shfl_xor_sync(0xFFFFFFFFu, cv, 16);
-                            if (lane < 2) cpart[cslot * TB + c * 32 + p + lane] = cv;
-                        }
+                        // column j: sum over the 16 same-parity lanes of this warp
+                        double cv = r2u * ak;
+                        cv += __shfl_xor_sync(0xFFFFFFFFu, cv, 2);
+                        cv += __shfl_xor_sync(0xFFFFFFFFu, cv, 4);
+                        cv += __shfl_xor_sync(0xFFFFFFFFu, cv, 8);
+                        cv += __shfl_xor_sync(0xFFFFFFFFu, cv, 16);
+                        if (lane < 2) cpart[cslot * TB + c * 32 + p + lane] = cv;
                     } else {
                         // K > 1: the masked r2u value goes to the tile's f64 slot in
                         // global memory (record k's row of TB values) for the banded
