@@ -838,7 +838,8 @@ def main():
         ctx2 = Context(local, fused_operands=True)
         ctx2.set_stream(stream.cuda_stream)
         for _ in range(2):
-            run_l2(ctx2, snps, panel, wm, 200, snp_level_masking=True, precision="int8", yes_really=True)
+            l2_fused = run_l2(ctx2, snps, panel, wm, 200, snp_level_masking=True, precision="int8",
+                              yes_really=True)[0]
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -852,7 +853,8 @@ def main():
         fused = {"pairs_per_s": npairs * args.fused_steps / t2, "ms_per_pass": 1e3 * t2 / args.fused_steps,
                  "gram_ms": 1e3 * float(np.mean([q.ab_dot_secs for q in tp])),
                  "decode_ms": 1e3 * float(np.mean([q.norm_secs for q in tp])),
-                 "operand_bytes_saved": 2 * m * ((spec.n_indiv + 127) // 128 * 128)}
+                 "operand_bytes_saved": 2 * m * ((spec.n_indiv + 127) // 128 * 128),
+                 "l2_bit_identical_to_two_pass": bool(np.array_equal(l2_fused, l2_last))}
         ctx2.close()
 
     # ---- end to end through the whole-file C ABI entry point, host buffers ----

@@ -253,6 +253,31 @@ def test_overlapped_decode_is_bit_identical(ctx, fused_ctx, subset, masking):
         panel.close()
 
 
+def test_fused_form_at_wide_rows(ctx, fused_ctx):
+    """Rows of 32,768 individuals or more run the fused Gram with four
+    epilogue and eight converter warps (narrower rows: eight and four); at
+    N = 33,001 (a ragged last stage) its l2 and MAF equal the two-pass form's
+    bit for bit, in both window modes."""
+    from ldsc_b200.api import WindowMode, run_l2
+    spec = synth.PanelSpec(n_indiv=33001, chrom_sizes=[700, 300], chrom_cm=[4.0, 2.0], founders=20, miss=0.02,
+                           seed=13)
+    chr_, cm, bp = synth.positions(spec)
+    snps = table(chr_, cm, bp)
+    body = synth.bed_body(spec)
+    pa, pb = ctx.upload(body, spec.n_indiv), fused_ctx.upload(body, spec.n_indiv)
+    try:
+        for masking in (True, False):
+            a, ma, _ = run_l2(ctx, snps, pa, WindowMode.Cm(1.0), 200, snp_level_masking=masking, precision="int8",
+                              yes_really=True)
+            b, mb, _ = run_l2(fused_ctx, snps, pb, WindowMode.Cm(1.0), 200, snp_level_masking=masking,
+                              precision="int8", yes_really=True)
+            np.testing.assert_array_equal(a, b)
+            np.testing.assert_array_equal(ma, mb)
+    finally:
+        pa.close()
+        pb.close()
+
+
 @pytest.mark.parametrize("n_indiv", [40, 128, 129, 1000])
 @pytest.mark.parametrize("form", ["fused", "staged"])
 def test_int8_form_at_small_and_ragged_n(ctx, fused_ctx, n_indiv, form):
