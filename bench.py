@@ -578,14 +578,14 @@ def run_serving_workload(args, ctx, duration_s: float, rates, seed: int = 7):
 
     n_slots = args.serve_slots
     srv = Server(torch.cuda.current_device(), n_slots=n_slots)
-    # warm-up: the shared sketch layout, then every slot grown to the largest
-    # request of each kind (one wave per kind, one job per slot)
+    # warm-up: the shared sketch layout, then every slot's workspace sized for
+    # the largest request of each kind (ldsc_server_prewarm runs a job on each
+    # slot in turn), so no request allocates device memory while others run
     srv.wait(submit(srv, "l2", dict(b=0, e=5000, K=1, sketch=1000)))
-    for wave in ([("l2", dict(b=i * 150000, e=i * 150000 + 200000, K=97, sketch=None)) for i in range(n_slots)],
-                 [("l2", dict(b=i * 150000, e=i * 150000 + 200000, K=97, sketch=1000)) for i in range(n_slots)],
-                 [("h2", {})] * n_slots + [("rg", dict(p0=0))] * n_slots):
-        for t in [submit(srv, k, p) for k, p in wave]:
-            srv.wait(t)
+    for k, p in [("l2", dict(b=500000, e=700000, K=97, sketch=None)), ("l2", dict(b=500000, e=700000, K=97, sketch=1000)),
+                 ("l2", dict(b=500000, e=700000, K=1, sketch=None)), ("l2", dict(b=500000, e=700000, K=1, sketch=1000)),
+                 ("h2", {}), ("rg", dict(p0=0))]:
+        srv.prewarm(lambda *a: submit(srv, k, p))
     setup_s = time.perf_counter() - t_setup
 
     def one_rate(rate):

@@ -419,6 +419,14 @@ int ldsc_server_create(int device, uint32_t n_slots, uint64_t device_budget, lds
 int ldsc_server_submit(ldsc_server *srv, const ldsc_job *job, uint64_t *ticket);
 /* Block until the job ends; returns its status and releases the ticket. */
 int ldsc_server_wait(ldsc_server *srv, uint64_t ticket, ldsc_job_result *result);
+/* Run `job` once on every slot, one slot after another, and return when the
+ * last has finished (no reference counterpart).  Each slot's workspace then
+ * holds what that job needs, so later jobs no larger than it start without
+ * allocating device memory: growing the device's memory pool while other
+ * slots run measured 0.1 - 0.9 s per allocation here, with the other slots'
+ * work held up meanwhile.  Prewarm with the largest job of each kind before
+ * serving.  The job's outputs are written once per slot. */
+int ldsc_server_prewarm(ldsc_server *srv, const ldsc_job *job);
 int ldsc_server_stats_get(ldsc_server *srv, ldsc_server_stats *stats);
 /* Finish running jobs, fail queued ones, free the slots. */
 int ldsc_server_destroy(ldsc_server *srv);

@@ -177,6 +177,7 @@ SIGNATURES = {
     "ldsc_server_submit": (C.c_int, [C.c_void_p, C.POINTER(Job), C.POINTER(C.c_uint64)]),
     "ldsc_server_wait": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(JobResult)]),
     "ldsc_server_stats_get": (C.c_int, [C.c_void_p, C.POINTER(ServerStats)]),
+    "ldsc_server_prewarm": (C.c_int, [C.c_void_p, C.POINTER(Job)]),
     "ldsc_server_destroy": (C.c_int, [C.c_void_p]),
     "ldsc_h2_batch": (C.c_int, [C.c_void_p, C.POINTER(H2Args), C.c_void_p]),
     "ldsc_rg_batch": (C.c_int, [C.c_void_p, C.POINTER(RgArgs), C.c_void_p]),

@@ -452,7 +452,8 @@ int ldsc_l2_workspace_bytes(const ldsc_l2_args* a, uint64_t n_indiv, uint64_t* b
     uint64_t b = m * (12 + 32 + 16 * K) + 8 * m + 8 * (ntiles + 1) + 64;  // stats, l2/aeff, left, tiles
     if (d && a->sketch_maf_aware) b += 16 * m;
     // f64 r2u tiles (K > 1) or per-tile row / column sums (K = 1), CSR tile lists
-    b += (K > 1 ? (uint64_t)8 * ta * tb * ntiles : (uint64_t)8 * (ta + tb) * ntiles) + 8 * ntiles +
+    const uint64_t nt_room = ntiles + ntiles / 8;  // the run's headroom on tile-count buffers
+    b += (K > 1 ? (uint64_t)8 * ta * tb * nt_room : (uint64_t)8 * (ta + tb) * nt_room) + 8 * nt_room +
          4 * (m / 64 + m / 128 + 4);
     if (a->annot && !a->annot_on_device) b += 8 * m * K;
     if (a->bed_idx) b += 8 * m;
@@ -874,7 +875,11 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
         band_tiles(L.left, ta, tb, &tiles);
         pf.n_tiles = tiles.size();
         CK(ctx->left.ensure(sizeof(int64_t) * nmom));
-        CK(ctx->tiles.ensure(sizeof(Tile) * (tiles.size() + 1)));
+        // buffers sized by the tile count get an eighth more when they grow: a
+        // later call over a few more tiles then reuses them instead of
+        // allocating (a pool growth while other work runs stalls it)
+        const size_t nt_room = tiles.size() + tiles.size() / 8;
+        CK(ctx->tiles.ensure(sizeof(Tile) * (nt_room + 1)));
         CK(cudaMemcpyAsync(ctx->left.p, L.left.data(), 8 * nmom, cudaMemcpyHostToDevice, up));
         if (!tiles.empty())
             CK(cudaMemcpyAsync(ctx->tiles.p, tiles.data(), sizeof(Tile) * tiles.size(), cudaMemcpyHostToDevice, up));
@@ -901,15 +906,15 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
                 idx_l[fl[tiles[t].a_blk]++] = t;
             }
             if (K > 1) {
-                CK(ctx->rtiles.ensure(sizeof(double) * (size_t)ta * tb * tiles.size()));
+                CK(ctx->rtiles.ensure(sizeof(double) * (size_t)ta * tb * nt_room));
             } else {
-                CK(ctx->prow.ensure(sizeof(double) * (size_t)ta * tiles.size()));
-                CK(ctx->pcol.ensure(sizeof(double) * (size_t)tb * tiles.size()));
+                CK(ctx->prow.ensure(sizeof(double) * (size_t)ta * nt_room));
+                CK(ctx->pcol.ensure(sizeof(double) * (size_t)tb * nt_room));
             }
             CK(ctx->cptr_r.ensure(4 * ptr_r.size()));
-            CK(ctx->cidx_r.ensure(4 * idx_r.size()));
+            CK(ctx->cidx_r.ensure(4 * nt_room));
             CK(ctx->cptr_l.ensure(4 * ptr_l.size()));
-            CK(ctx->cidx_l.ensure(4 * idx_l.size()));
+            CK(ctx->cidx_l.ensure(4 * nt_room));
             CK(cudaMemcpyAsync(ctx->cptr_r.p, ptr_r.data(), 4 * ptr_r.size(), cudaMemcpyHostToDevice, up));
             CK(cudaMemcpyAsync(ctx->cidx_r.p, idx_r.data(), 4 * idx_r.size(), cudaMemcpyHostToDevice, up));
             CK(cudaMemcpyAsync(ctx->cptr_l.p, ptr_l.data(), 4 * ptr_l.size(), cudaMemcpyHostToDevice, up));

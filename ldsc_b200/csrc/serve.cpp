@@ -31,6 +31,7 @@ struct JobRec {
     ldsc_job job;
     uint64_t need = 0;  // device workspace bytes
     int state = 0;      // 0 queued, 1 running, 2 done
+    int32_t pin = -1;   // slot that must run it (prewarm), or -1 for any
     ldsc_job_result res;
     Clock::time_point t_submit, t_start, t_end;
 };
@@ -103,6 +104,7 @@ struct ldsc_server {
         const uint64_t total = caps();
         for (size_t q = 0; q < pending.size(); q++) {
             JobRec* r = pending[q];
+            if (r->pin >= 0 && r->pin != (int32_t)i) continue;
             if (r->need <= sl.cap || total - sl.cap + r->need <= budget) {
                 if (r->need > sl.cap) sl.cap = r->need;
                 pending.erase(pending.begin() + (long)q);
@@ -217,7 +219,7 @@ int ldsc_server_create(int device, uint32_t n_slots, uint64_t device_budget, lds
     return LDSC_OK;
 }
 
-int ldsc_server_submit(ldsc_server* srv, const ldsc_job* job, uint64_t* ticket) {
+static int submit_pinned(ldsc_server* srv, const ldsc_job* job, int32_t pin, uint64_t* ticket) {
     if (!srv || !job || !ticket) return LDSC_E_INVALID;
     if (job->kind != LDSC_JOB_L2 && job->kind != LDSC_JOB_H2 && job->kind != LDSC_JOB_RG &&
         job->kind != LDSC_JOB_H2P)
@@ -252,12 +254,28 @@ int ldsc_server_submit(ldsc_server* srv, const ldsc_job* job, uint64_t* ticket) 
         return LDSC_E_NOMEM;
     }
     r->ticket = srv->next_ticket++;
+    r->pin = pin;
     r->t_submit = Clock::now();
     srv->jobs[r->ticket] = r;
     srv->pending.push_back(r);
     srv->submitted++;
     *ticket = r->ticket;
     srv->cv_work.notify_all();
+    return LDSC_OK;
+}
+
+int ldsc_server_submit(ldsc_server* srv, const ldsc_job* job, uint64_t* ticket) {
+    return submit_pinned(srv, job, -1, ticket);
+}
+
+int ldsc_server_prewarm(ldsc_server* srv, const ldsc_job* job) {
+    if (!srv || !job) return LDSC_E_INVALID;
+    for (uint32_t i = 0; i < (uint32_t)srv->slots.size(); i++) {
+        uint64_t t = 0;
+        int rc = submit_pinned(srv, job, (int32_t)i, &t);
+        if (rc == LDSC_OK) rc = ldsc_server_wait(srv, t, nullptr);
+        if (rc != LDSC_OK) return rc;
+    }
     return LDSC_OK;
 }
 

@@ -68,7 +68,23 @@ class Server:
         except Exception:
             pass
 
+    def prewarm(self, submit_fn, *args, **kw) -> None:
+        """Run one job on every slot, one after another (ldsc_server_prewarm):
+        ``srv.prewarm(srv.submit_l2, panel, snps, mode, ...)``.  Each slot's
+        workspace is then sized for that job, so later jobs no larger than it
+        allocate no device memory while others run."""
+        self._warm = True
+        try:
+            submit_fn(*args, **kw)
+        finally:
+            self._warm = False
+
     def _submit(self, job: L.Job, keep: dict) -> int:
+        if getattr(self, "_warm", False):
+            rc = self.lib.ldsc_server_prewarm(self.h, C.byref(job))
+            if rc != L.LDSC_OK:
+                raise LdscError(rc, "prewarm job failed")
+            return 0
         t = C.c_uint64()
         rc = self.lib.ldsc_server_submit(self.h, C.byref(job), C.byref(t))
         if rc != L.LDSC_OK:

@@ -126,6 +126,35 @@ def test_jobs_alone_equal_jobs_in_the_mix(ctx, resident):
         assert st["graph_launches"] > 0   # the regression pipelines replayed as graphs
 
 
+def test_prewarm_runs_the_job_on_every_slot(ctx, resident):
+    """ldsc_server_prewarm runs one job on each slot in turn (so every slot's
+    workspace is sized for it before serving starts); its output is the job's
+    own, and jobs submitted afterwards run as usual."""
+    from ldsc_b200.api import WindowMode, run_l2
+    from ldsc_b200.serve import Server
+    spec, panel, snps = resident
+    wm = WindowMode.Cm(1.0)
+    reg = _region(snps, 20000, 40000)
+    want = run_l2(ctx, reg, panel, wm, 200, snp_level_masking=True, precision="int8", yes_really=True)[0]
+    with Server(0, n_slots=3) as srv:
+        got = {}
+        orig = srv._submit
+
+        def keep(job, k):   # capture the prewarm job's output arrays
+            got.update(k)
+            return orig(job, k)
+
+        srv._submit = keep
+        srv.prewarm(srv.submit_l2, panel, reg, wm, 200, row_begin=20000, snp_level_masking=True)
+        srv._submit = orig
+        st = srv.stats()
+        assert st["completed"] == 3 and st["submitted"] == 3
+        np.testing.assert_array_equal(got["l2"], want)
+        t = srv.submit_l2(panel, _region(snps, 25000, 30000), wm, 200, row_begin=25000, snp_level_masking=True)
+        srv.wait(t)
+        assert srv.stats()["completed"] == 4
+
+
 def test_admission_by_device_budget(ctx, resident):
     """A budget that holds one large job at a time: every job still runs,
     the slots' workspace stays within the budget, and a job larger than the
