@@ -1614,11 +1614,11 @@ extern "C" int ldsc_h2_batch(ldsc_ctx* ctx, const ldsc_h2_args* a, ldsc_h2_resul
         }
         if (e2 != cudaSuccess || !a->want_lambda_gc) return e2;
         // median (src/h2.rs:394-414): middle order statistic, mean of the two for even n
-        e2 = launch_select(ctx->rg_jobs.as<RegJob>(), n, n / 2, ctx->rg_sel.as<double>(), T, gs);
-        if (e2 != cudaSuccess || n % 2) return e2;
-        return launch_select(ctx->rg_jobs.as<RegJob>(), n, n / 2 - 1, ctx->rg_sel.as<double>() + T, T, gs);
+        // (rank n/2 in sel[0, T), rank n/2 - 1 in sel[T, 2T) for even n)
+        return launch_select_mid(ctx->rg_jobs.as<RegJob>(), n, n % 2 ? n / 2 : n / 2 - 1, n / 2,
+                                 ctx->rg_sel.as<double>() + T, ctx->rg_sel.as<double>(), T, gs);
     }));
-    ctx->kernels += (two ? 19 : 8) + (a->want_lambda_gc ? (n % 2 == 0 ? 2 : 1) : 0);
+    ctx->kernels += (two ? 19 : 8) + (a->want_lambda_gc ? 1 : 0);
     std::vector<RegOut> outs(T);
     std::vector<double> sel(2 * T, NAN);
     std::vector<int32_t> n1(two ? T : 0);

@@ -6,9 +6,9 @@
 //   gencov_weights / run_hsq_ldsc / run_gencov_ldsc           (src/regressions.rs:1612-2052)
 // for the one-LD-score-column case (K = 1), many traits at once.
 //
-// Every per-SNP pass is one kernel over (jackknife block, job): a CTA sums
+// Every per-SNP pass is one kernel over (jackknife block, job): a warp sums
 // its block's contributions in f64, and per-job kernels combine the blocks in
-// block order, so results do not depend on scheduling.  The weighted least
+// a fixed order, so results do not depend on scheduling.  The weighted least
 // squares uses the 2 x 2 normal equations of the reference's weighted design
 // (the reference solves the same system by QR); the weights' global scale
 // 1/sum(w) cancels in every solve.
@@ -38,28 +38,45 @@ __device__ __forceinline__ double job_nx(const RegJob& jb, uint64_t i) {
     return jb.kind == REG_HSQ ? job_n1(jb, i) : sqrt(job_n1(jb, i) * job_n2(jb, i));
 }
 
+// Per-job constants of the weights, formed once per pass.
+struct WeightConsts {
+    double inv_nbar;  // 1 / nbar
+    double hm;        // REG_HSQ: clamp(hsq, 0, 1) / M
+    double h1m, h2m;  // REG_GENCOV: clamp(h1, 0, 1) / M, clamp(h2, 0, 1) / M
+    double sm;        // REG_GENCOV: rho_g / M
+};
+
+__device__ __forceinline__ WeightConsts weight_consts(const RegState& st, double m) {
+    WeightConsts k;
+    k.inv_nbar = 1.0 / st.nbar;
+    k.hm = fmin(fmax(st.slope, 0.0), 1.0) / m;
+    k.h1m = fmin(fmax(st.h1, 0.0), 1.0) / m;
+    k.h2m = fmin(fmax(st.h2, 0.0), 1.0) / m;
+    k.sm = st.slope / m;
+    return k;
+}
+
 // Regression weight of SNP i under the job's current parameters (the square
 // of the reference's w): ldsc_weights (src/h2.rs:185-206) or gencov_weights
-// (src/regressions.rs:1612-1645).
-__device__ __forceinline__ double job_weight(const RegJob& jb, const RegState& st, double ld_raw, double wld_raw,
-                                             uint64_t i, double m) {
-    const double oc = 1.0 / fmax(wld_raw, 1.0);
+// (src/regressions.rs:1612-1645).  The reference's two reciprocals (of the
+// heteroskedasticity term and of the overcounting LD score) are taken as one.
+__device__ __forceinline__ double job_weight(const RegJob& jb, const RegState& st, const WeightConsts& k,
+                                             double ld_raw, double wld_raw, uint64_t i) {
+    const double ocd = fmax(wld_raw, 1.0);
     if (jb.kind == REG_HSQ) {
         // step 1 of --two-step re-weights with the regressor in place of the LD
         // score (src/h2.rs:347-351: ldsc_weights(x1_col0, ...))
-        const double ld = jb.ld_from_x && st.n_updates > 0 ? fmax(job_n1(jb, i) * ld_raw / st.nbar, 1.0) : fmax(ld_raw, 1.0);
-        const double hsq = fmin(fmax(st.slope, 0.0), 1.0);
-        const double c = hsq * job_n1(jb, i) / m;
-        const double t = st.intercept + c * ld;
-        return 1.0 / (2.0 * t * t) * oc;
+        const double n1 = job_n1(jb, i);
+        const double ld = jb.ld_from_x && st.n_updates > 0 ? fmax(n1 * ld_raw * k.inv_nbar, 1.0) : fmax(ld_raw, 1.0);
+        const double t = st.intercept + k.hm * n1 * ld;
+        return 1.0 / (2.0 * t * t * ocd);
     }
     const double ld = fmax(ld_raw, 1.0);
-    const double h1 = fmin(fmax(st.h1, 0.0), 1.0), h2 = fmin(fmax(st.h2, 0.0), 1.0);
     const double n1 = job_n1(jb, i), n2 = job_n2(jb, i);
-    const double a = n1 * h1 * ld / m + st.int_h1;
-    const double b = n2 * h2 * ld / m + st.int_h2;
-    const double c = sqrt(n1 * n2) * st.slope * ld / m + st.intercept;
-    return 1.0 / (a * b + c * c) * oc;
+    const double a = n1 * k.h1m * ld + st.int_h1;
+    const double b = n2 * k.h2m * ld + st.int_h2;
+    const double c = sqrt(n1 * n2) * k.sm * ld + st.intercept;
+    return 1.0 / ((a * b + c * c) * ocd);
 }
 
 template <typename T>
@@ -84,42 +101,66 @@ __device__ __forceinline__ uint64_t sep(uint64_t n, int nb, int b) {
 // Per (jackknife block, job) sums.  MODE 0: sum y, sum ld*Nx, sum Nx.
 // MODE 1: with w = job weight and x0 = Nx*ld/nbar:
 //   sum w x0^2, sum w x0, sum w, sum w x0 y, sum w y.
+// One warp per (block, job), RJ jobs of the same block per CTA (their LD
+// scores are the same rows, read once into L1); each lane sums every 32nd SNP
+// of the block, RU loads in flight, then a warp reduction.  No block
+// barriers, and the order of the sums depends only on the block's bounds.
+constexpr int RJ = 8;  // jobs per CTA
+constexpr int RU = 4;  // SNPs per lane in flight
+
 template <int MODE>
-__global__ void __launch_bounds__(NT) k_reg_sums(const RegJob* __restrict__ jobs, const RegState* __restrict__ states,
-                                                 const double* __restrict__ ld, const double* __restrict__ wld,
-                                                 uint64_t n, int nb, double m, double* __restrict__ part) {
-    __shared__ double red[NT / 32];
-    const int b = blockIdx.x, j = blockIdx.y;
+__device__ __forceinline__ void reg_accum(const RegJob& jb, const RegState& st, const WeightConsts& k,
+                                          const double* __restrict__ ld, const double* __restrict__ wld, uint64_t i,
+                                          double* s) {
+    const double y = job_y(jb, i);
+    if (MODE == 1 && jb.use_mask && !(y < jb.mask_max)) return;
+    const double l = ld[i];
+    const double nx = job_nx(jb, i);
+    if (MODE == 0) {
+        s[0] += y;
+        s[1] += l * nx;
+        s[2] += nx;
+    } else {
+        const double w = job_weight(jb, st, k, l, wld[i], i);
+        const double x0 = nx * l * k.inv_nbar;
+        s[0] += w * x0 * x0;
+        s[1] += w * x0;
+        s[2] += w;
+        s[3] += w * x0 * y;
+        s[4] += w * y;
+    }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(RJ * 32) k_reg_sums(const RegJob* __restrict__ jobs,
+                                                      const RegState* __restrict__ states,
+                                                      const double* __restrict__ ld, const double* __restrict__ wld,
+                                                      uint64_t n, int nb, double m, int njobs,
+                                                      double* __restrict__ part) {
+    const int lane = threadIdx.x & 31;
+    const int b = blockIdx.x, j = blockIdx.y * RJ + (threadIdx.x >> 5);
+    if (j >= njobs) return;
     const RegJob jb = jobs[j];
     const RegState st = states[j];
     const uint64_t lo = jb.seps ? (uint64_t)jb.seps[b] : sep(n, nb, b);
     const uint64_t hi = jb.seps ? (uint64_t)jb.seps[b + 1] : sep(n, nb, b + 1);
+    const WeightConsts k = weight_consts(st, m);
     double s[5] = {0, 0, 0, 0, 0};
-    for (uint64_t i = lo + threadIdx.x; i < hi; i += NT) {
-        const double y = job_y(jb, i);
-        if (MODE == 1 && jb.use_mask && !(y < jb.mask_max)) continue;
-        const double l = ld[i];
-        const double nx = job_nx(jb, i);
-        if (MODE == 0) {
-            s[0] += y;
-            s[1] += l * nx;
-            s[2] += nx;
-        } else {
-            const double w = job_weight(jb, st, l, wld[i], i, m);
-            const double x0 = nx * l / st.nbar;
-            s[0] += w * x0 * x0;
-            s[1] += w * x0;
-            s[2] += w;
-            s[3] += w * x0 * y;
-            s[4] += w * y;
-        }
-    }
-    double* out = part + ((size_t)j * nb + b) * 5;
+    uint64_t i = lo + lane;
+    for (; i + 32 * (RU - 1) < hi; i += 32 * RU) {
 #pragma unroll
-    for (int q = 0; q < 5; q++) {
-        if (MODE == 0 && q >= 3) break;
-        const double t = block_sum(s[q], red);
-        if (threadIdx.x == 0) out[q] = t;
+        for (int u = 0; u < RU; u++) reg_accum<MODE>(jb, st, k, ld, wld, i + 32 * u, s);
+    }
+    for (; i < hi; i += 32) reg_accum<MODE>(jb, st, k, ld, wld, i, s);
+    constexpr int NQ = MODE == 0 ? 3 : 5;
+#pragma unroll
+    for (int q = 0; q < NQ; q++)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s[q] += __shfl_xor_sync(0xFFFFFFFFu, s[q], o);
+    if (lane == 0) {
+        double* out = part + ((size_t)j * nb + b) * 5;
+#pragma unroll
+        for (int q = 0; q < NQ; q++) out[q] = s[q];
     }
 }
 
@@ -142,13 +183,22 @@ template <int MODE>
 __global__ void k_reg_update(const RegJob* __restrict__ jobs, RegState* __restrict__ states,
                              const RegOut* __restrict__ ref_outs, const double* __restrict__ part, uint64_t n, int nb,
                              double m, int njobs) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    // one warp per job: lane l sums blocks l, l + 32, ..., then a fixed-order
+    // warp reduction
+    const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
     if (j >= njobs) return;
+    constexpr int NQ = MODE == 0 ? 3 : 5;
+    double S[5] = {0, 0, 0, 0, 0};
+    for (int b = lane; b < nb; b += 32)
+#pragma unroll
+        for (int q = 0; q < NQ; q++) S[q] += part[((size_t)j * nb + b) * 5 + q];
+#pragma unroll
+    for (int q = 0; q < NQ; q++)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) S[q] += __shfl_xor_sync(0xFFFFFFFFu, S[q], o);
+    if (lane) return;
     const RegJob jb = jobs[j];
     RegState st = states[j];
-    double S[5] = {0, 0, 0, 0, 0};
-    for (int b = 0; b < nb; b++)
-        for (int q = 0; q < (MODE == 0 ? 3 : 5); q++) S[q] += part[((size_t)j * nb + b) * 5 + q];
     if (MODE == 0) {
         const double nn = (double)n;
         st.mean_y = S[0] / nn;
@@ -313,8 +363,16 @@ __global__ void __launch_bounds__(NT) k_rg_finish(const RgPairIdx* __restrict__ 
     }
 }
 
-// Exact order statistic of each job's y (radix select over the order-
-// preserving 64-bit keys of the doubles), 8 bits per pass; one CTA per job.
+// The two middle order statistics of each job's y (ranks ra <= rb, rb - ra
+// <= 1), exactly: a radix select over the order-preserving 64-bit keys of the
+// doubles, 11 bits per digit, one CTA per job.  Each digit is one sweep over
+// the job's y; the sweep histograms the keys that share the prefix fixed so
+// far.  Once that prefix holds at most SEL_CAP keys, one more sweep gathers
+// them into shared memory and they are ranked there.  If the two ranks fall
+// in different buckets of a digit, ra is the largest key of its bucket and rb
+// the smallest of its own, found by one more sweep.  On LD-score chi2 values
+// two digits (sign and exponent, then the mantissa's top bits) usually leave
+// about a hundred keys, so the select reads each y three times.
 __device__ __forceinline__ uint64_t okey(double v) {
     const uint64_t b = (uint64_t)__double_as_longlong(v);
     return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
@@ -324,37 +382,152 @@ __device__ __forceinline__ double okey_value(uint64_t k) {
     return __longlong_as_double((long long)b);
 }
 
-__global__ void __launch_bounds__(NT) k_select(const RegJob* __restrict__ jobs, uint64_t n, uint64_t rank,
-                                               double* __restrict__ out) {
-    __shared__ uint32_t hist[256];
-    __shared__ uint64_t s_prefix, s_rank;
-    const RegJob jb = jobs[blockIdx.x];
-    uint64_t prefix = 0, r = rank;
-    for (int shift = 56; shift >= 0; shift -= 8) {
-        for (int i = threadIdx.x; i < 256; i += NT) hist[i] = 0;
-        __syncthreads();
-        const uint64_t pmask = shift == 56 ? 0ull : (~0ull << (shift + 8));
-        for (uint64_t i = threadIdx.x; i < n; i += NT) {
-            const uint64_t k = okey(job_y(jb, i));
-            if ((k & pmask) == prefix) atomicAdd(&hist[(k >> shift) & 0xFF], 1u);
+constexpr int SEL_T = 512;
+constexpr int SEL_W = SEL_T / 32;
+constexpr int SEL_BITS = 11;
+constexpr int SEL_BINS = 1 << SEL_BITS;
+constexpr int SEL_CAP = 2048;  // keys ranked in shared memory
+constexpr int SEL_U = 4;       // loads in flight per thread
+
+// Calls f(key, valid) for every y of the job; the trip count is the same in
+// every lane of a warp, so f may use warp-collective operations.
+template <class F>
+__device__ __forceinline__ void sel_sweep(const RegJob& jb, uint64_t n, F f) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (uint64_t i0 = (uint64_t)warp * 32 * SEL_U; i0 < n; i0 += (uint64_t)SEL_T * SEL_U) {
+        uint64_t k[SEL_U];
+        bool v[SEL_U];
+#pragma unroll
+        for (int u = 0; u < SEL_U; u++) {
+            const uint64_t i = i0 + (uint64_t)u * 32 + lane;
+            v[u] = i < n;
+            k[u] = v[u] ? okey(job_y(jb, i)) : 0ull;
         }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            uint64_t acc = 0;
-            int d = 0;
-            for (; d < 256; d++) {
-                if (acc + hist[d] > r) break;
-                acc += hist[d];
-            }
-            s_prefix = prefix | ((uint64_t)d << shift);
-            s_rank = r - acc;
-        }
-        __syncthreads();
-        prefix = s_prefix;
-        r = s_rank;
-        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < SEL_U; u++) f(k[u], v[u]);
     }
-    if (threadIdx.x == 0) out[blockIdx.x] = okey_value(prefix);
+}
+
+__global__ void __launch_bounds__(SEL_T) k_select_mid(const RegJob* __restrict__ jobs, uint64_t n, uint64_t ra,
+                                                      uint64_t rb, double* __restrict__ out_a,
+                                                      double* __restrict__ out_b) {
+    __shared__ uint32_t hist[SEL_BINS];
+    __shared__ uint64_t cand[SEL_CAP];
+    __shared__ uint32_t wsum[SEL_W];
+    __shared__ uint32_t s_da, s_db, s_acc_a, s_acc_b, s_cnt;
+    __shared__ unsigned long long s_ka, s_kb;
+    const RegJob jb = jobs[blockIdx.x];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint64_t prefix = 0, pmask = 0, cnt = n;
+    uint64_t qa = ra, qb = rb;  // ranks among the keys that match the prefix
+    int top = 64;               // bits below the prefix
+    for (;;) {
+        if (cnt <= SEL_CAP) {
+            // gather the prefix's keys and rank them in shared memory
+            if (threadIdx.x == 0) s_cnt = 0;
+            __syncthreads();
+            sel_sweep(jb, n, [&](uint64_t k, bool v) {
+                const bool take = v && (k & pmask) == prefix;
+                const unsigned m = __ballot_sync(0xFFFFFFFFu, take);
+                uint32_t base = 0;
+                if (lane == 0 && m) base = atomicAdd(&s_cnt, (uint32_t)__popc(m));
+                base = __shfl_sync(0xFFFFFFFFu, base, 0);
+                if (take) cand[base + __popc(m & ((1u << lane) - 1u))] = k;
+            });
+            __syncthreads();
+            const uint32_t c = s_cnt;
+            for (uint32_t i = threadIdx.x; i < c; i += SEL_T) {
+                const uint64_t ki = cand[i];
+                uint32_t r = 0;
+                for (uint32_t j = 0; j < c; j++) {
+                    const uint64_t kj = cand[j];
+                    r += (kj < ki || (kj == ki && j < i)) ? 1u : 0u;
+                }
+                if (r == qa) s_ka = ki;
+                if (r == qb) s_kb = ki;
+            }
+            __syncthreads();
+            break;
+        }
+        if (top == 0) {  // every key left equals the prefix
+            if (threadIdx.x == 0) s_ka = s_kb = prefix;
+            __syncthreads();
+            break;
+        }
+        const int width = top < SEL_BITS ? top : SEL_BITS;
+        const int shift = top - width;
+        const uint32_t dmask = (1u << width) - 1u;
+        for (int i = threadIdx.x; i < SEL_BINS; i += SEL_T) hist[i] = 0;
+        __syncthreads();
+        sel_sweep(jb, n, [&](uint64_t k, bool v) {
+            const bool take = v && (k & pmask) == prefix;
+            const uint32_t bin = take ? (uint32_t)(k >> shift) & dmask : 0xFFFFFFFFu;
+            const unsigned peers = __match_any_sync(0xFFFFFFFFu, bin);
+            if (take && lane == __ffs(peers) - 1) atomicAdd(&hist[bin], (uint32_t)__popc(peers));
+        });
+        __syncthreads();
+        // bins of this thread: [4 t, 4 t + 4); exclusive block scan of their sums
+        constexpr int PER = SEL_BINS / SEL_T;
+        uint32_t c[PER], tsum = 0;
+#pragma unroll
+        for (int q = 0; q < PER; q++) {
+            c[q] = hist[threadIdx.x * PER + q];
+            tsum += c[q];
+        }
+        uint32_t incl = tsum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t u = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= o) incl += u;
+        }
+        if (lane == 31) wsum[warp] = incl;
+        __syncthreads();
+        uint32_t acc = incl - tsum;
+        for (int w = 0; w < warp; w++) acc += wsum[w];
+#pragma unroll
+        for (int q = 0; q < PER; q++) {
+            if (qa >= acc && qa < acc + c[q]) {
+                s_da = threadIdx.x * PER + q;
+                s_acc_a = acc;
+            }
+            if (qb >= acc && qb < acc + c[q]) {
+                s_db = threadIdx.x * PER + q;
+                s_acc_b = acc;
+            }
+            acc += c[q];
+        }
+        __syncthreads();
+        const uint32_t da = s_da, db = s_db;
+        const uint64_t dm = (uint64_t)dmask << shift;
+        if (da == db) {
+            prefix |= (uint64_t)da << shift;
+            pmask |= dm;
+            qa -= s_acc_a;
+            qb -= s_acc_b;
+            cnt = hist[da];
+            top = shift;
+            __syncthreads();  // hist and the s_ values are rewritten by the next digit
+            continue;
+        }
+        // ra is the largest key of bucket da, rb the smallest of bucket db
+        const uint64_t pa = prefix | ((uint64_t)da << shift), pb = prefix | ((uint64_t)db << shift);
+        const uint64_t nm = pmask | dm;
+        if (threadIdx.x == 0) {
+            s_ka = 0ull;
+            s_kb = ~0ull;
+        }
+        __syncthreads();
+        sel_sweep(jb, n, [&](uint64_t k, bool v) {
+            if (v && (k & nm) == pa) atomicMax(&s_ka, (unsigned long long)k);
+            if (v && (k & nm) == pb) atomicMin(&s_kb, (unsigned long long)k);
+        });
+        __syncthreads();
+        break;
+    }
+    if (threadIdx.x == 0) {
+        out_a[blockIdx.x] = okey_value(s_ka);
+        out_b[blockIdx.x] = okey_value(s_kb);
+    }
 }
 
 // ---- --two-step ----
@@ -516,15 +689,15 @@ cudaError_t launch_regressions(const RegJob* jobs, RegState* states, RegOut* out
                                double* part, double* tot_delete, const double* ld, const double* wld, uint64_t n,
                                int nb, double m, int njobs, cudaStream_t s, double* dv) {
     if (njobs <= 0) return cudaSuccess;
-    const dim3 grid(nb, njobs);
-    const int ub = (njobs + 127) / 128;
-    k_reg_sums<0><<<grid, NT, 0, s>>>(jobs, states, ld, wld, n, nb, m, part);
+    const dim3 grid(nb, (njobs + RJ - 1) / RJ);
+    const int ub = (njobs + 3) / 4;  // k_reg_update: four warps (jobs) per CTA
+    k_reg_sums<0><<<grid, RJ * 32, 0, s>>>(jobs, states, ld, wld, n, nb, m, njobs, part);
     k_reg_update<0><<<ub, 128, 0, s>>>(jobs, states, ref_outs, part, n, nb, m, njobs);
     for (int it = 0; it < 2; it++) {  // irwls_ldsc: two re-weightings
-        k_reg_sums<1><<<grid, NT, 0, s>>>(jobs, states, ld, wld, n, nb, m, part);
+        k_reg_sums<1><<<grid, RJ * 32, 0, s>>>(jobs, states, ld, wld, n, nb, m, njobs, part);
         k_reg_update<1><<<ub, 128, 0, s>>>(jobs, states, ref_outs, part, n, nb, m, njobs);
     }
-    k_reg_sums<1><<<grid, NT, 0, s>>>(jobs, states, ld, wld, n, nb, m, part);
+    k_reg_sums<1><<<grid, RJ * 32, 0, s>>>(jobs, states, ld, wld, n, nb, m, njobs, part);
     k_reg_jackknife<<<njobs, NT, 0, s>>>(jobs, states, outs, part, nb, m, tot_delete, dv);
     return cudaGetLastError();
 }
@@ -536,9 +709,10 @@ cudaError_t launch_rg_finish(const RgPairIdx* pairs, const RegOut* outs, const d
     return cudaGetLastError();
 }
 
-cudaError_t launch_select(const RegJob* jobs, uint64_t n, uint64_t rank, double* out, int njobs, cudaStream_t s) {
-    if (njobs <= 0 || n == 0) return cudaSuccess;
-    k_select<<<njobs, NT, 0, s>>>(jobs, n, rank, out);
+cudaError_t launch_select_mid(const RegJob* jobs, uint64_t n, uint64_t ra, uint64_t rb, double* out_a, double* out_b,
+                              int njobs, cudaStream_t s) {
+    if (njobs <= 0 || n == 0 || ra > rb || rb - ra > 1 || rb >= n) return cudaErrorInvalidValue;
+    k_select_mid<<<njobs, SEL_T, 0, s>>>(jobs, n, ra, rb, out_a, out_b);
     return cudaGetLastError();
 }
 
@@ -549,7 +723,7 @@ cudaError_t preload_regress() {
     if (e == cudaSuccess) e = preload_kernel(k_reg_update<1>);
     if (e == cudaSuccess) e = preload_kernel(k_reg_jackknife);
     if (e == cudaSuccess) e = preload_kernel(k_rg_finish);
-    if (e == cudaSuccess) e = preload_kernel(k_select);
+    if (e == cudaSuccess) e = preload_kernel(k_select_mid);
     if (e == cudaSuccess) e = preload_kernel(k_ts_count);
     if (e == cudaSuccess) e = preload_kernel(k_ts_seps);
     if (e == cudaSuccess) e = preload_kernel(k_ts_combine);

@@ -84,8 +84,10 @@ cudaError_t launch_twostep_combine(const RegOut* out1, const RegOut* out2, const
 cudaError_t launch_rg_finish(const RgPairIdx* pairs, const RegOut* outs, const double* tot_delete, int nb,
                              RgOut* res, int npairs, cudaStream_t s);
 
-// k-th smallest y of each job (exact), out[job].
-cudaError_t launch_select(const RegJob* jobs, uint64_t n, uint64_t rank, double* out, int njobs, cudaStream_t s);
+// The ra-th and rb-th smallest y of each job (exact; ra <= rb <= ra + 1),
+// out_a[job] and out_b[job].
+cudaError_t launch_select_mid(const RegJob* jobs, uint64_t n, uint64_t ra, uint64_t rb, double* out_a, double* out_b,
+                              int njobs, cudaStream_t s);
 
 // ---- partitioned h2 (fit_h2_partitioned, src/regressions.rs:1121-1226) ----
 

@@ -55,6 +55,41 @@ def test_h2_batch_scalar_n(ctx, m):
         _check_h2(got[t], R.run_h2(chi2[t], ld, wld, n[t], big_m, 200))
 
 
+def _lgc_case(kind, rng):
+    if kind == "small_odd":          # fewer keys than the shared-memory capacity
+        return rng.chisquare(1, 7)
+    if kind == "at_capacity":
+        return rng.chisquare(1, 2048)
+    if kind == "above_capacity":
+        return rng.chisquare(1, 2050)
+    if kind == "split_octaves":      # the middle ranks fall in different buckets of the first digit
+        return rng.permutation(np.concatenate([rng.uniform(1.0, 2.0, 5000), rng.uniform(4.0, 8.0, 5000)]))
+    if kind == "all_equal":          # the prefix never narrows: every digit is taken
+        return np.full(10_000, 3.0)
+    if kind == "few_values":         # ties far above the capacity, odd count
+        return rng.integers(0, 6, 50_001).astype(np.float64)
+    if kind == "signed_zeros":       # y enters as given: negative values, -0.0 and 0.0 order exactly
+        return rng.choice(np.array([-1.5, -0.0, 0.0, 2.5]), 20_000)
+    raise ValueError(kind)
+
+
+@pytest.mark.parametrize("kind", ["small_odd", "at_capacity", "above_capacity", "split_octaves", "all_equal",
+                                  "few_values", "signed_zeros"])
+def test_lambda_gc_median_edge_cases(ctx, kind):
+    """lambda_GC = median(chi2) / 0.4549 (src/h2.rs:394-414) is an exact order
+    statistic: equal to numpy's median on ties, split buckets, capacity edges
+    and signed zeros."""
+    from ldsc_b200.api import h2_batch
+    rng = np.random.default_rng(sum(map(ord, kind)))
+    chi2 = _lgc_case(kind, rng)
+    m = len(chi2)
+    ld, wld = _ld(m, 21)
+    got = h2_batch(ctx, np.stack([chi2, chi2[::-1].copy()]), [1e5, 1e5], ld, wld, 1e6, min(5, m - 1))
+    want = np.median(chi2) / 0.4549
+    for t in range(2):
+        assert got[t]["lambda_gc"] == want, (kind, t, got[t]["lambda_gc"], want)
+
+
 def test_h2_batch_per_snp_n_and_fixed_intercept(ctx):
     from ldsc_b200.api import h2_batch
     from ldsc_b200.synth import gwas_traits
