@@ -481,6 +481,48 @@ def _partitioned_h2(ctx, stream, d_l2, annot, args, n_traits=8, n_blocks=200):
                     "annotations); the Gram rate is a lower bound (call time includes the solves)"}
 
 
+def run_regressions_workload(args, seed: int = 7):
+    """Batched regressions on device-resident inputs, as the serving mix runs
+    them: h2 over 1,000 synthetic traits x 200,000 regression SNPs (200-block
+    jackknife; with and without lambda GC) and rg over 200 trait pairs, each
+    through one server slot.  Prints one JSON line with the median run time
+    of each (the first call of each kind, which captures its graph, is left
+    out)."""
+    import torch
+    from ldsc_b200.serve import Server
+    T, P, n_reg, M = 1000, 200, 200_000, 1_200_000
+    dev = torch.device("cuda")
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    f64 = torch.float64
+    ld = 1 + 30 * torch.rand(n_reg, generator=g, device=dev, dtype=f64)
+    h2 = 0.05 + 0.45 * torch.rand(T, generator=g, device=dev, dtype=f64)
+    n_t = torch.exp(np.log(1e4) + (np.log(5e5) - np.log(1e4)) * torch.rand(T, generator=g, device=dev, dtype=f64))
+    z = torch.sqrt(n_t[:, None] * h2[:, None] * ld[None, :] / M) * torch.randn(T, n_reg, generator=g, device=dev,
+                                                                               dtype=f64)
+    z += torch.randn(T, n_reg, generator=g, device=dev, dtype=f64)
+    chi2 = (z * z).contiguous()
+    del z
+    z1 = torch.randn(P, n_reg, generator=g, device=dev, dtype=f64)
+    z2 = 0.5 * z1 + torch.randn(P, n_reg, generator=g, device=dev, dtype=f64)
+    n1 = torch.full((P,), 1e5, device=dev, dtype=f64)
+    torch.cuda.synchronize()
+    srv = Server(torch.cuda.current_device(), n_slots=1)
+    out = {"workload": "regressions", "metric": "run time per batched call (ms, median)",
+           "config": {"h2": f"{T} traits x {n_reg} SNPs, 200 blocks", "rg": f"{P} pairs x {n_reg} SNPs, 200 blocks",
+                      "inputs": "device-resident (chi2 / z, LD scores, N)"}}
+    try:
+        for name, fn in [("h2_lambda_gc", lambda: srv.submit_h2(chi2, n_t, ld, ld, float(M), 200)),
+                         ("h2", lambda: srv.submit_h2(chi2, n_t, ld, ld, float(M), 200, lambda_gc=False)),
+                         ("rg", lambda: srv.submit_rg(z1, z2, n1, n1, ld, ld, float(M), 200))]:
+            runs = [srv.wait(fn())[1].run_ms for _ in range(args.warmup + args.steps)]
+            out[name + "_ms"] = float(np.median(runs[args.warmup:]))
+    finally:
+        srv.close()
+    out["h2_bytes_per_weighted_pass"] = T * n_reg * 8
+    return out
+
+
 def run_serving_workload(args, ctx, duration_s: float, rates, seed: int = 7):
     """Serving mix on a resident N=20,000 x M=1,200,000 panel (22
     chromosomes, 3,500 cM).  Poisson arrivals at each rate (requests/s) for
@@ -683,7 +725,8 @@ def main():
     ap.add_argument("--weak", action="store_true",
                     help="N > 1: every rank runs its own panel (seed + rank) instead of a shard of one panel")
     ap.add_argument("--workload", default="biobank",
-                    choices=["biobank", "profile", "sketch", "partitioned", "partitioned-h2", "serving"])
+                    choices=["biobank", "profile", "sketch", "partitioned", "partitioned-h2", "serving",
+                             "regressions"])
     ap.add_argument("--h2p-snps", type=int, default=500_000, help="partitioned-h2: regression SNPs")
     ap.add_argument("--h2p-annot", type=int, default=97, help="partitioned-h2: LD-score columns K")
     ap.add_argument("--h2p-traits", type=int, default=8, help="partitioned-h2: traits per call")
@@ -738,6 +781,9 @@ def main():
         return
     if args.workload == "partitioned-h2":
         run_partitioned_h2_workload(args, ctx, stream)
+        return
+    if args.workload == "regressions":
+        print(json.dumps(run_regressions_workload(args)), flush=True)
         return
     if args.workload == "serving":
         rates = [float(x) for x in args.serve_rates.split(",")] if args.serve_rates else [args.serve_rate]

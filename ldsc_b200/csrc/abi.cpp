@@ -1925,7 +1925,7 @@ extern "C" int ldsc_rg_batch(ldsc_ctx* ctx, const ldsc_rg_args* a, ldsc_rg_resul
         if (e2 != cudaSuccess) return e2;
         e2 = launch_regressions(dj + 2 * P, dst + 2 * P, dout + 2 * P, dout,
                                 ctx->rg_part.as<double>() + (size_t)2 * P * nb * 5, dtd + (size_t)2 * P * nb, d_ld,
-                                d_wld, n, nb, a->m_snps, P, gs);
+                                d_wld, n, nb, a->m_snps, P, gs, nullptr, REG_GENCOV);
         if (e2 != cudaSuccess) return e2;
         return launch_rg_finish(ctx->rg_pairs.as<RgPairIdx>(), dout, dtd, nb, ctx->rg_res.as<RgOut>(), P, gs);
     }));

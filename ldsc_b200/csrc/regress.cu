@@ -34,8 +34,9 @@ __device__ __forceinline__ double job_y(const RegJob& jb, uint64_t i) {
 __device__ __forceinline__ double job_n1(const RegJob& jb, uint64_t i) { return jb.n1 ? jb.n1[i] : jb.n1s; }
 __device__ __forceinline__ double job_n2(const RegJob& jb, uint64_t i) { return jb.n2 ? jb.n2[i] : jb.n2s; }
 // sample size that scales the regressor: N (h2) or sqrt(N1 N2) (gencov)
+template <int KIND>
 __device__ __forceinline__ double job_nx(const RegJob& jb, uint64_t i) {
-    return jb.kind == REG_HSQ ? job_n1(jb, i) : sqrt(job_n1(jb, i) * job_n2(jb, i));
+    return KIND == REG_HSQ ? job_n1(jb, i) : sqrt(job_n1(jb, i) * job_n2(jb, i));
 }
 
 // Per-job constants of the weights, formed once per pass.
@@ -60,10 +61,11 @@ __device__ __forceinline__ WeightConsts weight_consts(const RegState& st, double
 // of the reference's w): ldsc_weights (src/h2.rs:185-206) or gencov_weights
 // (src/regressions.rs:1612-1645).  The reference's two reciprocals (of the
 // heteroskedasticity term and of the overcounting LD score) are taken as one.
+template <int KIND>
 __device__ __forceinline__ double job_weight(const RegJob& jb, const RegState& st, const WeightConsts& k,
                                              double ld_raw, double wld_raw, uint64_t i) {
     const double ocd = fmax(wld_raw, 1.0);
-    if (jb.kind == REG_HSQ) {
+    if (KIND == REG_HSQ) {
         // step 1 of --two-step re-weights with the regressor in place of the LD
         // score (src/h2.rs:347-351: ldsc_weights(x1_col0, ...))
         const double n1 = job_n1(jb, i);
@@ -106,22 +108,19 @@ __device__ __forceinline__ uint64_t sep(uint64_t n, int nb, int b) {
 // of the block, RU loads in flight, then a warp reduction.  No block
 // barriers, and the order of the sums depends only on the block's bounds.
 constexpr int RJ = 8;  // jobs per CTA
-constexpr int RU = 4;  // SNPs per lane in flight
+constexpr int RU = 4;  // SNPs per lane whose loads are issued together
 
-template <int MODE>
-__device__ __forceinline__ void reg_accum(const RegJob& jb, const RegState& st, const WeightConsts& k,
-                                          const double* __restrict__ ld, const double* __restrict__ wld, uint64_t i,
-                                          double* s) {
-    const double y = job_y(jb, i);
+template <int MODE, int KIND>
+__device__ __forceinline__ void reg_term(const RegJob& jb, const RegState& st, const WeightConsts& k, double y,
+                                         double l, double wl, uint64_t i, double* s) {
     if (MODE == 1 && jb.use_mask && !(y < jb.mask_max)) return;
-    const double l = ld[i];
-    const double nx = job_nx(jb, i);
+    const double nx = job_nx<KIND>(jb, i);
     if (MODE == 0) {
         s[0] += y;
         s[1] += l * nx;
         s[2] += nx;
     } else {
-        const double w = job_weight(jb, st, k, l, wld[i], i);
+        const double w = job_weight<KIND>(jb, st, k, l, wl, i);
         const double x0 = nx * l * k.inv_nbar;
         s[0] += w * x0 * x0;
         s[1] += w * x0;
@@ -131,7 +130,8 @@ __device__ __forceinline__ void reg_accum(const RegJob& jb, const RegState& st, 
     }
 }
 
-template <int MODE>
+// KIND: the kind of every job of the launch (a job of another kind gets NaN sums).
+template <int MODE, int KIND>
 __global__ void __launch_bounds__(RJ * 32) k_reg_sums(const RegJob* __restrict__ jobs,
                                                       const RegState* __restrict__ states,
                                                       const double* __restrict__ ld, const double* __restrict__ wld,
@@ -146,12 +146,25 @@ __global__ void __launch_bounds__(RJ * 32) k_reg_sums(const RegJob* __restrict__
     const uint64_t hi = jb.seps ? (uint64_t)jb.seps[b + 1] : sep(n, nb, b + 1);
     const WeightConsts k = weight_consts(st, m);
     double s[5] = {0, 0, 0, 0, 0};
-    uint64_t i = lo + lane;
-    for (; i + 32 * (RU - 1) < hi; i += 32 * RU) {
+    // lane l takes SNPs lo + l, lo + l + 32, ... in that order; RU of them per
+    // step have their loads in flight together
+    for (uint64_t i0 = lo + lane; i0 < hi; i0 += 32 * RU) {
+        double y[RU], l[RU], wl[RU];
 #pragma unroll
-        for (int u = 0; u < RU; u++) reg_accum<MODE>(jb, st, k, ld, wld, i + 32 * u, s);
+        for (int u = 0; u < RU; u++) {
+            const uint64_t i = i0 + 32 * (uint64_t)u;
+            const bool v = i < hi;
+            y[u] = v ? job_y(jb, i) : 0.0;
+            l[u] = v ? ld[i] : 0.0;
+            wl[u] = (MODE == 1 && v) ? wld[i] : 1.0;
+        }
+#pragma unroll
+        for (int u = 0; u < RU; u++)
+            if (i0 + 32 * (uint64_t)u < hi) reg_term<MODE, KIND>(jb, st, k, y[u], l[u], wl[u], i0 + 32 * (uint64_t)u, s);
     }
-    for (; i < hi; i += 32) reg_accum<MODE>(jb, st, k, ld, wld, i, s);
+    if (jb.kind != KIND)
+#pragma unroll
+        for (int q = 0; q < 5; q++) s[q] = NAN;
     constexpr int NQ = MODE == 0 ? 3 : 5;
 #pragma unroll
     for (int q = 0; q < NQ; q++)
@@ -382,7 +395,7 @@ __device__ __forceinline__ double okey_value(uint64_t k) {
     return __longlong_as_double((long long)b);
 }
 
-constexpr int SEL_T = 512;
+constexpr int SEL_T = 256;
 constexpr int SEL_W = SEL_T / 32;
 constexpr int SEL_BITS = 11;
 constexpr int SEL_BINS = 1 << SEL_BITS;
@@ -466,7 +479,7 @@ __global__ void __launch_bounds__(SEL_T) k_select_mid(const RegJob* __restrict__
             if (take && lane == __ffs(peers) - 1) atomicAdd(&hist[bin], (uint32_t)__popc(peers));
         });
         __syncthreads();
-        // bins of this thread: [4 t, 4 t + 4); exclusive block scan of their sums
+        // bins of this thread: [PER t, PER t + PER); exclusive block scan of their sums
         constexpr int PER = SEL_BINS / SEL_T;
         uint32_t c[PER], tsum = 0;
 #pragma unroll
@@ -687,17 +700,28 @@ cudaError_t launch_twostep_combine(const RegOut* out1, const RegOut* out2, const
 
 cudaError_t launch_regressions(const RegJob* jobs, RegState* states, RegOut* outs, const RegOut* ref_outs,
                                double* part, double* tot_delete, const double* ld, const double* wld, uint64_t n,
-                               int nb, double m, int njobs, cudaStream_t s, double* dv) {
+                               int nb, double m, int njobs, cudaStream_t s, double* dv, int kind) {
     if (njobs <= 0) return cudaSuccess;
+    if (kind != REG_HSQ && kind != REG_GENCOV) return cudaErrorInvalidValue;
     const dim3 grid(nb, (njobs + RJ - 1) / RJ);
     const int ub = (njobs + 3) / 4;  // k_reg_update: four warps (jobs) per CTA
-    k_reg_sums<0><<<grid, RJ * 32, 0, s>>>(jobs, states, ld, wld, n, nb, m, njobs, part);
+    auto sums = [&](int mode) {
+        if (mode == 0 && kind == REG_HSQ)
+            k_reg_sums<0, REG_HSQ><<<grid, RJ * 32, 0, s>>>(jobs, states, ld, wld, n, nb, m, njobs, part);
+        else if (mode == 0)
+            k_reg_sums<0, REG_GENCOV><<<grid, RJ * 32, 0, s>>>(jobs, states, ld, wld, n, nb, m, njobs, part);
+        else if (kind == REG_HSQ)
+            k_reg_sums<1, REG_HSQ><<<grid, RJ * 32, 0, s>>>(jobs, states, ld, wld, n, nb, m, njobs, part);
+        else
+            k_reg_sums<1, REG_GENCOV><<<grid, RJ * 32, 0, s>>>(jobs, states, ld, wld, n, nb, m, njobs, part);
+    };
+    sums(0);
     k_reg_update<0><<<ub, 128, 0, s>>>(jobs, states, ref_outs, part, n, nb, m, njobs);
     for (int it = 0; it < 2; it++) {  // irwls_ldsc: two re-weightings
-        k_reg_sums<1><<<grid, RJ * 32, 0, s>>>(jobs, states, ld, wld, n, nb, m, njobs, part);
+        sums(1);
         k_reg_update<1><<<ub, 128, 0, s>>>(jobs, states, ref_outs, part, n, nb, m, njobs);
     }
-    k_reg_sums<1><<<grid, RJ * 32, 0, s>>>(jobs, states, ld, wld, n, nb, m, njobs, part);
+    sums(1);
     k_reg_jackknife<<<njobs, NT, 0, s>>>(jobs, states, outs, part, nb, m, tot_delete, dv);
     return cudaGetLastError();
 }
@@ -717,8 +741,10 @@ cudaError_t launch_select_mid(const RegJob* jobs, uint64_t n, uint64_t ra, uint6
 }
 
 cudaError_t preload_regress() {
-    cudaError_t e = preload_kernel(k_reg_sums<0>);
-    if (e == cudaSuccess) e = preload_kernel(k_reg_sums<1>);
+    cudaError_t e = preload_kernel(k_reg_sums<0, REG_HSQ>);
+    if (e == cudaSuccess) e = preload_kernel(k_reg_sums<1, REG_HSQ>);
+    if (e == cudaSuccess) e = preload_kernel(k_reg_sums<0, REG_GENCOV>);
+    if (e == cudaSuccess) e = preload_kernel(k_reg_sums<1, REG_GENCOV>);
     if (e == cudaSuccess) e = preload_kernel(k_reg_update<0>);
     if (e == cudaSuccess) e = preload_kernel(k_reg_update<1>);
     if (e == cudaSuccess) e = preload_kernel(k_reg_jackknife);

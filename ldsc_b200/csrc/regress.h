@@ -58,14 +58,16 @@ struct RgOut {
     double mean_z1z2;
 };
 
-// Aggregate pass, two IRWLS updates and the block jackknife for all jobs.
+// Aggregate pass, two IRWLS updates and the block jackknife for all jobs,
+// every one of them of the given kind (REG_HSQ or REG_GENCOV).
 // outs[j] receives job j's result; ref_outs holds the h2 results that
 // REG_GENCOV jobs refer to by index.  part: njobs * nb * 5 doubles of
 // scratch; tot_delete (optional): njobs * nb; dv (optional): njobs * nb * 2
 // delete values.
 cudaError_t launch_regressions(const RegJob* jobs, RegState* states, RegOut* outs, const RegOut* ref_outs,
                                double* part, double* tot_delete, const double* ld, const double* wld, uint64_t n,
-                               int nb, double m, int njobs, cudaStream_t s, double* dv = nullptr);
+                               int nb, double m, int njobs, cudaStream_t s, double* dv = nullptr,
+                               int kind = REG_HSQ);
 
 // --two-step block starts: for each job, mask = y < mask_max, n1 = its size,
 // and seps[b] = index of the kept SNP of rank floor(b n1 / nb) (0 and n at
