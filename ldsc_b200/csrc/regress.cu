@@ -108,7 +108,10 @@ __device__ __forceinline__ uint64_t sep(uint64_t n, int nb, int b) {
 // of the block, RU loads in flight, then a warp reduction.  No block
 // barriers, and the order of the sums depends only on the block's bounds.
 constexpr int RJ = 8;  // jobs per CTA
-constexpr int RU = 4;  // SNPs per lane whose loads are issued together
+// SNPs per lane whose loads are issued together: six for h2 fits (three
+// CTAs per SM fit their registers), four for covariance fits
+template <int KIND>
+constexpr int reg_unroll() { return KIND == REG_HSQ ? 6 : 4; }
 
 template <int MODE, int KIND>
 __device__ __forceinline__ void reg_term(const RegJob& jb, const RegState& st, const WeightConsts& k, double y,
@@ -132,7 +135,7 @@ __device__ __forceinline__ void reg_term(const RegJob& jb, const RegState& st, c
 
 // KIND: the kind of every job of the launch (a job of another kind gets NaN sums).
 template <int MODE, int KIND>
-__global__ void __launch_bounds__(RJ * 32) k_reg_sums(const RegJob* __restrict__ jobs,
+__global__ void __launch_bounds__(RJ * 32, KIND == REG_HSQ ? 3 : 1) k_reg_sums(const RegJob* __restrict__ jobs,
                                                       const RegState* __restrict__ states,
                                                       const double* __restrict__ ld, const double* __restrict__ wld,
                                                       uint64_t n, int nb, double m, int njobs,
@@ -148,6 +151,7 @@ __global__ void __launch_bounds__(RJ * 32) k_reg_sums(const RegJob* __restrict__
     double s[5] = {0, 0, 0, 0, 0};
     // lane l takes SNPs lo + l, lo + l + 32, ... in that order; RU of them per
     // step have their loads in flight together
+    constexpr int RU = reg_unroll<KIND>();
     for (uint64_t i0 = lo + lane; i0 < hi; i0 += 32 * RU) {
         double y[RU], l[RU], wl[RU];
 #pragma unroll
@@ -400,7 +404,7 @@ constexpr int SEL_W = SEL_T / 32;
 constexpr int SEL_BITS = 11;
 constexpr int SEL_BINS = 1 << SEL_BITS;
 constexpr int SEL_CAP = 2048;  // keys ranked in shared memory
-constexpr int SEL_U = 4;       // loads in flight per thread
+constexpr int SEL_U = 8;       // loads in flight per thread
 
 // Calls f(key, valid) for every y of the job; the trip count is the same in
 // every lane of a warp, so f may use warp-collective operations.
@@ -421,7 +425,7 @@ __device__ __forceinline__ void sel_sweep(const RegJob& jb, uint64_t n, F f) {
     }
 }
 
-__global__ void __launch_bounds__(SEL_T) k_select_mid(const RegJob* __restrict__ jobs, uint64_t n, uint64_t ra,
+__global__ void __launch_bounds__(SEL_T, 8) k_select_mid(const RegJob* __restrict__ jobs, uint64_t n, uint64_t ra,
                                                       uint64_t rb, double* __restrict__ out_a,
                                                       double* __restrict__ out_b) {
     __shared__ uint32_t hist[SEL_BINS];
