@@ -734,7 +734,8 @@ def main():
     ap.add_argument("--serve-rates", default="", help="serving workload: comma-separated rates, one line each")
     ap.add_argument("--serve-seconds", type=float, default=30.0, help="serving: length of the arrival window")
     ap.add_argument("--serve-slots", type=int, default=6, help="serving: concurrent job slots")
-    ap.add_argument("--no-serving", action="store_true", help="skip the serving summary of the default run")
+    ap.add_argument("--no-serving", action="store_true",
+                    help="skip the serving and regression summaries of the default run")
     ap.add_argument("--sketch-d", default="200,1000,5000")
     ap.add_argument("--sketch-snps", type=int, default=0, help="truncate the sketch panel (profiling)")
     ap.add_argument("--part-snps", type=int, default=0,
@@ -981,6 +982,12 @@ def main():
             serving["config"] = sv["config"]
         except Exception as e:  # noqa: BLE001 -- reported in the line, the headline numbers stand
             serving = {"error": str(e)[:300]}
+    regressions = None
+    if world == 1 and not args.no_serving:
+        try:
+            regressions = run_regressions_workload(args)
+        except Exception as e:  # noqa: BLE001 -- reported in the line, the headline numbers stand
+            regressions = {"error": str(e)[:300]}
 
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": "r2 pairs/s", "n_gpus": world, "steps": args.steps,
@@ -990,6 +997,7 @@ def main():
                "data": "synthetic (seeded founder-mosaic panel generated on the device)",
                "config": config_dict(spec), "e2e": e2e, "gpu_launches": int(launches),
                "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks, "serving": serving,
+               "regressions": regressions,
                "int8_vs_oracle_max_rel_per_l2j": parity["int8_vs_oracle_max_rel_per_l2j"] if parity else None,
                "parity": parity,
                "forms": {"int8_pairs_per_s": value / world, "fp64_pairs_per_s": fp64_value,
