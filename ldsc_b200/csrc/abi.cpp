@@ -639,10 +639,14 @@ int ensure_overlap(ldsc_ctx* ctx, int n) {
 
 // Record chunks of the overlapped decode (each a multiple of the 128-record
 // right block), and the smallest run that overlaps.  On B200 at 50,000
-// individuals x 100,000 records, 4 and 8 chunks both cut a pass from 15.9 to
-// 15.4 ms; 16 chunks, or a decode confined to fewer blocks, slow the Gram
-// beside it more than they save.
+// individuals x 100,000 records, 4 and 8 equal chunks both cut a pass from
+// 15.9 to 15.4 ms; 16 chunks, or a decode confined to fewer blocks, slow the
+// Gram beside it more than they save.  A first chunk of 1/8 of the records
+// (the rest in three equal chunks) shortens the decode no Gram tile can
+// overlap: 15.23 / 15.46 -> 15.01 / 15.04 ms per pass over two runs each
+// (1/16: 15.04 / 15.08, 1/32: 15.45).
 constexpr int64_t OVERLAP_CHUNKS = 4;
+constexpr int64_t OVERLAP_FIRST_DIV = 8;
 constexpr int64_t OVERLAP_MIN_RECORDS = 16384;
 
 int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double* l2_out, double* maf_out,
@@ -952,8 +956,23 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
     // HBM-bound, the Gram tensor-bound, and decode blocks (40 registers x 256
     // threads, no shared memory) fit on an SM beside a Gram CTA.
     const bool overlap = !feed && exact_i8 && !fused_i8 && K == 1 && m >= OVERLAP_MIN_RECORDS;
-    const int64_t ov_per = overlap ? (int64_t)round_up((uint64_t)((m + OVERLAP_CHUNKS - 1) / OVERLAP_CHUNKS), 128) : 0;
-    const int ov_n = overlap ? (int)((m + ov_per - 1) / ov_per) : 0;
+    // chunk k = records [ov_b[k], ov_b[k + 1]); the first chunk is
+    // 1/OVERLAP_FIRST_DIV of the records (its decode runs before any Gram tile
+    // can), the rest are equal
+    std::vector<int64_t> ov_b;
+    if (overlap) {
+        const int64_t first = std::min<int64_t>(
+            m, (int64_t)round_up((uint64_t)((m + OVERLAP_FIRST_DIV - 1) / OVERLAP_FIRST_DIV), 128));
+        ov_b.push_back(0);
+        ov_b.push_back(first);
+        const int64_t rest = m - first, nrest = OVERLAP_CHUNKS - 1;
+        const int64_t per = rest > 0 ? (int64_t)round_up((uint64_t)((rest + nrest - 1) / nrest), 128) : 0;
+        for (int64_t r = first; r < m;) {
+            r = std::min<int64_t>(m, r + per);
+            ov_b.push_back(r);
+        }
+    }
+    const int ov_n = overlap ? (int)ov_b.size() - 1 : 0;
     if (stream_gram) {
         // the first chunk's copy runs while the host plans; the plan's uploads
         // queue behind that chunk only
@@ -1042,7 +1061,7 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
         CK(cudaEventRecord(ctx->ovl_go, s));
         CK(cudaStreamWaitEvent(ctx->side, ctx->ovl_go, 0));
         for (int k = 0; k < ov_n; k++) {
-            const int64_t r0 = k * ov_per, r1 = std::min<int64_t>(m, r0 + ov_per);
+            const int64_t r0 = ov_b[k], r1 = ov_b[k + 1];
             PanelView pc = pv;
             if (!rr) pc.rows = pv.rows + (uint64_t)r0 * pv.pitch;
             RecStats sc = st;
@@ -1106,7 +1125,7 @@ int run_l2(ldsc_ctx* ctx, const ldsc_panel* panel, const ldsc_l2_args* a, double
         // right block is complete once chunks [0, k] are decoded
         size_t t0 = 0;
         for (int k = 0; k < ov_n; k++) {
-            const int64_t r1 = std::min<int64_t>(m, (k + 1) * ov_per);
+            const int64_t r1 = ov_b[k + 1];
             size_t t1 = t0;
             while (t1 < tiles.size() && (r1 == m || (int64_t)(tiles[t1].b_blk + 1) * tb <= r1)) t1++;
             if (t1 == t0) continue;
@@ -1921,11 +1940,11 @@ extern "C" int ldsc_rg_batch(ldsc_ctx* ctx, const ldsc_rg_args* a, ldsc_rg_resul
                                      (uint64_t)ctx->rg_res.p};
     CK(graph_launch(ctx, gkey, s, [&](cudaStream_t gs) -> cudaError_t {
         cudaError_t e2 = launch_regressions(dj, dst, dout, nullptr, ctx->rg_part.as<double>(), dtd, d_ld, d_wld, n,
-                                            nb, a->m_snps, 2 * P, gs);
+                                            nb, a->m_snps, 2 * P, gs, nullptr, REG_FORM_HSQ_SQUARE);
         if (e2 != cudaSuccess) return e2;
         e2 = launch_regressions(dj + 2 * P, dst + 2 * P, dout + 2 * P, dout,
                                 ctx->rg_part.as<double>() + (size_t)2 * P * nb * 5, dtd + (size_t)2 * P * nb, d_ld,
-                                d_wld, n, nb, a->m_snps, P, gs, nullptr, REG_GENCOV);
+                                d_wld, n, nb, a->m_snps, P, gs, nullptr, REG_FORM_GENCOV_PRODUCT);
         if (e2 != cudaSuccess) return e2;
         return launch_rg_finish(ctx->rg_pairs.as<RgPairIdx>(), dout, dtd, nb, ctx->rg_res.as<RgOut>(), P, gs);
     }));

@@ -33,11 +33,6 @@ __device__ __forceinline__ double job_y(const RegJob& jb, uint64_t i) {
 }
 __device__ __forceinline__ double job_n1(const RegJob& jb, uint64_t i) { return jb.n1 ? jb.n1[i] : jb.n1s; }
 __device__ __forceinline__ double job_n2(const RegJob& jb, uint64_t i) { return jb.n2 ? jb.n2[i] : jb.n2s; }
-// sample size that scales the regressor: N (h2) or sqrt(N1 N2) (gencov)
-template <int KIND>
-__device__ __forceinline__ double job_nx(const RegJob& jb, uint64_t i) {
-    return KIND == REG_HSQ ? job_n1(jb, i) : sqrt(job_n1(jb, i) * job_n2(jb, i));
-}
 
 // Per-job constants of the weights, formed once per pass.
 struct WeightConsts {
@@ -63,18 +58,16 @@ __device__ __forceinline__ WeightConsts weight_consts(const RegState& st, double
 // heteroskedasticity term and of the overcounting LD score) are taken as one.
 template <int KIND>
 __device__ __forceinline__ double job_weight(const RegJob& jb, const RegState& st, const WeightConsts& k,
-                                             double ld_raw, double wld_raw, uint64_t i) {
+                                             double ld_raw, double wld_raw, double n1, double n2) {
     const double ocd = fmax(wld_raw, 1.0);
     if (KIND == REG_HSQ) {
         // step 1 of --two-step re-weights with the regressor in place of the LD
         // score (src/h2.rs:347-351: ldsc_weights(x1_col0, ...))
-        const double n1 = job_n1(jb, i);
         const double ld = jb.ld_from_x && st.n_updates > 0 ? fmax(n1 * ld_raw * k.inv_nbar, 1.0) : fmax(ld_raw, 1.0);
         const double t = st.intercept + k.hm * n1 * ld;
         return 1.0 / (2.0 * t * t * ocd);
     }
     const double ld = fmax(ld_raw, 1.0);
-    const double n1 = job_n1(jb, i), n2 = job_n2(jb, i);
     const double a = n1 * k.h1m * ld + st.int_h1;
     const double b = n2 * k.h2m * ld + st.int_h2;
     const double c = sqrt(n1 * n2) * k.sm * ld + st.intercept;
@@ -108,22 +101,20 @@ __device__ __forceinline__ uint64_t sep(uint64_t n, int nb, int b) {
 // of the block, RU loads in flight, then a warp reduction.  No block
 // barriers, and the order of the sums depends only on the block's bounds.
 constexpr int RJ = 8;  // jobs per CTA
-// SNPs per lane whose loads are issued together: six for h2 fits (three
-// CTAs per SM fit their registers), four for covariance fits
-template <int KIND>
-constexpr int reg_unroll() { return KIND == REG_HSQ ? 6 : 4; }
+constexpr int RU = 4;  // SNPs per lane whose loads are issued together
 
 template <int MODE, int KIND>
 __device__ __forceinline__ void reg_term(const RegJob& jb, const RegState& st, const WeightConsts& k, double y,
-                                         double l, double wl, uint64_t i, double* s) {
+                                         double l, double wl, double n1, double n2, double* s) {
     if (MODE == 1 && jb.use_mask && !(y < jb.mask_max)) return;
-    const double nx = job_nx<KIND>(jb, i);
+    // sample size that scales the regressor: N (h2) or sqrt(N1 N2) (gencov)
+    const double nx = KIND == REG_HSQ ? n1 : sqrt(n1 * n2);
     if (MODE == 0) {
         s[0] += y;
         s[1] += l * nx;
         s[2] += nx;
     } else {
-        const double w = job_weight<KIND>(jb, st, k, l, wl, i);
+        const double w = job_weight<KIND>(jb, st, k, l, wl, n1, n2);
         const double x0 = nx * l * k.inv_nbar;
         s[0] += w * x0 * x0;
         s[1] += w * x0;
@@ -133,13 +124,20 @@ __device__ __forceinline__ void reg_term(const RegJob& jb, const RegState& st, c
     }
 }
 
-// KIND: the kind of every job of the launch (a job of another kind gets NaN sums).
-template <int MODE, int KIND>
-__global__ void __launch_bounds__(RJ * 32, KIND == REG_HSQ ? 3 : 1) k_reg_sums(const RegJob* __restrict__ jobs,
-                                                      const RegState* __restrict__ states,
-                                                      const double* __restrict__ ld, const double* __restrict__ wld,
-                                                      uint64_t n, int nb, double m, int njobs,
-                                                      double* __restrict__ part) {
+// Kind and y of every job of a launch (FORM = REG_FORM_*).
+__host__ __device__ constexpr int form_kind(int f) { return f == REG_FORM_GENCOV_PRODUCT ? REG_GENCOV : REG_HSQ; }
+__host__ __device__ constexpr int form_ymode(int f) {
+    return f == REG_FORM_HSQ_DIRECT ? REG_Y_DIRECT : (f == REG_FORM_HSQ_SQUARE ? REG_Y_SQUARE : REG_Y_PRODUCT);
+}
+
+// FORM: the kind and y of every job of the launch (a job of another form gets
+// NaN sums).  The job's arrays are offset to its block once, so the per-SNP
+// indexing is 32-bit and the y form is fixed at compile time.
+template <int MODE, int FORM>
+__global__ void __launch_bounds__(RJ * 32, form_kind(FORM) == REG_HSQ ? 3 : 1)
+    k_reg_sums(const RegJob* __restrict__ jobs, const RegState* __restrict__ states, const double* __restrict__ ld,
+               const double* __restrict__ wld, uint64_t n, int nb, double m, int njobs, double* __restrict__ part) {
+    constexpr int KIND = form_kind(FORM), YM = form_ymode(FORM);
     const int lane = threadIdx.x & 31;
     const int b = blockIdx.x, j = blockIdx.y * RJ + (threadIdx.x >> 5);
     if (j >= njobs) return;
@@ -147,26 +145,37 @@ __global__ void __launch_bounds__(RJ * 32, KIND == REG_HSQ ? 3 : 1) k_reg_sums(c
     const RegState st = states[j];
     const uint64_t lo = jb.seps ? (uint64_t)jb.seps[b] : sep(n, nb, b);
     const uint64_t hi = jb.seps ? (uint64_t)jb.seps[b + 1] : sep(n, nb, b + 1);
+    const uint32_t cnt = (uint32_t)(hi - lo);  // n < 2^31 (checked by the launcher)
+    const double* __restrict__ ya = jb.ya + lo;
+    const double* __restrict__ yb = YM == REG_Y_PRODUCT ? jb.yb + lo : nullptr;
+    const double* __restrict__ n1p = jb.n1 ? jb.n1 + lo : nullptr;
+    const double* __restrict__ n2p = (KIND == REG_GENCOV && jb.n2) ? jb.n2 + lo : nullptr;
+    const double* __restrict__ lb = ld + lo;
+    const double* __restrict__ wb = wld + lo;
     const WeightConsts k = weight_consts(st, m);
     double s[5] = {0, 0, 0, 0, 0};
     // lane l takes SNPs lo + l, lo + l + 32, ... in that order; RU of them per
     // step have their loads in flight together
-    constexpr int RU = reg_unroll<KIND>();
-    for (uint64_t i0 = lo + lane; i0 < hi; i0 += 32 * RU) {
-        double y[RU], l[RU], wl[RU];
+    for (uint32_t k0 = lane; k0 < cnt; k0 += 32 * RU) {
+        double y[RU], l[RU], wl[RU], n1[RU], n2[RU];
 #pragma unroll
         for (int u = 0; u < RU; u++) {
-            const uint64_t i = i0 + 32 * (uint64_t)u;
-            const bool v = i < hi;
-            y[u] = v ? job_y(jb, i) : 0.0;
-            l[u] = v ? ld[i] : 0.0;
-            wl[u] = (MODE == 1 && v) ? wld[i] : 1.0;
+            const uint32_t q = k0 + 32 * u;
+            const bool v = q < cnt;
+            double a = v ? ya[q] : 0.0;
+            if (YM == REG_Y_SQUARE) a = fmax(a * a, 0.0);
+            if (YM == REG_Y_PRODUCT) a *= v ? yb[q] : 0.0;
+            y[u] = a;
+            l[u] = v ? lb[q] : 0.0;
+            wl[u] = (MODE == 1 && v) ? wb[q] : 1.0;
+            n1[u] = (n1p && v) ? n1p[q] : jb.n1s;
+            n2[u] = KIND == REG_GENCOV ? ((n2p && v) ? n2p[q] : jb.n2s) : 0.0;
         }
 #pragma unroll
         for (int u = 0; u < RU; u++)
-            if (i0 + 32 * (uint64_t)u < hi) reg_term<MODE, KIND>(jb, st, k, y[u], l[u], wl[u], i0 + 32 * (uint64_t)u, s);
+            if (k0 + 32 * u < cnt) reg_term<MODE, KIND>(jb, st, k, y[u], l[u], wl[u], n1[u], n2[u], s);
     }
-    if (jb.kind != KIND)
+    if (jb.kind != KIND || jb.ymode != YM)
 #pragma unroll
         for (int q = 0; q < 5; q++) s[q] = NAN;
     constexpr int NQ = MODE == 0 ? 3 : 5;
@@ -704,20 +713,23 @@ cudaError_t launch_twostep_combine(const RegOut* out1, const RegOut* out2, const
 
 cudaError_t launch_regressions(const RegJob* jobs, RegState* states, RegOut* outs, const RegOut* ref_outs,
                                double* part, double* tot_delete, const double* ld, const double* wld, uint64_t n,
-                               int nb, double m, int njobs, cudaStream_t s, double* dv, int kind) {
+                               int nb, double m, int njobs, cudaStream_t s, double* dv, int form) {
     if (njobs <= 0) return cudaSuccess;
-    if (kind != REG_HSQ && kind != REG_GENCOV) return cudaErrorInvalidValue;
+    if (form < REG_FORM_HSQ_DIRECT || form > REG_FORM_GENCOV_PRODUCT || n >= (1ull << 31))
+        return cudaErrorInvalidValue;
     const dim3 grid(nb, (njobs + RJ - 1) / RJ);
     const int ub = (njobs + 3) / 4;  // k_reg_update: four warps (jobs) per CTA
     auto sums = [&](int mode) {
-        if (mode == 0 && kind == REG_HSQ)
-            k_reg_sums<0, REG_HSQ><<<grid, RJ * 32, 0, s>>>(jobs, states, ld, wld, n, nb, m, njobs, part);
-        else if (mode == 0)
-            k_reg_sums<0, REG_GENCOV><<<grid, RJ * 32, 0, s>>>(jobs, states, ld, wld, n, nb, m, njobs, part);
-        else if (kind == REG_HSQ)
-            k_reg_sums<1, REG_HSQ><<<grid, RJ * 32, 0, s>>>(jobs, states, ld, wld, n, nb, m, njobs, part);
-        else
-            k_reg_sums<1, REG_GENCOV><<<grid, RJ * 32, 0, s>>>(jobs, states, ld, wld, n, nb, m, njobs, part);
+        if (form == REG_FORM_HSQ_DIRECT) {
+            if (mode == 0) k_reg_sums<0, REG_FORM_HSQ_DIRECT><<<grid, RJ * 32, 0, s>>>(jobs, states, ld, wld, n, nb, m, njobs, part);
+            else k_reg_sums<1, REG_FORM_HSQ_DIRECT><<<grid, RJ * 32, 0, s>>>(jobs, states, ld, wld, n, nb, m, njobs, part);
+        } else if (form == REG_FORM_HSQ_SQUARE) {
+            if (mode == 0) k_reg_sums<0, REG_FORM_HSQ_SQUARE><<<grid, RJ * 32, 0, s>>>(jobs, states, ld, wld, n, nb, m, njobs, part);
+            else k_reg_sums<1, REG_FORM_HSQ_SQUARE><<<grid, RJ * 32, 0, s>>>(jobs, states, ld, wld, n, nb, m, njobs, part);
+        } else {
+            if (mode == 0) k_reg_sums<0, REG_FORM_GENCOV_PRODUCT><<<grid, RJ * 32, 0, s>>>(jobs, states, ld, wld, n, nb, m, njobs, part);
+            else k_reg_sums<1, REG_FORM_GENCOV_PRODUCT><<<grid, RJ * 32, 0, s>>>(jobs, states, ld, wld, n, nb, m, njobs, part);
+        }
     };
     sums(0);
     k_reg_update<0><<<ub, 128, 0, s>>>(jobs, states, ref_outs, part, n, nb, m, njobs);
@@ -745,10 +757,12 @@ cudaError_t launch_select_mid(const RegJob* jobs, uint64_t n, uint64_t ra, uint6
 }
 
 cudaError_t preload_regress() {
-    cudaError_t e = preload_kernel(k_reg_sums<0, REG_HSQ>);
-    if (e == cudaSuccess) e = preload_kernel(k_reg_sums<1, REG_HSQ>);
-    if (e == cudaSuccess) e = preload_kernel(k_reg_sums<0, REG_GENCOV>);
-    if (e == cudaSuccess) e = preload_kernel(k_reg_sums<1, REG_GENCOV>);
+    cudaError_t e = preload_kernel(k_reg_sums<0, REG_FORM_HSQ_DIRECT>);
+    if (e == cudaSuccess) e = preload_kernel(k_reg_sums<1, REG_FORM_HSQ_DIRECT>);
+    if (e == cudaSuccess) e = preload_kernel(k_reg_sums<0, REG_FORM_HSQ_SQUARE>);
+    if (e == cudaSuccess) e = preload_kernel(k_reg_sums<1, REG_FORM_HSQ_SQUARE>);
+    if (e == cudaSuccess) e = preload_kernel(k_reg_sums<0, REG_FORM_GENCOV_PRODUCT>);
+    if (e == cudaSuccess) e = preload_kernel(k_reg_sums<1, REG_FORM_GENCOV_PRODUCT>);
     if (e == cudaSuccess) e = preload_kernel(k_reg_update<0>);
     if (e == cudaSuccess) e = preload_kernel(k_reg_update<1>);
     if (e == cudaSuccess) e = preload_kernel(k_reg_jackknife);

@@ -8,6 +8,9 @@ namespace ldsc {
 
 enum { REG_HSQ = 0, REG_GENCOV = 1 };
 enum { REG_Y_DIRECT = 0, REG_Y_SQUARE = 1, REG_Y_PRODUCT = 2 };
+// (kind, y) shared by every job of one launch_regressions call: h2 fits on
+// chi2, h2 fits on z (y = z^2), genetic-covariance fits (y = z1 z2)
+enum { REG_FORM_HSQ_DIRECT = 0, REG_FORM_HSQ_SQUARE = 1, REG_FORM_GENCOV_PRODUCT = 2 };
 
 // One regression: y ~ [x0 = Nx * ld / nbar, 1] with weights of its kind.
 struct RegJob {
@@ -59,7 +62,7 @@ struct RgOut {
 };
 
 // Aggregate pass, two IRWLS updates and the block jackknife for all jobs,
-// every one of them of the given kind (REG_HSQ or REG_GENCOV).
+// every one of them of the given form (REG_FORM_*); n < 2^31.
 // outs[j] receives job j's result; ref_outs holds the h2 results that
 // REG_GENCOV jobs refer to by index.  part: njobs * nb * 5 doubles of
 // scratch; tot_delete (optional): njobs * nb; dv (optional): njobs * nb * 2
@@ -67,7 +70,7 @@ struct RgOut {
 cudaError_t launch_regressions(const RegJob* jobs, RegState* states, RegOut* outs, const RegOut* ref_outs,
                                double* part, double* tot_delete, const double* ld, const double* wld, uint64_t n,
                                int nb, double m, int njobs, cudaStream_t s, double* dv = nullptr,
-                               int kind = REG_HSQ);
+                               int form = REG_FORM_HSQ_DIRECT);
 
 // --two-step block starts: for each job, mask = y < mask_max, n1 = its size,
 // and seps[b] = index of the kept SNP of rank floor(b n1 / nb) (0 and n at
