@@ -154,8 +154,9 @@ def cpu_gemm_fields(work):
     return {"gemm_gflops_per_core": work["gemm_gflops_per_core"],
             "gemm_share_of_time": work["gemm_share_of_time"],
             "useful_gflops_per_core": work["useful_gflops_per_core"],
-            "gemm_note": "cache-blocked dot-product kernel of the C restatement (64 x 64 column macro tiles, "
-                         "4 x 4 AVX-512 register blocks where the host has AVX-512, else 3 x 4 AVX2; no packing); "
+            "gemm_note": "cache-blocked Gram of the C restatement (64 x 64 column macro tiles, 256-individual "
+                         "slices; where the host has AVX-512 the slice's A columns are packed and a 16 x 8 "
+                         "outer-product micro kernel runs over them, else 3 x 4 AVX2 dot-product blocks); "
                          "gemm = dot products the chunk Grams computed, useful = 2 N per counted pair"}
 
 

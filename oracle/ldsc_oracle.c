@@ -326,12 +326,12 @@ static inline v8f ld8f(const float *p) {
 /* Cache-blocked column Gram.  Each thread owns a macro tile of GB_W A columns
  * x GB_C B columns and walks the individual axis in chunks of GB_K: a chunk
  * of the macro tile's columns (GB_W + GB_C columns x 2 KB) stays in the
- * core's L2 while every register block of the tile (3 x 4 AVX2 vectors, or
- * 4 x 4 AVX-512 vectors where the host has them) reads it, so a
- * column is fetched from memory once per chunk instead of once per register
- * block.  Within a block the dot products are vectorised along the
- * individual axis; tails are scalar.  Summation order differs from faer's,
- * as any blocked GEMM's would. */
+ * core's L2 while every register block of the tile reads it, so a column is
+ * fetched from memory once per chunk instead of once per register block.
+ * With AVX2 the register blocks are 3 x 4 dot products vectorised along the
+ * individual axis (scalar tails); with AVX-512 the A chunk is packed and a
+ * 16 x 8 outer-product micro kernel runs over it (gram_f64_packed).
+ * Summation order differs from faer's, as any blocked GEMM's would. */
 #ifndef GB_W
 #define GB_W 64
 #endif
@@ -342,12 +342,18 @@ static inline v8f ld8f(const float *p) {
 #define GB_K 256
 #endif
 
-/* The same on hosts with AVX-512 (chosen at run time): 4 x 4 register blocks
- * of 8-double vectors, 16 accumulators fed by 4 A and 4 B loads per step of
- * 8 individuals. */
+/* 8-double vectors for hosts with AVX-512 (chosen at run time). */
 typedef double v8d __attribute__((vector_size(64)));
 
-__attribute__((target("avx512f"))) static void gram_f64_avx512(int64_t n, int64_t w, int64_t c,
+/* Packed form for hosts with AVX-512: per macro tile and chunk of GB_K
+ * individuals, the tile's A columns are packed into 16-row panels (for each
+ * individual, 16 consecutive output rows contiguous), and a 16 x 8 micro
+ * kernel keeps 16 accumulators: per individual two panel loads, eight
+ * broadcasts of B and sixteen vector FMAs, with no horizontal sums.  Output
+ * rows past the tile are zero-padded in the panels and not stored. */
+#define PK_R 16
+#define PK_C 8
+__attribute__((target("avx512f"))) static void gram_f64_packed(int64_t n, int64_t w, int64_t c,
                                                                double *const *acol, double *const *bcol,
                                                                double *out) {
     const int64_t nwt = (w + GB_W - 1) / GB_W, nct = (c + GB_C - 1) / GB_C;
@@ -356,39 +362,50 @@ __attribute__((target("avx512f"))) static void gram_f64_avx512(int64_t n, int64_
         for (int64_t wt = 0; wt < nwt; wt++) {
             const int64_t i0 = wt * GB_W, i1 = i0 + GB_W < w ? i0 + GB_W : w;
             const int64_t j0 = ct * GB_C, j1 = j0 + GB_C < c ? j0 + GB_C : c;
+            const int64_t nr = i1 - i0, np = (nr + PK_R - 1) / PK_R;
             double tile[GB_W * GB_C];
             memset(tile, 0, sizeof(tile));
+            static __thread double pa[GB_W * GB_K] __attribute__((aligned(64)));
             for (int64_t k0 = 0; k0 < n; k0 += GB_K) {
-                const int64_t k1 = k0 + GB_K < n ? k0 + GB_K : n;
-                const int64_t kv = k0 + ((k1 - k0) & ~(int64_t)7);
-                for (int64_t jb = j0; jb < j1; jb += 4) {
-                    for (int64_t ib = i0; ib < i1; ib += 4) {
-                        const int64_t ie = ib + 4 < i1 ? ib + 4 : i1;
-                        const int64_t je = jb + 4 < j1 ? jb + 4 : j1;
-                        const double *ap[4], *bp[4];
-                        for (int t = 0; t < 4; t++) ap[t] = acol[ib + t < ie ? ib + t : ib];
-                        for (int t = 0; t < 4; t++) bp[t] = bcol[jb + t < je ? jb + t : jb];
-                        v8d acc[4][4];
-                        memset(acc, 0, sizeof(acc));
-                        for (int64_t k = k0; k < kv; k += 8) {
-                            v8d a[4];
-                            for (int t = 0; t < 4; t++) memcpy(&a[t], ap[t] + k, sizeof(v8d));
-                            for (int u = 0; u < 4; u++) {
-                                v8d b;
-                                memcpy(&b, bp[u] + k, sizeof(v8d));
-                                acc[0][u] += a[0] * b;
-                                acc[1][u] += a[1] * b;
-                                acc[2][u] += a[2] * b;
-                                acc[3][u] += a[3] * b;
+                const int64_t kc = (k0 + GB_K < n ? k0 + GB_K : n) - k0;
+                /* pack: panel p, individual kk, row r at pa[(p * GB_K + kk) * PK_R + r] */
+                for (int64_t p = 0; p < np; p++)
+                    for (int64_t r = 0; r < PK_R; r++) {
+                        const int64_t i = i0 + p * PK_R + r;
+                        double *dst = pa + (p * GB_K) * PK_R + r;
+                        if (i < i1) {
+                            const double *src = acol[i] + k0;
+                            for (int64_t kk = 0; kk < kc; kk++) dst[kk * PK_R] = src[kk];
+                        } else {
+                            for (int64_t kk = 0; kk < kc; kk++) dst[kk * PK_R] = 0.0;
+                        }
+                    }
+                for (int64_t jb = j0; jb < j1; jb += PK_C) {
+                    const int64_t je = jb + PK_C < j1 ? jb + PK_C : j1;
+                    const double *bp[PK_C];
+                    for (int t = 0; t < PK_C; t++) bp[t] = bcol[jb + t < je ? jb + t : jb] + k0;
+                    for (int64_t p = 0; p < np; p++) {
+                        const double *ap = pa + (p * GB_K) * PK_R;
+                        v8d acc0[PK_C], acc1[PK_C];
+                        memset(acc0, 0, sizeof(acc0));
+                        memset(acc1, 0, sizeof(acc1));
+                        for (int64_t kk = 0; kk < kc; kk++) {
+                            v8d a0, a1;
+                            memcpy(&a0, ap + kk * PK_R, sizeof(v8d));
+                            memcpy(&a1, ap + kk * PK_R + 8, sizeof(v8d));
+                            for (int t = 0; t < PK_C; t++) {
+                                const double bv = bp[t][kk];
+                                const v8d b = {bv, bv, bv, bv, bv, bv, bv, bv};
+                                acc0[t] += a0 * b;
+                                acc1[t] += a1 * b;
                             }
                         }
-                        for (int64_t i = ib; i < ie; i++)
-                            for (int64_t j = jb; j < je; j++) {
-                                v8d v = acc[i - ib][j - jb];
-                                double s = ((v[0] + v[1]) + (v[2] + v[3])) + ((v[4] + v[5]) + (v[6] + v[7]));
-                                for (int64_t k = kv; k < k1; k++) s += ap[i - ib][k] * bp[j - jb][k];
-                                tile[(i - i0) + (j - j0) * GB_W] += s;
-                            }
+                        for (int64_t j = jb; j < je; j++) {
+                            double *trow = tile + (j - j0) * GB_W + p * PK_R;
+                            const int64_t rmax = nr - p * PK_R < PK_R ? nr - p * PK_R : PK_R;
+                            for (int64_t r = 0; r < rmax; r++)
+                                trow[r] += r < 8 ? acc0[j - jb][r] : acc1[j - jb][r - 8];
+                        }
                     }
                 }
             }
@@ -401,7 +418,7 @@ __attribute__((target("avx512f"))) static void gram_f64_avx512(int64_t n, int64_
 static void gram_f64(int64_t n, int64_t w, int64_t c, double *const *acol, double *const *bcol,
                      double *out) {
     if (__builtin_cpu_supports("avx512f")) {
-        gram_f64_avx512(n, w, c, acol, bcol, out);
+        gram_f64_packed(n, w, c, acol, bcol, out);
         return;
     }
     const int64_t nwt = (w + GB_W - 1) / GB_W, nct = (c + GB_C - 1) / GB_C;
