@@ -102,6 +102,26 @@ def test_oracle_matches_brute_force(mode, wind, half, chunk, masking, per_chr, a
     assert np.max(np.abs(l2 - ref) / scale) < 1e-10
 
 
+@pytest.mark.parametrize("masking,chunk", [(True, 200), (False, 50)])
+def test_oracle_wide_panel_matches_brute_force(masking, chunk):
+    """700 individuals (several 256-individual slices of the chunk Grams, with
+    a ragged last slice) and windows wider than one 64-column macro tile, so
+    the blocked and packed Gram kernels' slice and tile edges are all
+    crossed."""
+    from ldsc_b200 import synth
+    spec = synth.PanelSpec(n_indiv=700, chrom_sizes=[320], chrom_cm=[2.0], founders=20, miss=0.02, seed=5)
+    body = synth.bed_body(spec)
+    chr_, cm, bp = synth.positions(spec)
+    a = OracleL2Args(bed_body=body, n_file_indiv=spec.n_indiv, chr=chr_, cm=cm, bp=bp, chunk_c=chunk,
+                     masking=masking)
+    l2, maf, pairs, _ = oracle_l2(a)
+    left = py_left_limits(chr_, cm, bp, "cm", 1.0, 0, chunk, masking, True)
+    assert int(np.max(np.arange(len(chr_)) - left)) > 64
+    ref, ref_maf = brute_force_l2(body, spec.n_indiv, chr_, cm, bp, left)
+    np.testing.assert_allclose(maf, ref_maf, atol=1e-15)
+    assert np.max(np.abs(l2 - ref) / np.maximum(np.abs(ref), 1.0)) < 1e-10
+
+
 def test_oracle_keep_subset_matches_brute_force():
     z = np.load(os.path.join(GOLDEN, "small_panel.npz"))
     body, n = z["body"], int(z["n_indiv"])
