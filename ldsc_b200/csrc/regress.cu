@@ -31,8 +31,6 @@ __device__ __forceinline__ double job_y(const RegJob& jb, uint64_t i) {
     if (jb.ymode == REG_Y_PRODUCT) return a * jb.yb[i];
     return a;
 }
-__device__ __forceinline__ double job_n1(const RegJob& jb, uint64_t i) { return jb.n1 ? jb.n1[i] : jb.n1s; }
-__device__ __forceinline__ double job_n2(const RegJob& jb, uint64_t i) { return jb.n2 ? jb.n2[i] : jb.n2s; }
 
 // Per-job constants of the weights, formed once per pass.
 struct WeightConsts {
